@@ -1,0 +1,153 @@
+/*
+ * yspec_gpu.h -- C-ABI of the B200 radial-integration engine.
+ *
+ * This boundary replaces, in the reference program (da380/YSpec, src/):
+ *   yspec.f90:250-426   the (omega,l) double loop: per-pair radial, toroidal
+ *                       and spheroidal solves (module_solver.f90:25-1847,
+ *                       module_int.f90:134-2138, module_start.f90:14-178)
+ *                       and the receiver l-sum with Legendre factors
+ *                       (yspec.f90:155-174 table, :291-293, :316-335,
+ *                       :396-419 sums)
+ *   yspec.f90:432-486   ifft (module_fourier.f90:55-145), e^{eps t},
+ *                       dimensionalisation and rotation to Z/N/E.
+ * The host keeps everything before (parameter file, read_model with its
+ * splines and gravity, delaz, fcal, radius indices) and the ASCII writer.
+ *
+ * Conventions: plain pointers and sizes only; host buffers are owned by the
+ * caller; complex(dp) arrays are interleaved (re, im) doubles; arrays are
+ * column-major with the reference's dimension order; knot and interval
+ * indices are 1-based exactly as the reference computes them.  Every call
+ * returns a status (YSG_OK == 0); nonzero codes replace the reference's
+ * `stop` statements and ysg_status_string() gives the message.
+ *
+ * One handle per host thread; a handle owns one CUDA stream on one device.
+ */
+#ifndef YSPEC_GPU_H
+#define YSPEC_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    YSG_OK = 0,
+    YSG_ERR_ARG = 1,          /* bad argument or size */
+    YSG_ERR_CUDA = 2,         /* CUDA runtime error */
+    YSG_ERR_NO_MODEL = 3,     /* ysg_model_upload not called */
+    YSG_ERR_NO_SPECTRA = 4,   /* traces requested before spectra */
+    YSG_ERR_DEVICE_WAIT = 5,  /* a bounded device-side wait gave up */
+    YSG_ERR_NO_DEVICE = 6,    /* no CUDA device */
+    YSG_ERR_LIMIT = 7         /* size beyond a fixed capacity */
+};
+
+typedef struct ysg_handle ysg_handle;
+
+/* Earth model after module_model.f90:175-383 (read_model): normalised knot
+ * values and per-layer natural-spline second derivatives.  Each pointer is
+ * an array of nknot doubles (knot 1 first).  The 13 parameters are, in
+ * order: rho, acon, ccon, fcon, lcon, ncon, kappa, mu, qkappa, qmu, grav,
+ * xlam, xa2 (module_model.f90:129-160). */
+typedef struct {
+    int nknot, nic, noc, nsl;        /* module_model.f90:121-125 */
+    int ocean, fic;                  /* module_model.f90:119-120 */
+    double tref;                     /* normalised 2 pi / T_ref (:195-197) */
+    double pibigg;                   /* module_model.f90:490 */
+    double fre_norm;                 /* module_model.f90:484 */
+    const double *r;
+    const double *val[13];
+    const double *cs[13];
+    const double *alpha, *beta;      /* module_model.f90:276-277 */
+} ysg_model;
+
+/* One event's spectral problem (yspec.f90:176-261 after normalisation). */
+typedef struct {
+    int lmin, lmax;
+    int nw;                          /* i2 - i1 + 1 frequencies */
+    int is, ir;                      /* find_radius_index of source, receiver */
+    int ats, grav, out, cor;         /* switches, yspec.f90:100-103 */
+    int nr;                          /* receivers */
+    double wmin, dw, ep;             /* omega_j = wmin + (j-1) dw - i ep */
+    double rs, rr;                   /* normalised source / receiver radius */
+    double mm[6];                    /* moment tensor / moment_norm */
+    const double *delta;             /* nr epicentral angles (delaz), rad */
+    const double *azst;              /* nr azimuths after yspec.f90:150 */
+} ysg_event;
+
+/* Time-series stage (fcal outputs, filter, output scaling). */
+typedef struct {
+    int nt, i1, i2;                  /* module_fourier.f90:362-397 */
+    int nr;
+    double df, dt, ep, tout;         /* normalised */
+    double f11, f12, f21, f22;       /* normalised corners; all 0 = no filter */
+    double t_norm;                   /* module_model.f90:485 */
+    double amp_norm;                 /* r_norm, vel_norm or acl_norm */
+    const double *azep;              /* nr azimuths after yspec.f90:149 */
+} ysg_time;
+
+/* Create a handle on CUDA device `device`.  Replaces nothing in the
+ * reference (which has no device); allocates the stream and status word. */
+int ysg_create(ysg_handle **h, int device);
+
+/* Upload the model (replaces the module_model.f90:118-160 globals that the
+ * solver modules read).  Copies the arrays; the caller may free them. */
+int ysg_model_upload(ysg_handle *h, const ysg_model *m);
+
+/* Spectra of one event: yspec.f90:250-426.  ur, ut, up are complex
+ * (nw, nr) column-major host arrays (interleaved re/im), or NULL to keep
+ * the spectra on the device only.  Also leaves the spectra on the device
+ * for ysg_event_traces. */
+int ysg_event_spectra(ysg_handle *h, const ysg_event *ev, double *ur, double *ut, double *up);
+
+/* Time series of the last spectra: module_fourier.f90:55-145 and
+ * yspec.f90:432-486.  out is (nout, 4, nr) column-major: time in seconds,
+ * then Re of the Z, N, E components in SI units, exactly the four columns
+ * the reference writes.  *nout receives the row count (yspec.f90:479-486);
+ * out must hold nout_max(tm) * 4 * nr doubles. */
+int ysg_event_traces(ysg_handle *h, const ysg_time *tm, double *out, int *nout);
+
+/* Rows the trace output will have for tm (yspec.f90:479-486). */
+int ysg_trace_rows(const ysg_time *tm);
+
+/* Spectra then traces without copying the spectra to the host. */
+int ysg_event_run(ysg_handle *h, const ysg_event *ev, const ysg_time *tm, double *out,
+                  int *nout);
+
+/* Several events through the batched persistent solver: one launch per
+ * stage for all events, CUDA-graph captured.  outs[e] receives the traces of
+ * event e as ysg_event_traces does; nouts[e] its row count.  Events share
+ * the uploaded model. */
+int ysg_batch_run(ysg_handle *h, int nev, const ysg_event *evs, const ysg_time *tms,
+                  double **outs, int *nouts);
+
+/* Per-(omega,l) l-sum coefficients uu(1:5), vv(1:5), ww(1:5) of
+ * yspec.f90:281-400 for one event: coef is complex (nw, 15, L) with
+ * L = lmax - lmin + 1, omega fastest.  Diagnostic entry point used by the
+ * parity tests; it runs only the solve stage. */
+int ysg_event_coef(ysg_handle *h, const ysg_event *ev, double *coef);
+
+/* Legendre table of yspec.f90:155-170 for nr angles: table is
+ * (8, nr, lmax+1) column-major with rows X_l0, X_l1, X_l2, dX_l0, dX_l1,
+ * dX_l2, X_l1/sin, X_l2/sin.  ct, st are cos and sin of delta. */
+int ysg_legendre_table(ysg_handle *h, int nr, int lmax, const double *delta, const double *ct,
+                       const double *st, double *table);
+
+/* Select the solve kernel: 0 = plain (one thread per (omega,l) pair, one
+ * event per launch), 1 = batched persistent (default). */
+int ysg_set_solver(ysg_handle *h, int which);
+
+/* Device times in ms of the last event's stages, measured with CUDA events
+ * on the handle's stream: [0] Legendre table, [1] solves, [2] l-sum,
+ * [3] filter + inverse FFT + post-processing. */
+int ysg_last_timings(ysg_handle *h, float ms[4]);
+
+/* Counters of the last solve stage: number of (omega,l) pairs and the
+ * algorithmic FP64 flop count of the stepping work actually performed. */
+int ysg_last_work(ysg_handle *h, double *pairs, double *flops);
+
+const char *ysg_status_string(int status);
+void ysg_destroy(ysg_handle *h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

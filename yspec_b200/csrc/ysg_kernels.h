@@ -1,0 +1,39 @@
+// ysg_kernels.h -- launchers of the device stages, used by the C-ABI layer.
+#pragma once
+#include <cuda_runtime.h>
+#include "ysg_model.cuh"
+
+namespace ysg {
+
+// K1 plain: one thread per (omega,l) pair of one event.
+size_t solve_plain_smem(int nknot);
+cudaError_t launch_solve_plain(const Knot* kn, const ModelHdr& mh, const EventDev& ev, cd* coef,
+                               unsigned long long* work, int* status, cudaStream_t st);
+
+// K1 batched persistent: work items of several events, warp-cooperative.
+struct BatchItem;
+cudaError_t launch_solve_batched(const Knot* kn, const ModelHdr& mh, const EventDev* evs_dev,
+                                 int nev, cd* const* coefs_dev, const int* items, int nitems,
+                                 int* counter, unsigned long long* work, int* status, int nblocks,
+                                 int warps_per_block, cudaStream_t st);
+
+// K2: Legendre table, T[((l * nr) + k) * 8 + q].
+cudaError_t launch_legendre(int nr, int lmax, const double* delta, const double* ct,
+                            const double* st, double* T, cudaStream_t s);
+
+// K3: receiver l-sum.  coef (nw, 15, L) complex; T as above; E (5, nr)
+// complex powers e^{i m azst}, m = -2..2; outputs (nw, nr) complex.
+cudaError_t launch_lsum(int nw, int nr, int lmin, int lmax, const cd* coef, const double* T,
+                        const cd* E, cd* ur, cd* ut, cd* up, cudaStream_t s);
+
+// K4: filter + Hermitian extension + inverse FFT + post-processing.
+struct TraceDev {
+    int nt, i1, i2, nw, nr, nout, log2n, b1;
+    double dt, scale, t_norm, amp_norm;
+};
+size_t ifft_scratch_bytes(int nt, int nr);
+cudaError_t launch_ifft(const TraceDev& td, const cd* ur, const cd* ut, const cd* up,
+                        const double* filt, const cd* tw, const double* expt,
+                        const double* cs_azep, cd* scratch, double* out, cudaStream_t s);
+
+}  // namespace ysg

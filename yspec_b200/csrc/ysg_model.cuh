@@ -1,0 +1,80 @@
+// ysg_model.cuh -- device layout of the earth model and event constants.
+//
+// The host (module_model.f90:175-383 restated in host/model.cpp) produces the
+// normalised knot values and the per-layer natural-spline second derivatives.
+// On the device each knot is one 256-byte record so that a spline evaluation
+// on knot interval i touches two adjacent records; the whole table (51 KB at
+// 200 knots, 102 KB at 400) is staged into shared memory by a TMA bulk copy.
+#pragma once
+#include "ysg_cplx.cuh"
+
+namespace ysg {
+
+// Parameter slots of a knot record (module_model.f90:129-160).
+enum Param {
+    P_RHO = 0, P_ACON, P_CCON, P_FCON, P_LCON, P_NCON, P_KAPPA, P_MU,
+    P_QKAPPA, P_QMU, P_GRAV, P_XLAM, P_XA2, NPARAM
+};
+
+struct Knot {
+    double r, alpha, beta, pad0;
+    double v[NPARAM][2];       // value, spline second derivative
+    double pad1[2];
+};
+static_assert(sizeof(Knot) == 256, "knot record must be 256 bytes");
+
+// Scalar part of the model.  Indices are 1-based as in the reference.
+struct ModelHdr {
+    int nknot, nic, noc, nsl, ocean, fic;
+    int imin_alpha;      // iminloc(alpha)            (module_int.f90:1157)
+    int imin_beta;       // iminloc(beta(noc+1:nsl))+noc (module_int.f90:200-201)
+    double tref;         // normalised reference angular frequency
+    double pibigg;       // module_model.f90:490
+    double fre_norm;     // module_model.f90:484
+    double pad;
+};
+
+// Per-event constants of the (omega,l) loop (yspec.f90:176-261).
+struct EventDev {
+    int lmin, lmax, nw, is, ir, ats, grav, out, cor, nr;
+    int pad0, pad1;
+    double rs, rr, ep, wmin, dw, grav_ir;
+    double mm[6];
+};
+
+// Number of l-sum coefficients per (omega,l): uu(1:5), vv(1:5), ww(1:5).
+constexpr int NCOEF = 15;
+
+// Knot-interval spline evaluator (module_spline.f90:262-283).  The interval
+// weights are formed once per radius and reused for every parameter.
+struct SplPt {
+    double A, B, A3, B3, h26;
+    int lo;
+    bool flat;
+};
+
+__device__ __forceinline__ SplPt spl_at(const Knot* kn, int klo, double x)
+{
+    SplPt s;
+    s.lo = klo;
+    double xa = kn[klo].r, xb = kn[klo + 1].r;
+    double h = xb - xa;
+    s.flat = (h == 0.0);
+    double ih = s.flat ? 0.0 : 1.0 / h;
+    s.A = (xb - x) * ih;
+    s.B = (x - xa) * ih;
+    s.A3 = s.A * s.A * s.A - s.A;
+    s.B3 = s.B * s.B * s.B - s.B;
+    s.h26 = h * h * (1.0 / 6.0);
+    return s;
+}
+
+__device__ __forceinline__ double spl(const Knot* kn, const SplPt& s, int p)
+{
+    const Knot& a = kn[s.lo];
+    if (s.flat) return a.v[p][0];
+    const Knot& b = kn[s.lo + 1];
+    return s.A * a.v[p][0] + s.B * b.v[p][0] + (s.A3 * a.v[p][1] + s.B3 * b.v[p][1]) * s.h26;
+}
+
+}  // namespace ysg

@@ -1,0 +1,870 @@
+// ysg_ode.cuh -- per-(omega,l) radial solves on the device.
+//
+// Device restatement of the reference's ODE machinery:
+//   module_int.f90    coefficient matrices, minor / b-vector systems, start
+//                     values, minor algebra, Cash-Karp stepping (yint/rkck),
+//                     per-solve constants (set_l/set_omega/steps)
+//   module_start.f90  start-level search
+//   module_solver.f90 the BVP drivers and source vectors
+// The reference keeps solve state in module globals; here it is a Ctx in
+// registers, so every thread can run an independent (omega,l) solve.
+//
+// Quantities that steer integer decisions (start level, step counts, grid
+// points of the l = 0 gravity solve) are formed with explicitly rounded
+// operations so they agree bit for bit with the reference's unfused FP64.
+#pragma once
+#include "ysg_model.cuh"
+
+namespace ysg {
+
+// nrtype.f90:18-27: pi_d and twopi_d are single-precision literals.
+constexpr double PI_D = (double)3.14159265358979323846f;
+constexpr double TWOPI_D = (double)6.28318530717958647692f;
+constexpr double FOURPI_D = 12.56637061;
+constexpr double SC_TINY = 1.0e-20;           // module_int.f90:80
+constexpr double SC_HUGE = 1.0 / 1.0e-20;     // module_int.f90:81
+constexpr int NW_STEP = 4;                    // module_int.f90:74
+constexpr double TOL_START = 11.0;            // module_start.f90:6
+
+// Step counters per system (index = Sys::CLS), for the algorithmic work
+// model: 0 toroidal, 1 radial, 2 fluid minors ng/cow, 3 b-vector ng/cow,
+// 4 solid minors ng/cow, 5 fluid minors g, 6 solid minors g, 7 b-vector g.
+constexpr int NSYS = 8;
+
+struct Ctx {
+    const Knot* kn;
+    const ModelHdr* mh;
+    int ll, llp1, il;
+    unsigned nst[NSYS];
+    double zeta, zeta2, zeta2m2, szeta2m2, nu, dr, ats;
+    cd omega, omega2, omegai, omegai2, lno;
+};
+
+// module_int.f90:2072-2089
+__device__ __forceinline__ void set_l(Ctx& c, int l)
+{
+    c.ll = l;
+    c.llp1 = l + 1;
+    c.zeta2 = (double)(float)(l * (l + 1));
+    c.zeta = sqrt(c.zeta2);
+    c.zeta2m2 = c.zeta2 - 2.0;
+    c.szeta2m2 = c.zeta2m2 > 0.0 ? sqrt(c.zeta2m2) : 0.0;
+    c.nu = sqrt((double)(float)(2 * l + 1) / FOURPI_D);
+}
+
+// module_int.f90:2091-2102
+__device__ __forceinline__ void set_omega(Ctx& c, cd w)
+{
+    c.omega = w;
+    c.omega2 = w * w;
+    c.omegai = 1.0 / w;
+    c.omegai2 = c.omegai * c.omegai;
+    cd z = imul(w) / c.mh->tref;
+    c.lno = c.ats * ((2.0 * clog(z)) / PI_D);
+}
+
+// module_int.f90:2121-2138
+__device__ __forceinline__ double steps(const Ctx& c, int i)
+{
+    const Knot* kn = c.kn;
+    double tmp = i < c.mh->nknot ? fmax(kn[i].alpha, kn[i + 1].alpha) : kn[i].alpha;
+    double s = __dmul_rn((double)NW_STEP, c.omega.x) / tmp;
+    return 1.0 / s;
+}
+
+// module_int.f90:1145-1166 sph_steps / :394-414 rad_steps
+__device__ __forceinline__ void alpha_steps(Ctx& c)
+{
+    double a = c.kn[c.mh->imin_alpha].alpha;
+    c.dr = (c.omega.x == 0.0) ? 1.0 / NW_STEP : 1.0 / (__dmul_rn((double)NW_STEP, c.omega.x) / a);
+}
+
+// ---------------------------------------------------------------------------
+// Coefficient matrices
+// ---------------------------------------------------------------------------
+
+// module_int.f90:134-164 tor_amat (t real, k and s complex)
+struct TorCoef { double t; cd k, s; };
+
+__device__ __forceinline__ TorCoef tor_amat(const Ctx& c, double rr)
+{
+    SplPt s = spl_at(c.kn, c.il, rr);
+    double rrho = spl(c.kn, s, P_RHO), rlcon = spl(c.kn, s, P_LCON);
+    double rncon = spl(c.kn, s, P_NCON), rqmu = spl(c.kn, s, P_QMU);
+    cd qll = 1.0 + rqmu * c.lno;
+    cd clcon = rlcon * qll, cncon = rncon * qll;
+    double ri = 1.0 / rr;
+    TorCoef a;
+    a.t = 2.0 * ri;
+    a.k = 1.0 / clcon;
+    a.s = -(c.omega2 * rrho) + (ri * ri * c.zeta2m2) * cncon;
+    return a;
+}
+
+// module_int.f90:261-304 rad_amat.  rad_derivs_ng also calls this gravity
+// form (module_int.f90:388), so both radial systems share it.
+struct RadCoef { cd t, k, s; };
+
+__device__ __forceinline__ RadCoef rad_amat(const Ctx& c, double rr)
+{
+    SplPt s = spl_at(c.kn, c.il, rr);
+    const Knot* kn = c.kn;
+    double rrho = spl(kn, s, P_RHO), racon = spl(kn, s, P_ACON), rccon = spl(kn, s, P_CCON);
+    double rfcon = spl(kn, s, P_FCON), rncon = spl(kn, s, P_NCON), gg = spl(kn, s, P_GRAV);
+    double rqmu = spl(kn, s, P_QMU), rxlam = spl(kn, s, P_XLAM), rxa2 = spl(kn, s, P_XA2);
+    cd qaa = 1.0 + rxa2 * c.lno, qff = 1.0 + rxlam * c.lno, qll = 1.0 + rqmu * c.lno;
+    cd cacon = racon * qaa, cfcon = rfcon * qff, cncon = rncon * qll;
+    cd cccon = 1.0 / (rccon * qaa);
+    cd gamma = cacon - cncon - cfcon * cfcon * cccon;
+    double ri = 1.0 / rr;
+    RadCoef a;
+    a.t = (1.0 - 2.0 * cfcon * cccon) * ri;
+    a.k = cccon;
+    a.s = -(c.omega2 * rrho) + (4.0 * (gamma - rrho * gg * rr)) * (ri * ri);
+    return a;
+}
+
+// Spheroidal coefficients.  KIND: 2 = self-gravitation
+// (module_int.f90:500-560 / 676-715), 1 = Cowling (:619-672 / :751-786),
+// 0 = no gravity (:564-616 / :720-747).  Entries that are real in value
+// are kept real.
+struct SolidCoef {
+    cd t11, t12, k11, k22, s11, s12, s22;
+    double t21, t22, t31, t33, k33, s13, s23;
+};
+
+template <int KIND>
+__device__ __forceinline__ SolidCoef solid_amat(const Ctx& c, double rr)
+{
+    SplPt s = spl_at(c.kn, c.il, rr);
+    const Knot* kn = c.kn;
+    double rrho = spl(kn, s, P_RHO), racon = spl(kn, s, P_ACON), rccon = spl(kn, s, P_CCON);
+    double rfcon = spl(kn, s, P_FCON), rncon = spl(kn, s, P_NCON), rlcon = spl(kn, s, P_LCON);
+    double rqmu = spl(kn, s, P_QMU), rxlam = spl(kn, s, P_XLAM), rxa2 = spl(kn, s, P_XA2);
+    cd qaa = 1.0 + rxa2 * c.lno, qff = 1.0 + rxlam * c.lno, qll = 1.0 + rqmu * c.lno;
+    cd cacon = racon * qaa, cfcon = rfcon * qff, cncon = rncon * qll, clcon = rlcon * qll;
+    cd cccon = 1.0 / (rccon * qaa);
+    cd fc = cfcon * cccon;
+    cd gamma = cacon - cncon - cfcon * fc;
+    double ri = 1.0 / rr, ri2 = ri * ri;
+    SolidCoef a;
+    a.t11 = (1.0 - 2.0 * fc) * ri;
+    a.t12 = (c.zeta * ri) * fc;
+    a.t21 = -(c.zeta * ri);
+    a.t22 = 2.0 * ri;
+    a.k11 = cccon;
+    a.k22 = 1.0 / clcon;
+    cd mw2r = -(c.omega2 * rrho);
+    a.s22 = mw2r + (c.zeta2 * (gamma + cncon) - 2.0 * cncon) * ri2;
+    if (KIND == 0) {
+        a.s11 = mw2r + (4.0 * gamma) * ri2;
+        a.s12 = (-2.0 * c.zeta) * gamma * ri2;
+    } else {
+        double gg = spl(kn, s, P_GRAV);
+        double rgr = rrho * gg * rr;
+        a.s11 = mw2r + (4.0 * (gamma - rgr)) * ri2;
+        a.s12 = (c.zeta * (rgr - 2.0 * gamma)) * ri2;
+    }
+    if (KIND == 2) {
+        double pib = c.mh->pibigg;
+        a.t31 = -(4.0 * pib * rrho);
+        a.t33 = -((double)c.ll * ri);
+        a.k33 = 4.0 * pib;
+        a.s13 = -(rrho * (double)c.llp1 * ri);
+        a.s23 = rrho * c.zeta * ri;
+    } else {
+        a.t31 = a.t33 = a.k33 = a.s13 = a.s23 = 0.0;
+    }
+    return a;
+}
+
+struct FluidCoef {
+    cd t11, t12, k11, s11, s12, s22;
+    double t21, t22, k22;
+};
+
+template <int KIND>
+__device__ __forceinline__ FluidCoef fluid_amat(const Ctx& c, double rr)
+{
+    SplPt s = spl_at(c.kn, c.il, rr);
+    const Knot* kn = c.kn;
+    double rrho = spl(kn, s, P_RHO), rccon = spl(kn, s, P_CCON), rxa2 = spl(kn, s, P_XA2);
+    cd qaa = 1.0 + rxa2 * c.lno;
+    cd cccon = 1.0 / (rccon * qaa);
+    double ri = 1.0 / rr;
+    FluidCoef a;
+    a.k11 = cccon - ((c.zeta2 * c.omegai2) * (ri * ri)) / rrho;
+    if (KIND == 0) {
+        a.t11 = mk(-ri);
+        a.s11 = -(c.omega2 * rrho);
+        a.t12 = a.s12 = a.s22 = mk(0.0);
+        a.t21 = a.t22 = a.k22 = 0.0;
+        return a;
+    }
+    double gg = spl(kn, s, P_GRAV);
+    cd gzw = (gg * c.zeta2) * c.omegai2;
+    a.t11 = (gzw * ri - 1.0) * ri;
+    a.s11 = -(c.omega2 * rrho) + (rrho * gg) * ((gzw * ri - 4.0) * ri);
+    if (KIND == 2) {
+        double pib = c.mh->pibigg;
+        a.t12 = (c.zeta2 * c.omegai2) * (ri * ri);
+        a.t21 = -4.0 * pib * rrho;
+        a.t22 = -((double)c.ll * ri);
+        a.k22 = 4.0 * pib;
+        a.s12 = rrho * ((gzw * ri - (double)c.llp1) * ri);
+        a.s22 = (rrho * c.zeta2 * ri * ri) * c.omegai2;
+    } else {
+        a.t12 = a.s12 = a.s22 = mk(0.0);
+        a.t21 = a.t22 = a.k22 = 0.0;
+    }
+    return a;
+}
+
+// ---------------------------------------------------------------------------
+// Right-hand sides.  Each system is a tag type with N components and f().
+// ---------------------------------------------------------------------------
+struct TorSys {
+    static constexpr int N = 2, CLS = 0;
+    __device__ static __forceinline__ void f(const Ctx& c, double r, const cd* y, cd* d)
+    {
+        TorCoef a = tor_amat(c, r);       // module_int.f90:168-184
+        d[0] = a.t * y[0] + a.k * y[1];
+        d[1] = a.s * y[0] - a.t * y[1];
+    }
+};
+
+struct RadSys {
+    static constexpr int N = 2, CLS = 1;
+    __device__ static __forceinline__ void f(const Ctx& c, double r, const cd* y, cd* d)
+    {
+        RadCoef a = rad_amat(c, r);       // module_int.f90:357-392
+        d[0] = a.t * y[0] + a.k * y[1];
+        d[1] = a.s * y[0] - a.t * y[1];
+    }
+};
+
+// module_int.f90:818-871 sph_minors_solid_derivs
+struct MinorSolidG {
+    static constexpr int N = 14, CLS = 6;
+    __device__ static __forceinline__ void f(const Ctx& c, double r, const cd* m, cd* d)
+    {
+        SolidCoef a = solid_amat<2>(c, r);
+        cd a123 = a.t11 + (a.t22 + a.t33), a126 = a.t11 + (a.t22 - a.t33);
+        cd a135 = a.t11 - (a.t22 - a.t33), a234 = (a.t22 + a.t33) - a.t11;
+        d[0] = a.k33 * m[3] - a.k22 * m[5] + a.k11 * m[9] + m[0] * a123;
+        d[1] = -(a.k22 * m[6]) + m[0] * a.s13 - m[2] * a.t21 + m[1] * a.t22 - m[3] * a.t31;
+        d[2] = -(a.k11 * m[10]) + m[0] * a.s23 + m[2] * a.t11 - m[1] * a.t12;
+        d[3] = a.k22 * m[8] - a.k11 * m[11] + m[3] * a126;
+        d[4] = -(a.k33 * m[7]) - m[0] * a.s12 + m[9] * a.t12 - m[5] * a.t21 + m[2] * a.t31 +
+               m[4] * a.t33;
+        d[5] = -(a.k33 * m[8]) - a.k11 * m[12] - m[0] * a.s22 - 2.0 * (m[4] * a.t12) +
+               m[5] * a135;
+        d[6] = m[2] * a.s12 + m[5] * a.s13 - m[1] * a.s22 - m[4] * a.s23 + m[10] * a.t12 -
+               m[6] * a.t22 + m[8] * a.t31;
+        d[7] = m[3] * a.s12 - m[2] * a.s13 - m[1] * a.s23 + m[11] * a.t12 - m[8] * a.t21 -
+               m[7] * a.t33;
+        d[8] = a.k11 * m[13] + m[3] * a.s22 - 2.0 * (m[2] * a.s23) - 2.0 * (m[7] * a.t12) -
+               m[8] * a234;
+        d[9] = -(a.k33 * m[11]) + a.k22 * m[12] + m[0] * a.s11 + 2.0 * (m[4] * a.t21) -
+               2.0 * (m[1] * a.t31) + m[9] * a234;
+        d[10] = -(m[2] * a.s11) + m[1] * a.s12 - m[4] * a.s13 - m[9] * a.s23 -
+                m[10] * a.t11 + m[6] * a.t21 - m[7] * a.t31;
+        d[11] = -(a.k22 * m[13]) - m[3] * a.s11 + 2.0 * (m[1] * a.s13) +
+                2.0 * (m[7] * a.t21) - m[11] * a135;
+        d[12] = a.k33 * m[13] - m[5] * a.s11 + 2.0 * (m[4] * a.s12) + m[9] * a.s22 +
+                2.0 * (m[6] * a.t31) - m[12] * a126;
+        d[13] = m[8] * a.s11 - 2.0 * (m[7] * a.s12) + 2.0 * (m[6] * a.s13) - m[11] * a.s22 +
+                2.0 * (m[10] * a.s23) - m[13] * a123;
+    }
+};
+
+// module_int.f90:874-936 sph_minors_solid_derivs_ng / _cow
+template <int KIND>
+struct MinorSolidNC {
+    static constexpr int N = 5, CLS = 4;
+    __device__ static __forceinline__ void f(const Ctx& c, double r, const cd* m, cd* d)
+    {
+        SolidCoef a = solid_amat<KIND>(c, r);
+        cd a11 = a.t11 + a.t22, a22 = a.t11 - a.t22;
+        d[0] = a11 * m[0] + a.k22 * m[2] - a.k11 * m[3];
+        d[1] = a.s12 * m[0] - a.t21 * m[2] + a.t12 * m[3];
+        d[2] = a.s22 * m[0] - 2.0 * (a.t12 * m[1]) + a22 * m[2] + a.k11 * m[4];
+        d[3] = -(a.s11 * m[0]) + (2.0 * a.t21) * m[1] - a22 * m[3] - a.k22 * m[4];
+        d[4] = -2.0 * (a.s12 * m[1]) + a.s11 * m[2] - a.s22 * m[3] - a11 * m[4];
+    }
+};
+
+// module_int.f90:941-967 sph_minors_fluid_derivs
+struct MinorFluidG {
+    static constexpr int N = 5, CLS = 5;
+    __device__ static __forceinline__ void f(const Ctx& c, double r, const cd* m, cd* d)
+    {
+        FluidCoef a = fluid_amat<2>(c, r);
+        cd tp = a.t11 + a.t22, tm = a.t11 - a.t22;
+        d[0] = a.k22 * m[2] - a.k11 * m[3] + m[0] * tp;
+        d[1] = m[0] * a.s12 + m[3] * a.t12 - m[2] * a.t21;
+        d[2] = a.k11 * m[4] + m[0] * a.s22 - 2.0 * (m[1] * a.t12) + m[2] * tm;
+        d[3] = -(a.k22 * m[4]) - m[0] * a.s11 + (2.0 * a.t21) * m[1] - m[3] * tm;
+        d[4] = m[2] * a.s11 - 2.0 * (m[1] * a.s12) - m[3] * a.s22 - m[4] * tp;
+    }
+};
+
+// module_int.f90:971-1012 sph_minors_fluid_derivs_ng / _cow
+template <int KIND>
+struct MinorFluidNC {
+    static constexpr int N = 2, CLS = 2;
+    __device__ static __forceinline__ void f(const Ctx& c, double r, const cd* m, cd* d)
+    {
+        FluidCoef a = fluid_amat<KIND>(c, r);
+        d[0] = a.t11 * m[0] + a.k11 * m[1];
+        d[1] = a.s11 * m[0] - a.t11 * m[1];
+    }
+};
+
+// module_int.f90:1016-1057 sph_bvec_solid_derivs
+struct BvecSolidG {
+    static constexpr int N = 14, CLS = 7;
+    __device__ static __forceinline__ void f(const Ctx& c, double r, const cd* b, cd* d)
+    {
+        SolidCoef a = solid_amat<2>(c, r);
+        const cd t11 = a.t11, t12 = a.t12, k11 = a.k11, k22 = a.k22;
+        const cd s11 = a.s11, s12 = a.s12, s22 = a.s22;
+        const double t21 = a.t21, t22 = a.t22, t31 = a.t31, t33 = a.t33, k33 = a.k33;
+        const double s13 = a.s13, s23 = a.s23;
+        d[0] = s11 * b[6] + s12 * (b[7] - b[2]) + s13 * b[8] - s22 * b[3] - s23 * b[4] -
+               (t11 + t22) * b[0] + t31 * b[5];
+        d[1] = s11 * b[9] + s12 * b[10] - s13 * (2.0 * b[2] + b[7]) - s23 * b[3] -
+               t21 * b[5] - (t11 + t33) * b[1];
+        d[2] = s12 * b[11] + s13 * b[12] + t12 * b[3] - t21 * b[6] - t31 * b[9];
+        d[3] = -(k22 * b[0]) - s11 * b[11] + s13 * b[13] + t21 * (b[2] - b[7]) +
+               (t22 - t11) * b[3] - t31 * b[10];
+        d[4] = -(k33 * b[1]) - s11 * b[12] - s12 * b[13] - t21 * b[8] +
+               t31 * (2.0 * b[2] + b[7]) + (t33 - t11) * b[4];
+        d[5] = s12 * b[9] - s13 * b[6] + s22 * b[10] - s23 * (b[2] + 2.0 * b[7]) -
+               t12 * b[1] - (t22 + t33) * b[5];
+        d[6] = k11 * b[0] + s22 * b[11] + s23 * b[12] - t12 * (b[2] - b[7]) + (t11 - t22) * b[6];
+        d[7] = -(s12 * b[11]) + s23 * b[13] - t12 * b[3] + t21 * b[6];
+        d[8] = -(k33 * b[5]) - s12 * b[12] - s22 * b[13] - t12 * b[4] - t22 * b[8] +
+               t31 * b[6] + t33 * b[8];
+        d[9] = k11 * b[1] + s23 * b[11] + t12 * b[10] + (t11 - t33) * b[9];
+        d[10] = k22 * b[5] - s13 * b[11] + t21 * b[9] + (t22 - t33) * b[10];
+        d[11] = -(k11 * b[3]) + k22 * b[6] + (t11 + t22) * b[11];
+        d[12] = -(k11 * b[4]) + k33 * b[9] + t12 * b[13] + (t11 + t33) * b[12];
+        d[13] = -(k22 * b[8]) + k33 * b[10] + t21 * b[12] - t31 * b[11] + (t22 + t33) * b[13];
+    }
+};
+
+// module_int.f90:1060-1110 sph_bvec_solid_derivs_ng / _cow
+template <int KIND>
+struct BvecSolidNC {
+    static constexpr int N = 4, CLS = 3;
+    __device__ static __forceinline__ void f(const Ctx& c, double r, const cd* b, cd* d)
+    {
+        SolidCoef a = solid_amat<KIND>(c, r);
+        d[0] = -(a.s11 * b[2]) - a.s12 * b[3] - a.t11 * b[0] - a.t21 * b[1];
+        d[1] = -(a.s12 * b[2]) - a.s22 * b[3] - a.t12 * b[0] - a.t22 * b[1];
+        d[2] = -(a.k11 * b[0]) + a.t11 * b[2] + a.t12 * b[3];
+        d[3] = -(a.k22 * b[1]) + a.t21 * b[2] + a.t22 * b[3];
+    }
+};
+
+// ---------------------------------------------------------------------------
+// Cash-Karp RK5 (module_int.f90:2016-2064), fifth-order solution only, with
+// the 1e+-20 rescaling of yint (module_int.f90:1910-1919).
+// ---------------------------------------------------------------------------
+template <class Sys>
+__device__ __forceinline__ void rkck_step(const Ctx& c, cd* y, double x, double h)
+{
+    constexpr int N = Sys::N;
+    constexpr double a2 = 0.2, a3 = 0.3, a4 = 0.6, a5 = 1.0, a6 = 0.875;
+    constexpr double b21 = 0.2, b31 = 3.0 / 40.0, b32 = 9.0 / 40.0;
+    constexpr double b41 = 0.3, b42 = -0.9, b43 = 1.2;
+    constexpr double b51 = -11.0 / 54.0, b52 = 2.5, b53 = -70.0 / 27.0, b54 = 35.0 / 27.0;
+    constexpr double b61 = 1631.0 / 55296.0, b62 = 175.0 / 512.0, b63 = 575.0 / 13824.0,
+                     b64 = 44275.0 / 110592.0, b65 = 253.0 / 4096.0;
+    constexpr double c1 = 37.0 / 378.0, c3 = 250.0 / 621.0, c4 = 125.0 / 594.0,
+                     c6 = 512.0 / 1771.0;
+    cd k1[N], k2[N], k3[N], k4[N], k5[N], yt[N];
+    Sys::f(c, x, y, k1);
+    const double hb21 = b21 * h;
+#pragma unroll
+    for (int i = 0; i < N; i++) yt[i] = y[i] + hb21 * k1[i];
+    Sys::f(c, x + a2 * h, yt, k2);
+#pragma unroll
+    for (int i = 0; i < N; i++) yt[i] = y[i] + h * (b31 * k1[i] + b32 * k2[i]);
+    Sys::f(c, x + a3 * h, yt, k3);
+#pragma unroll
+    for (int i = 0; i < N; i++) yt[i] = y[i] + h * (b41 * k1[i] + b42 * k2[i] + b43 * k3[i]);
+    Sys::f(c, x + a4 * h, yt, k4);
+#pragma unroll
+    for (int i = 0; i < N; i++)
+        yt[i] = y[i] + h * (b51 * k1[i] + b52 * k2[i] + b53 * k3[i] + b54 * k4[i]);
+    Sys::f(c, x + a5 * h, yt, k5);
+#pragma unroll
+    for (int i = 0; i < N; i++)
+        yt[i] = y[i] + h * (b61 * k1[i] + b62 * k2[i] + b63 * k3[i] + b64 * k4[i] + b65 * k5[i]);
+    Sys::f(c, x + a6 * h, yt, k2);   // k6 reuses k2's storage
+#pragma unroll
+    for (int i = 0; i < N; i++)
+        y[i] = y[i] + h * (c1 * k1[i] + c3 * k3[i] + c4 * k4[i] + c6 * k2[i]);
+}
+
+template <int N>
+__device__ __forceinline__ void rescale(cd* y, int* scale)
+{
+    bool all_small = true, any_big = false;
+#pragma unroll
+    for (int k = 0; k < N; k++) all_small = all_small && (cabs(y[k]) < SC_TINY);
+    if (all_small) {
+        (*scale)++;
+#pragma unroll
+        for (int k = 0; k < N; k++) y[k] = y[k] * SC_HUGE;
+    }
+#pragma unroll
+    for (int k = 0; k < N; k++) any_big = any_big || (cabs(y[k]) > SC_HUGE);
+    if (any_big) {
+        (*scale)--;
+#pragma unroll
+        for (int k = 0; k < N; k++) y[k] = y[k] * SC_TINY;
+    }
+}
+
+// module_int.f90:1847-1968 yint
+template <class Sys>
+__device__ void yint(Ctx& c, int i1, int i2, double r1, double r2, cd* y, int* scale)
+{
+    if (r2 == r1) return;
+    const bool up = r2 > r1;
+    const Knot* kn = c.kn;
+    const int di = up ? 1 : -1;
+    for (int i = i1; up ? (i <= i2) : (i >= i2); i += di) {
+        double rr1, rr2;
+        if (up) {
+            rr1 = (i == i1) ? r1 : kn[i].r;
+            rr2 = (i == i2) ? r2 : kn[i + 1].r;
+        } else {
+            rr1 = (i == i1) ? r1 : kn[i + 1].r;
+            rr2 = (i == i2) ? r2 : kn[i].r;
+        }
+        if (rr1 == rr2) continue;
+        c.il = i;
+        double drr = steps(c, i);
+        const double nf = floor(fabs(rr2 - rr1) / drr);
+        // nf is finite and small for omega > 0; the cap only bounds the loop
+        int n = 2 + (int)fmin(nf, 4194304.0);
+        drr = (rr2 - rr1) / (double)(n - 1);
+        c.nst[Sys::CLS] += (unsigned)(n - 1);
+        for (int j = 1; j <= n - 1; j++) {
+            double rr = __dadd_rn(rr1, __dmul_rn((double)(j - 1), drr));
+            rkck_step<Sys>(c, y, rr, drr);
+            if (scale) rescale<Sys::N>(y, scale);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Start levels, module_start.f90:14-178
+// ---------------------------------------------------------------------------
+__device__ inline int start_level(const Ctx& c, int l, double w, int i1, int i2, int wt)
+{
+    const Knot* kn = c.kn;
+    int isign = (i2 >= i1) ? 1 : -1;
+    double pp = (double)(float)(l * (l + 1)) / __dmul_rn(w, w);
+    int j = i2;
+    for (int i = i1; isign == 1 ? i <= i2 : i >= i2; i += isign) {
+        double v = wt == 1 ? kn[i].beta : kn[i].alpha;
+        double q1 = 1.0 / __dmul_rn(v, v) - pp / __dmul_rn(kn[i].r, kn[i].r);
+        if (isign == 1) {
+            if (q1 > 0.0) { j = max(i1, i - 1); break; }
+        } else {
+            if (q1 < 0.0) { j = i; break; }
+        }
+    }
+    int is = j;
+    int lo = min(i1, i2);
+    if (is == lo) return is;
+    int j1 = is;
+    is = lo;
+    double sum = 0.0;
+    for (int i = j1; i >= lo + 1; i--) {
+        double v1 = wt == 1 ? kn[i].beta : kn[i].alpha;
+        double v2 = wt == 1 ? kn[i - 1].beta : kn[i - 1].alpha;
+        double q1 = 1.0 / __dmul_rn(v1, v1) - pp / __dmul_rn(kn[i].r, kn[i].r);
+        double q2 = 1.0 / __dmul_rn(v2, v2) - pp / __dmul_rn(kn[i - 1].r, kn[i - 1].r);
+        if (q1 > 0.0 || q2 > 0.0) {
+            sum = 0.0;
+        } else {
+            q1 = sqrt(-q1);
+            q2 = sqrt(-q2);
+            double t = __dmul_rn(__dmul_rn(__dmul_rn(0.5, w), __dadd_rn(q1, q2)),
+                                 __dsub_rn(kn[i].r, kn[i - 1].r));
+            sum = __dadd_rn(sum, t);
+        }
+        if (sum > TOL_START) { is = i - 1; break; }
+    }
+    return is;
+}
+
+__device__ __forceinline__ int tor_start_level(const Ctx& c, int l, double w, int it)
+{
+    return start_level(c, l, w, c.mh->noc + 1, it, 1);
+}
+
+__device__ inline int sph_start_level(const Ctx& c, int l, double w, int it)
+{
+    const ModelHdr* mh = c.mh;
+    const double aw = -2.00e-3, bw = 2.25e-3, dw = 1.28e-3;
+    double wdim = __dmul_rn(w, mh->fre_norm);
+    double wsoc = __dadd_rn(aw, __dmul_rn(dw, (double)l));
+    int is;
+    if (wdim <= wsoc) {
+        is = start_level(c, l, w, mh->noc + 1, it, 1);
+        if (is == mh->nsl) is = is - 1;
+        if (is > mh->noc + 1) return is;
+    }
+    double wsic = __dadd_rn(aw, __dmul_rn(bw, (double)l));
+    if (wdim <= wsic) {
+        is = start_level(c, l, w, mh->nic + 1, mh->noc, 2);
+        if (is == mh->noc) is = is - 1;
+        if (is > mh->nic + 1) return is;
+    }
+    is = start_level(c, l, w, 2, mh->nic, mh->fic ? 2 : 1);
+    if (is == mh->nic) is = is - 1;
+    return is;
+}
+
+// ---------------------------------------------------------------------------
+// Start values
+// ---------------------------------------------------------------------------
+// module_function.f90:447-490: the ratio j_{l+1}/j_l is the stub x/(2l+3).
+__device__ __forceinline__ cd sbessj2(int l, cd x) { return x / (double)(float)(2 * l + 3); }
+
+// module_function.f90:520-581 bfs: Lentz continued fraction for
+// (r dj/dr)/j, or its power series when Re(x^2) <= 0.
+__device__ inline cd bfs(int l, cd xsq, double eps)
+{
+    if (xsq.x > 0.0) {
+        cd x = csqrt(xsq);
+        int lp1 = l + 1;
+        cd rx = 2.0 / x;
+        double nu = (double)lp1 - 0.5;
+        cd rj = nu * rx;
+        rx = -rx;
+        cd denom = (nu + 1.0) * rx;
+        cd numer = denom + 1.0 / rj;
+        rj = (rj * numer) / denom;
+        int nm1 = 1;
+        for (int it = 0; it < 100000; it++) {
+            nm1 = nm1 + 1;
+            rx = -rx;
+            cd a3 = (nu + (double)nm1) * rx;
+            denom = a3 + 1.0 / denom;
+            numer = a3 + 1.0 / numer;
+            cd ratio = numer / denom;
+            rj = rj * ratio;
+            if (fabs(cabs(ratio) - 1.0) <= eps) break;
+        }
+        return rj * x - (double)lp1;
+    }
+    cd f = mk(1.0), fp = mk((double)(float)l), a = mk(1.0);
+    double b = (double)(float)(l + l) + 1.0, cc = 2.0, d = (double)(float)l + 2.0;
+    for (int it = 0; it < 100000; it++) {
+        a = -(a * xsq) / (cc * (b + cc));
+        f = f + a;
+        fp = fp + a * d;
+        if (cabs(a * d) < eps) break;
+        cc = cc + 2.0;
+        d = d + 2.0;
+    }
+    return fp / f;
+}
+
+// module_function.f90:497-516 bfs_dum: the argument is sqrt(|x^2|).
+__device__ __forceinline__ cd bfs_dum(int l, cd xsq)
+{
+    cd fp = bfs(l, xsq, 1.e-9);
+    double x = sqrt(cabs(xsq));
+    return ((double)l - fp) / x;
+}
+
+// module_int.f90:213-250 tor_ystart
+__device__ inline void tor_ystart(const Ctx& c, int is, double rr, cd* y)
+{
+    SplPt s = spl_at(c.kn, is, rr);
+    double rrho = spl(c.kn, s, P_RHO), rmu = spl(c.kn, s, P_MU), rqmu = spl(c.kn, s, P_QMU);
+    cd cmu = rmu * (1.0 + rqmu * c.lno);
+    cd cbeta = csqrt(cmu / rrho);
+    cd arg = (c.omega / cbeta) * rr;
+    cd ratio = sbessj2(c.llp1, arg);
+    y[0] = mk(c.zeta * rr);
+    y[1] = c.zeta * (cmu * ((double)(c.ll - 1) - arg * ratio));
+}
+
+// module_int.f90:417-489 rad_ystart (GRAV) / rad_ystart_ng
+template <bool GRAV>
+__device__ inline void rad_ystart(const Ctx& c, int is, double rr, cd* y)
+{
+    SplPt s = spl_at(c.kn, is, rr);
+    const Knot* kn = c.kn;
+    double rrho = spl(kn, s, P_RHO), rmu = spl(kn, s, P_MU), rqmu = spl(kn, s, P_QMU);
+    double rkappa = spl(kn, s, P_KAPPA), rqkappa = spl(kn, s, P_QKAPPA);
+    cd cmu = rmu * (1.0 + rqmu * c.lno);
+    cd ckappa = rkappa * (1.0 + rqkappa * c.lno);
+    cd calpha = ckappa + (4.0 * cmu) / 3.0;
+    cd gamma = GRAV ? c.omega2 + (16.0 * c.mh->pibigg * rrho) / 3.0 : c.omega2;
+    gamma = (rrho * gamma) / calpha;
+    cd arg = gamma * rr;
+    cd ratio = sbessj2(1, arg);
+    y[0] = rr * ratio;
+    y[1] = (rr * calpha) * gamma - (4.0 * cmu) * ratio;
+}
+
+__device__ __forceinline__ cd det2(cd a1, cd a2, cd b1, cd b2) { return a1 * b2 - a2 * b1; }
+
+// module_int.f90:1192-1270 sph_solid_start followed by the 14 minors of
+// module_int.f90:1451-1485 (sph_minor_solid_start).
+__device__ inline void sph_minor_solid_start(const Ctx& c, int is, double rr, cd* m)
+{
+    SplPt s = spl_at(c.kn, is, rr);
+    const Knot* kn = c.kn;
+    double pib = c.mh->pibigg;
+    double rrho = spl(kn, s, P_RHO), rmu = spl(kn, s, P_MU), rqmu = spl(kn, s, P_QMU);
+    double rkappa = spl(kn, s, P_KAPPA), rqkappa = spl(kn, s, P_QKAPPA);
+    cd cmu = rmu * (1.0 + rqmu * c.lno);
+    cd ckappa = rkappa * (1.0 + rqkappa * c.lno);
+    cd calpha = (ckappa + 1.3333333333 * cmu) / rrho;
+    cd cbeta = cmu / rrho;
+    cd tmp1 = c.omega2 / cbeta;
+    cd tmp2 = (c.omega2 + (5.3333333 * pib) * rrho) / calpha;
+    double t3 = 2.666666666 * pib * c.zeta * rrho;
+    cd tmp3 = (t3 * t3) / (calpha * cbeta);
+    double ll = (double)c.ll, llp1 = (double)c.llp1;
+    cd y[6][3];
+    double sign = 1.0;
+    for (int i = 0; i < 2; i++) {
+        cd dd = tmp1 - tmp2;
+        cd gamma = dd * dd + tmp3;
+        gamma = 0.5 * (tmp1 + tmp2) + (0.5 * sign) * csqrt(gamma);
+        cd gamma2 = gamma;
+        gamma = csqrt(gamma);
+        cd zt = ((0.75 * cbeta) * (gamma2 - tmp1)) / (pib * rrho);
+        cd xi = zt - llp1;
+        cd args = (gamma2 * rr) * rr;
+        cd ratio = bfs_dum(c.ll, args);
+        cd grr = (gamma * rr) * ratio;
+        y[0][i] = ll * xi - zt * grr;
+        y[1][i] = c.zeta * (xi + grr);
+        y[2][i] = -(((4.0 * pib * rrho) * rr) * zt);
+        y[3][i] = -((((rrho * calpha) * zt) * rr) * gamma2) +
+                  (((2.0 * cmu) * ll) * (ll - 1.0)) * xi / rr +
+                  ((2.0 * cmu) * (2.0 * zt + c.zeta2)) * gamma * ratio;
+        cd y5 = rr * gamma2 + ((2.0 * (ll - 1.0)) * xi) / rr - ((2.0 * (zt + 1.0)) * gamma) * ratio;
+        y[4][i] = (cmu * c.zeta) * y5;
+        y[5][i] = -(rrho * (c.zeta2 + llp1 * zt));
+        sign = -sign;
+    }
+    y[0][2] = mk(ll);
+    y[1][2] = mk(c.zeta);
+    y[2][2] = (c.omega2 - (4.0 * pib * rrho * ll) / 3.0) * rr;
+    y[3][2] = ((2.0 * ll * (ll - 1.0)) * cmu) / rr;
+    y[4][2] = ((2.0 * c.zeta * (ll - 1.0)) * cmu) / rr;
+    y[5][2] = ((double)(2 * c.ll + 1) * c.omega2 - (8.0 * pib * ll * (ll - 1.0) * rrho) / 3.0);
+    y[5][2] = (0.25 * y[5][2]) / pib;
+    // index triples of module_int.f90:1468-1481 (1-based rows)
+    const unsigned char idx[14][3] = {{1, 2, 3}, {1, 2, 4}, {1, 2, 5}, {1, 2, 6}, {1, 3, 4},
+                                      {1, 3, 5}, {1, 4, 5}, {1, 4, 6}, {1, 5, 6}, {2, 3, 4},
+                                      {2, 4, 5}, {2, 4, 6}, {3, 4, 5}, {4, 5, 6}};
+#pragma unroll
+    for (int q = 0; q < 14; q++) {
+        int a = idx[q][0] - 1, b = idx[q][1] - 1, e = idx[q][2] - 1;
+        m[q] = y[a][0] * det2(y[b][1], y[e][1], y[b][2], y[e][2]) -
+               y[a][1] * det2(y[b][0], y[e][0], y[b][2], y[e][2]) +
+               y[a][2] * det2(y[b][0], y[e][0], y[b][1], y[e][1]);
+    }
+}
+
+__device__ __forceinline__ void minors_of_2col(const cd y[4][2], cd* m)
+{
+    m[0] = det2(y[0][0], y[1][0], y[0][1], y[1][1]);
+    m[1] = det2(y[0][0], y[2][0], y[0][1], y[2][1]);
+    m[2] = det2(y[0][0], y[3][0], y[0][1], y[3][1]);
+    m[3] = det2(y[1][0], y[2][0], y[1][1], y[2][1]);
+    m[4] = det2(y[2][0], y[3][0], y[2][1], y[3][1]);
+}
+
+// 32-bit wrap of the reference's default-integer products
+__device__ __forceinline__ int imul32(int a, int b) { return (int)((unsigned)a * (unsigned)b); }
+
+// module_int.f90:1275-1341 sph_solid_start_ng + :1489-1506 minors
+__device__ inline void sph_minor_solid_start_ng(const Ctx& c, int is, double rr, cd* m)
+{
+    SplPt s = spl_at(c.kn, is, rr);
+    const Knot* kn = c.kn;
+    double rrho = spl(kn, s, P_RHO), rmu = spl(kn, s, P_MU), rqmu = spl(kn, s, P_QMU);
+    double rkappa = spl(kn, s, P_KAPPA), rqkappa = spl(kn, s, P_QKAPPA);
+    cd cmu = rmu * (1.0 + rqmu * c.lno);
+    cd ckappa = rkappa * (1.0 + rqkappa * c.lno);
+    cd calpha = (ckappa + 1.3333333333 * cmu) / rrho;
+    cd cbeta = cmu / rrho;
+    int l = c.ll, lp1 = c.llp1;
+    double ll = (double)l;
+    cd y[4][2];
+    cd arg = (c.omega * rr) / csqrt(calpha);
+    cd jl2 = sbessj2(lp1, arg);
+    y[0][0] = ll - arg * jl2;
+    y[1][0] = mk(c.zeta);
+    y[2][0] = (-((((rrho * calpha) * arg) * arg)) +
+               (2.0 * cmu) * ((double)imul32(l, l - 1) + (2.0 * arg) * jl2)) / rr;
+    y[3][0] = (((2.0 * c.zeta) * cmu) * ((double)(l - 1) - arg * jl2)) / rr;
+    arg = (c.omega * rr) / csqrt(cbeta);
+    jl2 = sbessj2(lp1, arg);
+    y[0][1] = mk(-(double)imul32(l, lp1));
+    y[1][1] = -(c.zeta * (double)lp1) + arg * jl2;
+    y[2][1] = ((-2.0 * cmu) * ((double)imul32(l, imul32(l, l) - 1) -
+                               ((double)imul32(l, lp1) * arg) * jl2)) / rr;
+    y[3][1] = ((c.zeta * cmu) * (arg * arg - 2.0 * (double)(imul32(l, l) - 1) - (2.0 * arg) * jl2)) / rr;
+    minors_of_2col(y, m);
+}
+
+// module_int.f90:1346-1405 sph_fluid_start + :1509-1534 minors
+__device__ inline void sph_minor_fluid_start(const Ctx& c, int is, double rr, cd* m)
+{
+    SplPt s = spl_at(c.kn, is, rr);
+    const Knot* kn = c.kn;
+    double pib = c.mh->pibigg;
+    double rrho = spl(kn, s, P_RHO), rkappa = spl(kn, s, P_KAPPA), rqkappa = spl(kn, s, P_QKAPPA);
+    cd ckappa = rkappa * (1.0 + rqkappa * c.lno);
+    cd calpha = ckappa / rrho;
+    double gamg = (4.0 * pib * rrho) / 3.0;
+    cd gamma = ((c.omega2 + 4.0 * gamg) - ((c.zeta2 * gamg) * gamg) * c.omegai2) / calpha;
+    cd gamma2 = gamma;
+    gamma = csqrt(gamma);
+    cd zt = -c.omega2 / gamg;
+    cd xi = zt - (double)c.llp1;
+    cd args = (gamma2 * rr) * rr;
+    cd ratio = bfs_dum(c.ll, args);
+    double ll = (double)c.ll;
+    cd y[4][2];
+    y[0][0] = ll * xi - ((zt * gamma) * rr) * ratio;
+    y[1][0] = -(((4.0 * pib * rrho) * rr) * zt);
+    y[2][0] = -((((rrho * calpha) * zt) * rr) * gamma2);
+    y[3][0] = -(rrho * (c.zeta2 + (double)c.llp1 * zt));
+    y[0][1] = mk(ll);
+    y[1][1] = (c.omega2 - (4.0 * pib * rrho * ll) / 3.0) * rr;
+    y[2][1] = mk(0.0);
+    y[3][1] = ((double)(2 * c.ll + 1) * c.omega2 - (8.0 * pib * ll * (ll - 1.0) * rrho) / 3.0);
+    y[3][1] = (0.25 * y[3][1]) / pib;
+    minors_of_2col(y, m);
+}
+
+// module_int.f90:1407-1447 sph_fluid_start_ng (2 components)
+__device__ inline void sph_fluid_start_ng(const Ctx& c, int is, double rr, cd* y)
+{
+    SplPt s = spl_at(c.kn, is, rr);
+    const Knot* kn = c.kn;
+    double rrho = spl(kn, s, P_RHO), rkappa = spl(kn, s, P_KAPPA), rqkappa = spl(kn, s, P_QKAPPA);
+    cd ckappa = rkappa * (1.0 + rqkappa * c.lno);
+    cd calpha = ckappa / rrho;
+    cd arg = (c.omega * rr) / csqrt(calpha);
+    cd ratio = sbessj2(c.llp1, arg);
+    y[0] = (double)c.ll - arg * ratio;
+    y[1] = (-((rrho * calpha) * arg * arg)) / rr;
+}
+
+// ---------------------------------------------------------------------------
+// Minor algebra, module_int.f90:1563-1837 (1-based names M(k), S(k), B(k))
+// ---------------------------------------------------------------------------
+#define YM(k) m[(k) - 1]
+#define YS(k) s[(k) - 1]
+#define YB(k) b[(k) - 1]
+
+__device__ __forceinline__ void b_solid_start(const cd* m, const cd* s, cd* b)
+{
+    b[0] = YM(14) * YS(3) - YM(7) * YS(4) - YM(11) * YS(5) - YM(13) * YS(6);
+    b[1] = -(YM(14) * YS(2)) - YM(8) * YS(4) - YM(12) * YS(5) + YM(11) * YS(6);
+    b[2] = YM(7) * YS(2) + YM(8) * YS(3) + YM(2) * YS(5) + YM(5) * YS(6);
+    b[3] = YM(11) * YS(2) + YM(12) * YS(3) - YM(2) * YS(4) + YM(10) * YS(6);
+    b[4] = YM(13) * YS(2) - YM(11) * YS(3) - YM(5) * YS(4) - YM(10) * YS(5);
+    b[5] = YM(14) * YS(1) - YM(9) * YS(4) + YM(8) * YS(5) - YM(7) * YS(6);
+    b[6] = -(YM(7) * YS(1)) + YM(9) * YS(3) + YM(3) * YS(5) + YM(6) * YS(6);
+    b[7] = -(YM(11) * YS(1)) - YM(8) * YS(3) - YM(3) * YS(4) - YM(5) * YS(6);
+    b[8] = -(YM(13) * YS(1)) + YM(7) * YS(3) - YM(6) * YS(4) + YM(5) * YS(5);
+    b[9] = -(YM(8) * YS(1)) - YM(9) * YS(2) + YM(4) * YS(5) - YM(3) * YS(6);
+    b[10] = -(YM(12) * YS(1)) + YM(8) * YS(2) - YM(4) * YS(4) + YM(2) * YS(6);
+    b[11] = YM(2) * YS(1) + YM(3) * YS(2) + YM(4) * YS(3) - YM(1) * YS(6);
+    b[12] = YM(5) * YS(1) + YM(6) * YS(2) - YM(3) * YS(3) + YM(1) * YS(5);
+    b[13] = YM(10) * YS(1) - YM(5) * YS(2) + YM(2) * YS(3) - YM(1) * YS(4);
+}
+
+__device__ __forceinline__ void b_solid_start_ngcow(const cd* m, const cd* s, cd* b)
+{
+    b[0] = -(YM(5) * YS(2)) - YM(2) * YS(3) - YM(4) * YS(4);
+    b[1] = YM(5) * YS(1) - YM(3) * YS(3) + YM(2) * YS(4);
+    b[2] = YM(2) * YS(1) + YM(3) * YS(2) - YM(1) * YS(4);
+    b[3] = YM(4) * YS(1) - YM(2) * YS(2) + YM(1) * YS(3);
+}
+
+__device__ __forceinline__ void s2f(const cd* m1, cd* m2)
+{
+    m2[0] = -m1[5]; m2[1] = -m1[6]; m2[2] = m1[8]; m2[3] = -m1[12]; m2[4] = m1[13];
+}
+__device__ __forceinline__ void s2f_ngcow(const cd* m1, cd* m2) { m2[0] = -m1[2]; m2[1] = -m1[4]; }
+__device__ __forceinline__ void f2s(const cd* m1, cd* m2)
+{
+#pragma unroll
+    for (int k = 0; k < 14; k++) m2[k] = mk(0.0);
+    m2[0] = m1[0]; m2[1] = m1[1]; m2[3] = m1[2]; m2[9] = -m1[3]; m2[11] = -m1[4];
+}
+__device__ __forceinline__ void f2s_ngcow(const cd* m1, cd* m2)
+{
+#pragma unroll
+    for (int k = 0; k < 5; k++) m2[k] = mk(0.0);
+    m2[0] = m1[0];
+    m2[3] = -m1[1];
+}
+
+__device__ __forceinline__ cd delta_solid(const cd* a, const cd* b)
+{
+#define DA(k) a[(k) - 1]
+#define DB(k) b[(k) - 1]
+    return -(DA(14) * DB(1)) + 2.0 * (DA(7) * DB(2)) + 2.0 * (DA(11) * DB(3)) + DA(13) * DB(4) +
+           2.0 * (DA(8) * DB(5)) + DA(12) * DB(6) - 2.0 * (DA(2) * DB(7)) - 2.0 * (DA(5) * DB(8)) -
+           DA(10) * DB(9) + DA(9) * DB(10) - 2.0 * (DA(3) * DB(11)) - DA(6) * DB(12) -
+           DA(4) * DB(13) + DA(1) * DB(14);
+}
+__device__ __forceinline__ cd delta_solid_ngcow(const cd* a, const cd* b)
+{
+    return DA(5) * DB(1) + 2.0 * (DA(2) * DB(2)) + DA(4) * DB(3) + DA(3) * DB(4) + DA(1) * DB(5);
+#undef DA
+#undef DB
+}
+
+__device__ __forceinline__ void sph_ysol(const cd* m, const cd* b, cd* y)
+{
+    y[0] = YM(3) * YB(3) + YM(1) * YB(6) + YM(2) * YB(7) + 2.0 * (YM(3) * YB(8)) + YM(4) * YB(9) +
+           YM(5) * YB(10) + YM(6) * YB(11) + YM(7) * YB(12) + YM(8) * YB(13) + YM(9) * YB(14);
+    y[1] = -(YM(1) * YB(2)) - YM(2) * (2.0 * YB(3) + YB(8)) - YM(3) * YB(4) - YM(4) * YB(5) -
+           YM(5) * YB(11) - YM(8) * YB(14) + YM(10) * YB(10) + YM(11) * YB(12) + YM(12) * YB(13);
+    y[2] = YM(1) * YB(1) - YM(2) * YB(9) + YM(3) * YB(5) + YM(5) * (YB(8) - YB(3)) -
+           YM(6) * YB(4) + YM(7) * YB(14) - YM(10) * YB(7) - YM(11) * YB(13) + YM(13) * YB(12);
+    y[3] = YM(2) * YB(1) + YM(5) * YB(2) - YM(7) * YB(4) - YM(8) * YB(5) + YM(10) * YB(6) -
+           YM(11) * (YB(3) + 2.0 * YB(8)) - YM(12) * YB(9) - YM(13) * YB(11) + YM(14) * YB(14);
+    y[4] = YM(3) * YB(1) - YM(5) * YB(6) + YM(6) * YB(2) + YM(7) * (2.0 * YB(3) + YB(8)) +
+           YM(8) * YB(9) - YM(9) * YB(5) + YM(11) * YB(7) + YM(13) * YB(10) - YM(14) * YB(13);
+    y[5] = YM(2) * YB(6) - YM(3) * YB(2) + YM(4) * YB(1) + YM(7) * YB(11) +
+           YM(8) * (YB(3) - YB(8)) + YM(9) * YB(4) - YM(11) * YB(10) + YM(12) * YB(7) +
+           YM(14) * YB(12);
+}
+
+__device__ __forceinline__ void sph_ysol_ngcow(const cd* m, const cd* b, cd* y)
+{
+    y[0] = YM(1) * YB(2) + YM(2) * YB(3) + YM(3) * YB(4);
+    y[1] = -(YM(1) * YB(1)) + YM(4) * YB(3) - YM(2) * YB(4);
+    y[2] = -(YM(2) * YB(1)) - YM(4) * YB(2) + YM(5) * YB(4);
+    y[3] = -(YM(3) * YB(1)) + YM(2) * YB(2) - YM(5) * YB(3);
+}
+#undef YM
+#undef YS
+#undef YB
+
+}  // namespace ysg

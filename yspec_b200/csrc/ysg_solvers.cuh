@@ -1,0 +1,568 @@
+// ysg_solvers.cuh -- two-point boundary-value drivers and source vectors.
+//
+// Device restatement of module_solver.f90: tor_solver (:25-142),
+// rad_solver_ng (:335-441), rad_solver_wg (:446-561), the six sph_solver*
+// variants (:640-1740) and source_vector_{tor,rad,sph} (:145-215, :566-627,
+// :1747-1847), plus the per-(omega,l) epilogue of yspec.f90:263-400 (output
+// type scaling, potential/tilt correction, uu/vv/ww coefficients).
+#pragma once
+#include "ysg_ode.cuh"
+
+namespace ysg {
+
+__device__ __forceinline__ double huge_pow(int k)
+{
+    // huge**k for the integer exponents produced by the rescaling counters
+    return k == 0 ? 1.0 : pow(SC_HUGE, (double)k);
+}
+
+// module_solver.f90:25-142.  Unit source jumps ss = I (yspec.f90:230-232).
+__device__ inline void tor_solver(Ctx& c, double rr, double rs, int ir, int is, cd yout[2][2])
+{
+    const ModelHdr* mh = c.mh;
+    const Knot* kn = c.kn;
+    int scale1 = 0, scale2 = 0, scale3 = 0;
+    cd y1[2], y2[2], y3[2];
+    const bool up = rr >= rs;
+    int it = up ? is : ir;
+    int i1 = tor_start_level(c, c.ll, c.omega.x, it);
+    if (i1 == it && i1 > mh->noc + 1) i1 = i1 - 1;
+    double rt = kn[i1].r;
+    if (i1 == mh->noc + 1) { y1[0] = mk(1.0); y1[1] = mk(0.0); }
+    else tor_ystart(c, i1, rt, y1);
+    cd delta;
+    if (up) {
+        yint<TorSys>(c, i1, is, rt, rs, y1, &scale1);
+        y3[0] = y1[0]; y3[1] = y1[1];
+        if (rr != rs) yint<TorSys>(c, is, ir, rs, rr, y3, &scale3);
+        y2[0] = mk(1.0); y2[1] = mk(0.0);
+        if (rr != kn[mh->nsl].r) yint<TorSys>(c, mh->nsl - 1, ir, kn[mh->nsl].r, rr, y2, &scale2);
+        delta = 1.0 / (y2[1] * y3[0] - y2[0] * y3[1]);
+        // b = y1(2)*ss(1,i) - y1(1)*ss(2,i); yout(:,i) = -delta*y2*b
+        cd b0 = y1[1], b1 = -y1[0];
+        cd dy0 = delta * y2[0], dy1 = delta * y2[1];
+        yout[0][0] = -(dy0 * b0); yout[1][0] = -(dy1 * b0);
+        yout[0][1] = -(dy0 * b1); yout[1][1] = -(dy1 * b1);
+    } else {
+        yint<TorSys>(c, i1, ir, rt, rr, y1, &scale1);
+        y2[0] = mk(1.0); y2[1] = mk(0.0);
+        if (rs != kn[mh->nsl].r) yint<TorSys>(c, mh->nsl - 1, is, kn[mh->nsl].r, rs, y2, &scale2);
+        y3[0] = y2[0]; y3[1] = y2[1];
+        if (rr != rs) yint<TorSys>(c, is, ir, rs, rr, y3, &scale3);
+        delta = 1.0 / (y3[1] * y1[0] - y3[0] * y1[1]);
+        cd b0 = y2[1], b1 = -y2[0];
+        cd dy0 = delta * y1[0], dy1 = delta * y1[1];
+        yout[0][0] = -(dy0 * b0); yout[1][0] = -(dy1 * b0);
+        yout[0][1] = -(dy0 * b1); yout[1][1] = -(dy1 * b1);
+    }
+    if (scale3 != 0) {
+        double f = huge_pow(scale3);
+        for (int a = 0; a < 2; a++)
+            for (int b = 0; b < 2; b++) yout[a][b] = yout[a][b] * f;
+    }
+}
+
+// module_solver.f90:335-441 rad_solver_ng (rad_derivs_ng == gravity matrix)
+__device__ inline void rad_solver_ng(Ctx& c, double rr, double rs, int ir, int is, cd yout[2][2])
+{
+    const ModelHdr* mh = c.mh;
+    const Knot* kn = c.kn;
+    int scale1 = 0, scale2 = 0, scale3 = 0;
+    cd y1[2], y2[2], y3[2], delta;
+    double rt = fmin(0.1 * c.dr, 0.1 * kn[2].r);
+    rad_ystart<false>(c, 1, rt, y1);
+    const bool up = rr >= rs;
+    if (up) {
+        yint<RadSys>(c, 1, is, rt, rs, y1, &scale1);
+        y2[0] = mk(1.0); y2[1] = mk(0.0);
+        if (rr != kn[mh->nknot].r) yint<RadSys>(c, mh->nknot - 1, ir, kn[mh->nknot].r, rr, y2, &scale2);
+        y3[0] = y2[0]; y3[1] = y2[1];
+        if (rs != rr) yint<RadSys>(c, ir, is, rr, rs, y3, &scale3);
+    } else {
+        yint<RadSys>(c, 1, ir, rt, rr, y1, &scale1);
+        y2[0] = mk(1.0); y2[1] = mk(0.0);
+        if (rs != kn[mh->nsl].r) yint<RadSys>(c, mh->nsl - 1, is, kn[mh->nsl].r, rs, y2, &scale2);
+        y3[0] = y2[0]; y3[1] = y2[1];
+        if (rr != rs) yint<RadSys>(c, is, ir, rs, rr, y3, &scale3);
+    }
+    delta = y3[1] * y1[0] - y3[0] * y1[1];
+    delta = cabs(delta) < 1.0e-100 ? mk(0.0) : 1.0 / delta;
+    const cd* ya = up ? y1 : y2;   // source-side solution forming b
+    const cd* yb = up ? y2 : y1;   // solution evaluated at the receiver
+    cd b0 = ya[1], b1 = -ya[0];
+    cd dy0 = delta * yb[0], dy1 = delta * yb[1];
+    yout[0][0] = -(dy0 * b0); yout[1][0] = -(dy1 * b0);
+    yout[0][1] = -(dy0 * b1); yout[1][1] = -(dy1 * b1);
+    if (up) {
+        if (scale3 != 0) {
+            double f = huge_pow(scale3);
+            for (int a = 0; a < 2; a++)
+                for (int b = 0; b < 2; b++) yout[a][b] = yout[a][b] * f;
+        }
+    } else {
+        // module_solver.f90:433-437 only undoes positive scale3
+        for (int k = 0; k < scale3; k++)
+            for (int a = 0; a < 2; a++)
+                for (int b = 0; b < 2; b++) yout[a][b] = yout[a][b] * SC_HUGE;
+    }
+}
+
+// Grid of module_model.f90:578-787 (grid_count / make_grid), generated on
+// the fly.  visit(k, interval, r) sees 1-based grid index k in increasing
+// order; the reverse walk sees the same points from the top down.
+struct GridSeg { double a, b; int first; };
+
+__device__ __forceinline__ int grid_segs(double r1, double r2, double rs, double rr, GridSeg* sg,
+                                         int* src_after, int* rec_after)
+{
+    // returns number of segments; *_after = segment index after which the
+    // source / receiver point is the last point written (-1 if absent)
+    bool ls = (rs > r1 && rs <= r2), lr = (rr > r1 && rr <= r2);
+    *src_after = -1;
+    *rec_after = -1;
+    if (ls && lr) {
+        if (rs < rr) {
+            sg[0] = {r1, rs, 1}; sg[1] = {rs, rr, 2}; sg[2] = {rr, r2, 2};
+            *src_after = 0; *rec_after = 1; return 3;
+        } else if (rr < rs) {
+            sg[0] = {r1, rr, 1}; sg[1] = {rr, rs, 2}; sg[2] = {rs, r2, 2};
+            *rec_after = 0; *src_after = 1; return 3;
+        }
+        sg[0] = {r1, rs, 1}; sg[1] = {rs, r2, 2};
+        *src_after = 0; *rec_after = 0; return 2;
+    } else if (ls) {
+        sg[0] = {r1, rs, 1}; sg[1] = {rs, r2, 2};
+        *src_after = 0; return 2;
+    } else if (lr) {
+        sg[0] = {r1, rr, 1}; sg[1] = {rr, r2, 2};
+        *rec_after = 0; return 2;
+    }
+    sg[0] = {r1, r2, 1};
+    return 1;
+}
+
+__device__ __forceinline__ int seg_npts(const GridSeg& s, double drr)
+{
+    return (int)floor((s.b - s.a) / drr) + 2;
+}
+
+// module_solver.f90:446-561 rad_solver_wg.  The potential pout is not used
+// by the driver (yspec.f90:277-281) and is not formed.
+__device__ inline void rad_solver_wg(Ctx& c, double rr, double rs, cd yout[2][2])
+{
+    const ModelHdr* mh = c.mh;
+    const Knot* kn = c.kn;
+    const double drr = c.dr;
+    // pass 1: grid size and source / receiver indices
+    int ngrid = 0, iss = 0, irr = 0;
+    for (int i = 1; i <= mh->nknot - 1; i++) {
+        double r1 = kn[i].r, r2 = kn[i + 1].r;
+        if (r1 == r2) continue;
+        GridSeg sg[3];
+        int sa, ra;
+        int ns = grid_segs(r1, r2, rs, rr, sg, &sa, &ra);
+        for (int q = 0; q < ns; q++) {
+            ngrid += seg_npts(sg[q], drr) - (sg[q].first - 1);
+            if (q == sa) iss = ngrid;
+            if (q == ra) irr = ngrid;
+        }
+    }
+    // pass 2: upward from rt through grid points 2..iss
+    cd y1[2], yrec[2] = {mk(0.0), mk(0.0)};
+    bool have_rec = false;
+    {
+        int k = 0, iprev = 0;
+        double rprev = 0.0;
+        bool started = false;
+        for (int i = 1; i <= mh->nknot - 1 && k < iss; i++) {
+            double r1 = kn[i].r, r2 = kn[i + 1].r;
+            if (r1 == r2) continue;
+            GridSeg sg[3];
+            int sa, ra;
+            int ns = grid_segs(r1, r2, rs, rr, sg, &sa, &ra);
+            for (int q = 0; q < ns && k < iss; q++) {
+                int np = seg_npts(sg[q], drr);
+                double drt = (sg[q].b - sg[q].a) / (double)(np - 1);
+                for (int jj = sg[q].first; jj <= np && k < iss; jj++) {
+                    k++;
+                    double rk = __dadd_rn(sg[q].a, __dmul_rn((double)(jj - 1), drt));
+                    if (k == 2) {
+                        double rt = fmin(0.1 * drr, 0.1 * rk);
+                        rad_ystart<true>(c, 1, rt, y1);
+                        yint<RadSys>(c, 1, i, rt, rk, y1, nullptr);
+                        started = true;
+                    } else if (k > 2) {
+                        yint<RadSys>(c, iprev, i, rprev, rk, y1, nullptr);
+                    }
+                    if (started && k == irr) { yrec[0] = y1[0]; yrec[1] = y1[1]; have_rec = true; }
+                    iprev = i;
+                    rprev = rk;
+                }
+            }
+        }
+    }
+    // pass 3: downward from grid point ngrid to iss
+    cd y2[2] = {mk(1.0), mk(0.0)};
+    {
+        int k = ngrid + 1, iprev = 0;
+        double rprev = 0.0;
+        for (int i = mh->nknot - 1; i >= 1 && k > iss; i--) {
+            double r1 = kn[i].r, r2 = kn[i + 1].r;
+            if (r1 == r2) continue;
+            GridSeg sg[3];
+            int sa, ra;
+            int ns = grid_segs(r1, r2, rs, rr, sg, &sa, &ra);
+            for (int q = ns - 1; q >= 0 && k > iss; q--) {
+                int np = seg_npts(sg[q], drr);
+                double drt = (sg[q].b - sg[q].a) / (double)(np - 1);
+                for (int jj = np; jj >= sg[q].first && k > iss; jj--) {
+                    k--;
+                    double rk = __dadd_rn(sg[q].a, __dmul_rn((double)(jj - 1), drt));
+                    if (k < ngrid) yint<RadSys>(c, iprev, i, rprev, rk, y2, nullptr);
+                    if (k == irr && irr > iss) { yrec[0] = y2[0]; yrec[1] = y2[1]; have_rec = true; }
+                    iprev = i;
+                    rprev = rk;
+                }
+            }
+        }
+    }
+    (void)have_rec;
+    cd delta = 1.0 / (y2[1] * y1[0] - y2[0] * y1[1]);
+    cd b0, b1;
+    if (irr <= iss) { b0 = y2[1]; b1 = -y2[0]; }
+    else { b0 = y1[1]; b1 = -y1[0]; }
+    cd dy0 = delta * yrec[0], dy1 = delta * yrec[1];
+    yout[0][0] = -(dy0 * b0); yout[1][0] = -(dy1 * b0);
+    yout[0][1] = -(dy0 * b1); yout[1][1] = -(dy1 * b1);
+}
+
+// Spheroidal solve with self-gravitation: sph_solver (:640-823) and
+// sph_solver_fic (:1203-1382).  yout[6][4] holds the responses to unit
+// jumps in components 1, 2, 4, 5 (yspec.f90:234-238).
+__device__ inline void sph_solver_g(Ctx& c, double rr, double rs, int ir, int is, cd yout[6][4])
+{
+    const ModelHdr* mh = c.mh;
+    const Knot* kn = c.kn;
+    const bool fic = mh->fic != 0;
+    int scale1 = 0, scale2 = 0, scale3 = 0;
+    cd ms1[14], ms2[14], ms3[14], mf[5];
+    const bool up = rr >= rs;
+    const int it = up ? is : ir;
+    const double rtop = up ? rs : rr;
+    int i1 = sph_start_level(c, c.ll, c.omega.x, it);
+    double rt = kn[i1].r;
+    if (i1 == 1 && (up || fic)) rt = fmin(0.1 * c.dr, 0.1 * kn[2].r);
+    if (i1 >= it) { i1 = it - 1; rt = kn[i1].r; }
+    if (i1 <= mh->nic) {
+        if (fic && up) {
+            sph_minor_fluid_start(c, i1, rt, mf);
+            yint<MinorFluidG>(c, i1, mh->noc, rt, kn[mh->noc].r, mf, &scale1);
+        } else {
+            // the receiver-below-source branch of sph_solver_fic starts a
+            // solid minor inside the fluid inner core (:1323-1332), kept
+            sph_minor_solid_start(c, i1, rt, ms1);
+            yint<MinorSolidG>(c, i1, mh->nic, rt, kn[mh->nic].r, ms1, &scale1);
+            s2f(ms1, mf);
+            yint<MinorFluidG>(c, mh->nic + 1, mh->noc, kn[mh->nic].r, kn[mh->noc].r, mf, &scale1);
+        }
+        f2s(mf, ms1);
+        yint<MinorSolidG>(c, mh->noc + 1, it, kn[mh->noc + 1].r, rtop, ms1, &scale1);
+    } else if (i1 <= mh->noc) {
+        sph_minor_fluid_start(c, i1, rt, mf);
+        yint<MinorFluidG>(c, i1, mh->noc, rt, kn[mh->noc].r, mf, &scale1);
+        f2s(mf, ms1);
+        yint<MinorSolidG>(c, mh->noc + 1, it, kn[mh->noc + 1].r, rtop, ms1, &scale1);
+    } else if (i1 <= mh->nsl) {
+        sph_minor_solid_start(c, i1, rt, ms1);
+        yint<MinorSolidG>(c, i1, it, rt, rtop, ms1, &scale1);
+    }
+#pragma unroll
+    for (int k = 0; k < 14; k++) ms3[k] = ms1[k];
+    if (up) { if (rr > rs) yint<MinorSolidG>(c, is, ir, rs, rr, ms3, &scale3); }
+    else { if (rs > rr) yint<MinorSolidG>(c, ir, is, rr, rs, ms3, &scale3); }
+    const int ibot = up ? ir : is;
+    const double rbot = up ? rr : rs;
+    if (mh->ocean) {
+        cd mf2[5] = {mk(1.0), mk(0.0), mk(0.0), mk(0.0), mk(0.0)};
+        yint<MinorFluidG>(c, mh->nknot - 1, mh->nsl + 1, kn[mh->nknot].r, kn[mh->nsl + 1].r, mf2, &scale2);
+        f2s(mf2, ms2);
+        yint<MinorSolidG>(c, mh->nsl, ibot, kn[mh->nsl].r, rbot, ms2, &scale2);
+    } else {
+#pragma unroll
+        for (int k = 0; k < 14; k++) ms2[k] = mk(0.0);
+        ms2[0] = mk(1.0);
+        yint<MinorSolidG>(c, up ? mh->nknot - 1 : mh->nknot, ibot, kn[mh->nknot].r, rbot, ms2, &scale2);
+    }
+    cd delta = delta_solid(ms3, ms2);
+    const int jump[4] = {0, 1, 3, 4};
+    for (int i = 0; i < 4; i++) {
+        cd s[6] = {mk(0.0), mk(0.0), mk(0.0), mk(0.0), mk(0.0), mk(0.0)};
+        s[jump[i]] = mk(1.0);
+        int scale4 = 0;
+        cd b[14], ys[6];
+        if (up) {
+            b_solid_start(ms1, s, b);
+            yint<BvecSolidG>(c, is, ir, rs, rr, b, &scale4);
+            sph_ysol(ms2, b, ys);
+            for (int k = 0; k < 6; k++) ys[k] = (-ys[k]) / delta;
+        } else {
+            b_solid_start(ms2, s, b);
+            for (int k = 0; k < 14; k++) b[k] = (-b[k]) / delta;
+            yint<BvecSolidG>(c, is, ir, rs, rr, b, &scale4);
+            sph_ysol(ms1, b, ys);
+        }
+        double f = huge_pow(scale3 - scale4);
+        for (int k = 0; k < 6; k++) yout[k][i] = ys[k] * f;
+    }
+}
+
+// No gravity (KIND 0) / Cowling (KIND 1): sph_solver_ng (:827-1010),
+// sph_solver_cow (:1014-1195), sph_solver_ng_fic (:1386-1562),
+// sph_solver_cow_fic (:1568-1740).  yout[4][4], ss = I (yspec.f90:240-243).
+template <int KIND>
+__device__ inline void sph_solver_nc(Ctx& c, double rr, double rs, int ir, int is, cd yout[4][4])
+{
+    const ModelHdr* mh = c.mh;
+    const Knot* kn = c.kn;
+    const bool fic = mh->fic != 0;
+    int scale1 = 0, scale2 = 0, scale3 = 0;
+    cd ms1[5], ms2[5], ms3[5], mf[2];
+    const bool up = rr >= rs;
+    const int it = up ? is : ir;
+    const double rtop = up ? rs : rr;
+    int i1 = sph_start_level(c, c.ll, c.omega.x, it);
+    double rt = kn[i1].r;
+    if (i1 == 1 && (up || fic)) rt = fmin(0.1 * c.dr, 0.1 * kn[2].r);
+    if (i1 >= it) { i1 = it - 1; rt = kn[i1].r; }
+    if (i1 <= mh->nic) {
+        if (fic) {
+            sph_fluid_start_ng(c, i1, rt, mf);
+            yint<MinorFluidNC<KIND>>(c, i1, mh->noc, rt, kn[mh->noc].r, mf, &scale1);
+        } else {
+            sph_minor_solid_start_ng(c, i1, rt, ms1);
+            yint<MinorSolidNC<KIND>>(c, i1, mh->nic, rt, kn[mh->nic].r, ms1, &scale1);
+            s2f_ngcow(ms1, mf);
+            yint<MinorFluidNC<KIND>>(c, mh->nic + 1, mh->noc, kn[mh->nic].r, kn[mh->noc].r, mf, &scale1);
+        }
+        f2s_ngcow(mf, ms1);
+        yint<MinorSolidNC<KIND>>(c, mh->noc + 1, it, kn[mh->noc + 1].r, rtop, ms1, &scale1);
+    } else if (i1 <= mh->noc) {
+        sph_fluid_start_ng(c, i1, rt, mf);
+        yint<MinorFluidNC<KIND>>(c, i1, mh->noc, rt, kn[mh->noc].r, mf, &scale1);
+        f2s_ngcow(mf, ms1);
+        yint<MinorSolidNC<KIND>>(c, mh->noc + 1, it, kn[mh->noc + 1].r, rtop, ms1, &scale1);
+    } else if (i1 <= mh->nsl) {
+        sph_minor_solid_start_ng(c, i1, rt, ms1);
+        yint<MinorSolidNC<KIND>>(c, i1, it, rt, rtop, ms1, &scale1);
+    }
+#pragma unroll
+    for (int k = 0; k < 5; k++) ms3[k] = ms1[k];
+    if (up) { if (rr > rs) yint<MinorSolidNC<KIND>>(c, is, ir, rs, rr, ms3, &scale3); }
+    else { if (rs > rr) yint<MinorSolidNC<KIND>>(c, ir, is, rr, rs, ms3, &scale3); }
+    const int ibot = up ? ir : is;
+    const double rbot = up ? rr : rs;
+    if (mh->ocean) {
+        cd mf2[2] = {mk(1.0), mk(0.0)};
+        yint<MinorFluidNC<KIND>>(c, mh->nknot - 1, mh->nsl + 1, kn[mh->nknot].r, kn[mh->nsl + 1].r, mf2, &scale2);
+        f2s_ngcow(mf2, ms2);
+        yint<MinorSolidNC<KIND>>(c, mh->nsl, ibot, kn[mh->nsl].r, rbot, ms2, &scale2);
+    } else {
+#pragma unroll
+        for (int k = 0; k < 5; k++) ms2[k] = mk(0.0);
+        ms2[0] = mk(1.0);
+        yint<MinorSolidNC<KIND>>(c, mh->nknot, ibot, kn[mh->nknot].r, rbot, ms2, &scale2);
+    }
+    cd delta = delta_solid_ngcow(ms3, ms2);
+    for (int i = 0; i < 4; i++) {
+        cd s[4] = {mk(0.0), mk(0.0), mk(0.0), mk(0.0)};
+        s[i] = mk(1.0);
+        int scale4 = 0;
+        cd b[4], ys[4];
+        if (up) {
+            b_solid_start_ngcow(ms1, s, b);
+            yint<BvecSolidNC<KIND>>(c, is, ir, rs, rr, b, &scale4);
+            sph_ysol_ngcow(ms2, b, ys);
+            for (int k = 0; k < 4; k++) ys[k] = ys[k] / delta;
+        } else {
+            b_solid_start_ngcow(ms2, s, b);
+            for (int k = 0; k < 4; k++) b[k] = (-b[k]) / delta;
+            yint<BvecSolidNC<KIND>>(c, is, ir, rs, rr, b, &scale4);
+            sph_ysol_ngcow(ms1, b, ys);
+        }
+        double f = huge_pow(scale3 - scale4);
+        for (int k = 0; k < 4; k++) yout[k][i] = ys[k] * f;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Source vectors
+// ---------------------------------------------------------------------------
+// module_solver.f90:145-215 (svt(:,1) and svt(:,2))
+__device__ inline void source_vector_tor(const Ctx& c, int is, double rs, const double* mm,
+                                         cd svt[5][2])
+{
+    SplPt s = spl_at(c.kn, is, rs);
+    double rlcon = spl(c.kn, s, P_LCON), rqmu = spl(c.kn, s, P_QMU);
+    cd clcon = rlcon * (1.0 + rqmu * c.lno);
+    for (int i = 0; i < 5; i++) svt[i][0] = svt[i][1] = mk(0.0);
+    if (c.ll >= 1) {
+        svt[1][0] = ((0.5 * rs) * mk(-mm[2], mm[1])) / clcon;
+        svt[3][0] = ((0.5 * rs) * mk(mm[2], mm[1])) / clcon;
+    }
+    if (c.ll >= 2) {
+        svt[0][1] = (0.25 * c.szeta2m2) * mk(2.0 * mm[4], -mm[3] + mm[5]);
+        svt[4][1] = (0.25 * c.szeta2m2) * mk(2.0 * mm[4], mm[3] - mm[5]);
+    }
+    cd den = (imul(c.omega) * rs) * rs;
+    for (int i = 0; i < 5; i++) {
+        svt[i][0] = (c.nu * svt[i][0]) / den;
+        svt[i][1] = (c.nu * svt[i][1]) / den;
+    }
+}
+
+// module_solver.f90:566-627
+__device__ inline void source_vector_rad(const Ctx& c, int is, double rs, const double* mm, cd s0[2])
+{
+    SplPt s = spl_at(c.kn, is, rs);
+    double rccon = spl(c.kn, s, P_CCON), rfcon = spl(c.kn, s, P_FCON);
+    double rxa2 = spl(c.kn, s, P_XA2), rxlam = spl(c.kn, s, P_XLAM);
+    cd cccon = 1.0 / (rccon * (1.0 + rxa2 * c.lno));
+    cd cfcon = rfcon * (1.0 + rxlam * c.lno);
+    s0[0] = (rs * mm[0]) * cccon;
+    s0[1] = (-mm[3] - mm[5]) + ((2.0 * mm[0]) * cfcon) * cccon;
+    cd den = (imul(c.omega) * rs) * rs;
+    s0[0] = (c.nu * s0[0]) / den;
+    s0[1] = (c.nu * s0[1]) / den;
+}
+
+// module_solver.f90:1747-1847.  qaa, qff and qll are declared real(dp)
+// there (:1771-1772), so only Re(1 + q*lno) enters the spheroidal source.
+__device__ inline void source_vector_sph(const Ctx& c, int is, double rs, const double* mm,
+                                         cd svs[5][6])
+{
+    SplPt s = spl_at(c.kn, is, rs);
+    const Knot* kn = c.kn;
+    double rlcon = spl(kn, s, P_LCON), rccon = spl(kn, s, P_CCON), rfcon = spl(kn, s, P_FCON);
+    double rqmu = spl(kn, s, P_QMU), rxlam = spl(kn, s, P_XLAM), rxa2 = spl(kn, s, P_XA2);
+    double qaa = 1.0 + rxa2 * c.lno.x;
+    double qff = 1.0 + rxlam * c.lno.x;
+    double qll = 1.0 + rqmu * c.lno.x;
+    double cccon = 1.0 / (rccon * qaa);
+    double cfcon = rfcon * qff, clcon = rlcon * qll;
+    for (int i = 0; i < 5; i++)
+        for (int j = 0; j < 6; j++) svs[i][j] = mk(0.0);
+    double z = c.zeta;
+    if (c.ll != 1) svs[0][4] = (0.25 * c.szeta2m2) * mk(-mm[3] + mm[5], -2.0 * mm[4]);
+    svs[1][1] = ((0.5 * rs) * mk(mm[1], mm[2])) / clcon;
+    svs[2][0] = mk(((rs * mm[0]) * cccon));
+    svs[2][3] = mk((-mm[3] - mm[5]) + ((2.0 * mm[0]) * cfcon) * cccon);
+    svs[2][4] = mk((0.5 * z) * (mm[3] + mm[5]) - ((z * mm[0]) * cfcon) * cccon);
+    svs[3][1] = ((0.5 * rs) * mk(-mm[1], mm[2])) / clcon;
+    if (c.ll != 1) svs[4][4] = (0.25 * c.szeta2m2) * mk(-mm[3] + mm[5], 2.0 * mm[4]);
+    cd den = (imul(c.omega) * rs) * rs;
+    for (int i = 0; i < 5; i++)
+        for (int j = 0; j < 6; j++) svs[i][j] = (c.nu * svs[i][j]) / den;
+}
+
+// ---------------------------------------------------------------------------
+// One (omega_j, l) pair: yspec.f90:259-400.  coef = uu(1:5), vv(1:5), ww(1:5).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ cd omega_of(const EventDev& ev, int j)
+{
+    // w = wmin + (j-1)*dw - i*ep, formed without contraction (yspec.f90:261)
+    return mk(__dadd_rn(ev.wmin, __dmul_rn((double)(j - 1), ev.dw)), -ev.ep);
+}
+
+__device__ __forceinline__ cd out_factor(int out, cd w)
+{
+    // multiply by i*w (velocity) or -w*w (acceleration), yspec.f90:284-288
+    return out == 1 ? imul(w) : (out == 2 ? -(w * w) : mk(1.0));
+}
+
+// l == 0: radial mode, yspec.f90:263-293
+__device__ inline void pair_radial(Ctx& c, const EventDev& ev, int j, cd* coef)
+{
+    cd w = omega_of(ev, j);
+    set_l(c, 0);
+    set_omega(c, w);
+    cd sr0[2], yrad[2][2];
+    source_vector_rad(c, ev.is, ev.rs, ev.mm, sr0);
+    alpha_steps(c);
+    if (ev.grav == 0) rad_solver_ng(c, ev.rr, ev.rs, ev.ir, ev.is, yrad);
+    else rad_solver_wg(c, ev.rr, ev.rs, yrad);
+    cd u3 = (sr0[0] * yrad[0][0] + sr0[1] * yrad[0][1]) / ev.rr;
+    if (ev.out != 0) u3 = out_factor(ev.out, w) * u3;
+    for (int q = 0; q < NCOEF; q++) coef[q] = mk(0.0);
+    coef[2] = u3;
+}
+
+// l >= 2: toroidal part, yspec.f90:301-316 -> ww(1:5)
+__device__ inline void pair_toroidal(Ctx& c, const EventDev& ev, int l, int j, cd* ww)
+{
+    cd w = omega_of(ev, j);
+    set_l(c, l);
+    set_omega(c, w);
+    cd svt[5][2], ytor[2][2];
+    source_vector_tor(c, ev.is, ev.rs, ev.mm, svt);
+    tor_solver(c, ev.rr, ev.rs, ev.ir, ev.is, ytor);
+    if (ev.out != 0) {
+        cd f = out_factor(ev.out, w);
+        for (int a = 0; a < 2; a++)
+            for (int b = 0; b < 2; b++) ytor[a][b] = f * ytor[a][b];
+    }
+    double zeta = (double)sqrtf((float)(l * (l + 1)));   // yspec.f90:255 (FP32)
+    double zr = zeta * ev.rr;
+    for (int q = 0; q < 5; q++) ww[q] = (svt[q][0] * ytor[0][0] + svt[q][1] * ytor[0][1]) / zr;
+}
+
+// l >= 1: spheroidal part, yspec.f90:344-400 -> uu(1:5), vv(1:5)
+__device__ inline void pair_spheroidal(Ctx& c, const EventDev& ev, int l, int j, cd* uu, cd* vv)
+{
+    cd w = omega_of(ev, j);
+    set_l(c, l);
+    set_omega(c, w);
+    alpha_steps(c);
+    cd svs[5][6], ysph[6][4];
+    source_vector_sph(c, ev.is, ev.rs, ev.mm, svs);
+    if (ev.grav == 2) {
+        sph_solver_g(c, ev.rr, ev.rs, ev.ir, ev.is, ysph);
+    } else {
+        cd yng[4][4];
+        if (ev.grav == 1) sph_solver_nc<1>(c, ev.rr, ev.rs, ev.ir, ev.is, yng);
+        else sph_solver_nc<0>(c, ev.rr, ev.rs, ev.ir, ev.is, yng);
+        for (int b = 0; b < 4; b++) {                  // yspec.f90:367-374
+            ysph[0][b] = yng[0][b];
+            ysph[1][b] = yng[1][b];
+            ysph[2][b] = mk(0.0);
+        }
+    }
+    double zeta = (double)sqrtf((float)(l * (l + 1)));   // yspec.f90:255 (FP32)
+    if (ev.out == 1) {
+        cd f = imul(w);
+        for (int b = 0; b < 4; b++)
+            for (int a = 0; a < 3; a++) ysph[a][b] = f * ysph[a][b];
+    } else if (ev.out == 2) {
+        cd mw2 = -(w * w);
+        if (ev.cor == 0) {
+            for (int b = 0; b < 4; b++)
+                for (int a = 0; a < 3; a++) ysph[a][b] = mw2 * ysph[a][b];
+        } else {                                       // yspec.f90:388-391
+            double gr = ev.grav_ir;
+            for (int b = 0; b < 4; b++) {
+                cd c1 = (-((double)(l + 1) * ysph[2][b] + (2.0 * gr) * ysph[0][b])) / ev.rr;
+                cd c2 = (zeta * (ysph[2][b] + gr * ysph[0][b])) / ev.rr;
+                ysph[0][b] = mw2 * ysph[0][b] + c1;
+                ysph[1][b] = mw2 * ysph[1][b] + c2;
+            }
+        }
+    }
+    double zr = zeta * ev.rr;
+    for (int q = 0; q < 5; q++) {                      // yspec.f90:396-400
+        uu[q] = (ysph[0][0] * svs[q][0] + ysph[0][1] * svs[q][1] + ysph[0][2] * svs[q][3] +
+                 ysph[0][3] * svs[q][4]) / ev.rr;
+        vv[q] = (ysph[1][0] * svs[q][0] + ysph[1][1] * svs[q][1] + ysph[1][2] * svs[q][3] +
+                 ysph[1][3] * svs[q][4]) / zr;
+    }
+}
+
+}  // namespace ysg
