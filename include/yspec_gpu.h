@@ -108,9 +108,22 @@ int ysg_event_traces(ysg_handle *h, const ysg_time *tm, double *out, int *nout);
 /* Rows the trace output will have for tm (yspec.f90:479-486). */
 int ysg_trace_rows(const ysg_time *tm);
 
-/* Spectra then traces without copying the spectra to the host. */
+/* Spectra then traces without copying the spectra to the host
+ * (= ysg_event_prepare + ysg_event_execute + ysg_event_fetch). */
 int ysg_event_run(ysg_handle *h, const ysg_event *ev, const ysg_time *tm, double *out,
                   int *nout);
+
+/* The three phases of ysg_event_run, for callers that time or overlap the
+ * device work.  prepare copies the event's inputs to the device and returns
+ * when they are resident; execute enqueues every kernel of the event on the
+ * handle's stream and returns at once; fetch copies the traces of the last
+ * execute to `out` (if non-NULL), waits, and reports the status. */
+int ysg_event_prepare(ysg_handle *h, const ysg_event *ev, const ysg_time *tm);
+int ysg_event_execute(ysg_handle *h);
+int ysg_event_fetch(ysg_handle *h, double *out, int *nout);
+
+/* The handle's cudaStream_t, as a void pointer. */
+int ysg_get_stream(ysg_handle *h, void **stream);
 
 /* Several events through the batched persistent solver: one launch per
  * stage for all events, CUDA-graph captured.  outs[e] receives the traces of
@@ -143,6 +156,14 @@ int ysg_last_timings(ysg_handle *h, float ms[4]);
 /* Counters of the last solve stage: number of (omega,l) pairs and the
  * algorithmic FP64 flop count of the stepping work actually performed. */
 int ysg_last_work(ysg_handle *h, double *pairs, double *flops);
+
+/* Host<->device bytes moved by the last ysg_event_run / prepare+fetch:
+ * event inputs and tables copied in, traces copied out. */
+int ysg_last_bytes(ysg_handle *h, double *h2d, double *d2h);
+
+/* Measured FP64 fused-multiply-add throughput of `device` in TFLOP/s
+ * (roofline denominator of the solve stage). */
+int ysg_fp64_peak(int device, double *tflops);
 
 const char *ysg_status_string(int status);
 void ysg_destroy(ysg_handle *h);

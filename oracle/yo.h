@@ -109,9 +109,11 @@ void yo_solve_pair(const yo_model *m, const yo_norms *n, const yo_params *p,
                    yo_counts *cnt);
 
 /* Full spectra: ur/ut/up are (nw, nr) column-major (omega fastest), summed
- * over l exactly as yspec.f90:250-426.  nthreads <= 0 uses OpenMP default.
+ * over l exactly as yspec.f90:250-426.
  * lsub_lo/lsub_hi restrict the l range (inclusive) when lsub_hi >= 0.
- * jsub restricts omega to j < jsub when > 0 (bounded CPU samples). */
+ * jsub > 0 restricts omega to j <= jsub; jsub < 0 takes every |jsub|-th
+ * frequency j = 1, 1+|jsub|, ... (bounded CPU samples across the band).
+ * nthreads <= 0 uses every online core. */
 int yo_spectra(const yo_model *m, const yo_norms *n, const yo_params *p,
                const yo_grid *g, yo_cd *ur, yo_cd *ut, yo_cd *up,
                int nthreads, int lsub_lo, int lsub_hi, int jsub,

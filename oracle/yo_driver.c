@@ -191,7 +191,7 @@ typedef struct {
     yo_cd *ur, *ut, *up;
     const double *xa, *xpa, *xca;
     const yo_cd *eia;
-    int lo, hi, jmax, next;
+    int lo, hi, jmax, jstride, next;
     pthread_mutex_t lock;
 } spectra_job;
 
@@ -249,8 +249,9 @@ static void *spectra_worker(void *a)
     spectra_job *jb = arg->job;
     for (;;) {
         pthread_mutex_lock(&jb->lock);
-        int j = ++jb->next;
+        int k = ++jb->next;
         pthread_mutex_unlock(&jb->lock);
+        int j = 1 + (k - 1) * jb->jstride;
         if (j > jb->jmax) break;
         spectra_one(jb, j, arg->cnt);
     }
@@ -266,8 +267,9 @@ int yo_spectra(const yo_model *m, const yo_norms *n, const yo_params *p,
     int nr = p->nr, lmax = p->lmax, nw = g->nw;
     int lo = p->lmin, hi = p->lmax;
     if (lsub_hi >= 0) { lo = lsub_lo; hi = lsub_hi; }
-    int jmax = nw;
+    int jmax = nw, jstride = 1;
     if (jsub > 0 && jsub < nw) jmax = jsub;
+    if (jsub < 0) jstride = -jsub;
     double *delta = (double *)malloc((size_t)nr * sizeof(double));
     double *azep = (double *)malloc((size_t)nr * sizeof(double));
     double *azst = (double *)malloc((size_t)nr * sizeof(double));
@@ -285,9 +287,9 @@ int yo_spectra(const yo_model *m, const yo_norms *n, const yo_params *p,
 
     int nth = nthreads > 0 ? nthreads : (int)sysconf(_SC_NPROCESSORS_ONLN);
     if (nth < 1) nth = 1;
-    if (nth > jmax) nth = jmax;
+    if (nth > (jmax - 1) / jstride + 1) nth = (jmax - 1) / jstride + 1;
     yo_counts *tc = (yo_counts *)calloc((size_t)nth, sizeof(yo_counts));
-    spectra_job job = {m, n, p, g, ur, ut, up, xa, xpa, xca, eia, lo, hi, jmax, 0,
+    spectra_job job = {m, n, p, g, ur, ut, up, xa, xpa, xca, eia, lo, hi, jmax, jstride, 0,
                        PTHREAD_MUTEX_INITIALIZER};
     pthread_t *th = (pthread_t *)malloc((size_t)nth * sizeof(pthread_t));
     spectra_arg *args = (spectra_arg *)malloc((size_t)nth * sizeof(spectra_arg));

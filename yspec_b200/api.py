@@ -162,6 +162,23 @@ class Engine:
                                       N.dptr(out), C.byref(n)), "run")
         return out
 
+    def prepare(self, event: Event) -> None:
+        N.check(N.lib().ysg_event_prepare(self.h, C.byref(event.raw.ev), C.byref(event.raw.tm)), "prepare")
+
+    def execute(self) -> None:
+        N.check(N.lib().ysg_event_execute(self.h), "execute")
+
+    def fetch(self, out: np.ndarray | None = None, out_ptr: int | None = None) -> int:
+        n = C.c_int()
+        ptr = N.dptr(out) if out is not None else (C.cast(out_ptr, N._dp) if out_ptr else None)
+        N.check(N.lib().ysg_event_fetch(self.h, ptr, C.byref(n)), "fetch")
+        return n.value
+
+    def stream(self) -> int:
+        s = C.c_void_p()
+        N.check(N.lib().ysg_get_stream(self.h, C.byref(s)), "stream")
+        return s.value or 0
+
     def batch_run(self, events: list[Event]) -> list[np.ndarray]:
         nev = len(events)
         evs = (N.YsgEvent * nev)(*[e.raw.ev for e in events])
@@ -191,10 +208,22 @@ class Engine:
         N.check(N.lib().ysg_last_timings(self.h, ms), "timings")
         return list(ms)
 
+    def bytes_moved(self) -> tuple[float, float]:
+        a, b = C.c_double(), C.c_double()
+        N.check(N.lib().ysg_last_bytes(self.h, C.byref(a), C.byref(b)), "bytes")
+        return a.value, b.value
+
     def work(self) -> tuple[float, float]:
         p, f = C.c_double(), C.c_double()
         N.check(N.lib().ysg_last_work(self.h, C.byref(p), C.byref(f)), "work")
         return p.value, f.value
+
+
+def fp64_peak_tflops(device: int = 0) -> float:
+    """Measured FP64 FMA throughput of the device (TFLOP/s)."""
+    t = C.c_double()
+    N.check(N.lib().ysg_fp64_peak(device, C.byref(t)), "fp64_peak")
+    return t.value
 
 
 def run_file(param_file: str | os.PathLike, device: int = 0, write_files: bool = False) -> np.ndarray:

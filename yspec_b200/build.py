@@ -40,6 +40,7 @@ SOURCES = [
     CSRC / "k_legendre.cu",
     CSRC / "k_lsum.cu",
     CSRC / "k_ifft.cu",
+    CSRC / "k_peak.cu",
     CSRC / "host" / "ysh_host.cpp",
 ]
 

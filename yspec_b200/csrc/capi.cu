@@ -7,6 +7,11 @@
 // host-side tables (cos/sin of the epicentral angles, e^{i m azst} powers,
 // the taper, FFT twiddles, e^{eps t}) are formed here on the host, in FP64,
 // as the reference forms them, and uploaded with each event.
+//
+// Internally every call is upload (host -> device, synchronous) followed by
+// enqueue (kernels only, asynchronous) and finish (device -> host, counters).
+// ysg_event_prepare / _execute / _fetch expose the three phases so a caller
+// can time the device work alone.
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -43,10 +48,10 @@ struct DevBuf {
 };
 
 // Algorithmic FP64 flops of one Cash-Karp step per system class (index =
-// Sys::CLS in ysg_ode.cuh): 6 right-hand sides plus the stage
+// Sys::CLS in ysg_ode.cuh): six right-hand sides plus the stage
 // combinations (88 flops per complex component).  The per-RHS counts are
-// hand tallies of the coefficient matrix and derivative expressions.
-const double kStepFlops[8] = {
+// hand tallies of the coefficient-matrix and derivative expressions.
+const double kStepFlops[NSYS_COUNT] = {
     6 * 88.0 + 88.0 * 2,     // toroidal
     6 * 177.0 + 88.0 * 2,    // radial
     6 * 100.0 + 88.0 * 2,    // fluid minors, no gravity / Cowling
@@ -63,7 +68,7 @@ struct ysg_handle {
     int device = 0;
     cudaStream_t st = nullptr;
     cudaEvent_t ev[5] = {};
-    int solver = 0;
+    int solver = 1;
     // model
     DevBuf kn;
     ModelHdr hdr{};
@@ -71,131 +76,23 @@ struct ysg_handle {
     bool has_model = false;
     // event buffers
     DevBuf coef, leg, E, delta, ct, stv, spec, filt, tw, expt, cs, scratch, out;
-    DevBuf work, status;
-    bool has_spectra = false;
-    int last_nw = 0, last_nr = 0;
+    DevBuf work, status, items, counter, evdev, coefptr;
+    int nitems = 0, solve_blocks = 0, solve_block = 64;
+    // uploaded event / time stage
+    bool ev_ready = false, tm_ready = false, has_spectra = false;
+    EventDev pev{};
+    TraceDev ptd{};
+    int p_nr = 0, p_lmax = 0;
     float ms[4] = {0, 0, 0, 0};
+    double h2d = 0.0, d2h = 0.0;     // bytes moved since the last prepare
     double pairs = 0.0, flops = 0.0;
 };
 
-#define CK(x)                                   \
-    do {                                        \
-        cudaError_t e_ = (x);                   \
+#define CK(x)                                       \
+    do {                                            \
+        cudaError_t e_ = (x);                       \
         if (e_ != cudaSuccess) return YSG_ERR_CUDA; \
     } while (0)
-
-extern "C" {
-
-const char* ysg_status_string(int s)
-{
-    switch (s) {
-        case YSG_OK: return "ok";
-        case YSG_ERR_ARG: return "bad argument";
-        case YSG_ERR_CUDA: return "CUDA runtime error";
-        case YSG_ERR_NO_MODEL: return "no model uploaded";
-        case YSG_ERR_NO_SPECTRA: return "traces requested before spectra";
-        case YSG_ERR_DEVICE_WAIT: return "a bounded device-side wait gave up";
-        case YSG_ERR_NO_DEVICE: return "no CUDA device";
-        case YSG_ERR_LIMIT: return "size beyond a fixed capacity";
-        default: return "unknown status";
-    }
-}
-
-int ysg_create(ysg_handle** out, int device)
-{
-    if (!out) return YSG_ERR_ARG;
-    *out = nullptr;
-    int n = 0;
-    if (cudaGetDeviceCount(&n) != cudaSuccess || n <= 0) return YSG_ERR_NO_DEVICE;
-    if (device < 0 || device >= n) return YSG_ERR_ARG;
-    ysg_handle* h = new ysg_handle;
-    h->device = device;
-    if (cudaSetDevice(device) != cudaSuccess ||
-        cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking) != cudaSuccess) {
-        delete h;
-        return YSG_ERR_CUDA;
-    }
-    for (auto& e : h->ev) cudaEventCreate(&e);
-    if (h->status.ensure(sizeof(int)) != cudaSuccess || h->work.ensure(8 * sizeof(unsigned long long)) != cudaSuccess) {
-        ysg_destroy(h);
-        return YSG_ERR_CUDA;
-    }
-    *out = h;
-    return YSG_OK;
-}
-
-void ysg_destroy(ysg_handle* h)
-{
-    if (!h) return;
-    cudaSetDevice(h->device);
-    if (h->st) cudaStreamSynchronize(h->st);
-    for (DevBuf* b : {&h->kn, &h->coef, &h->leg, &h->E, &h->delta, &h->ct, &h->stv, &h->spec,
-                      &h->filt, &h->tw, &h->expt, &h->cs, &h->scratch, &h->out, &h->work,
-                      &h->status})
-        b->release();
-    for (auto& e : h->ev)
-        if (e) cudaEventDestroy(e);
-    if (h->st) cudaStreamDestroy(h->st);
-    delete h;
-}
-
-int ysg_set_solver(ysg_handle* h, int which)
-{
-    if (!h || which < 0 || which > 1) return YSG_ERR_ARG;
-    h->solver = which;
-    return YSG_OK;
-}
-
-int ysg_model_upload(ysg_handle* h, const ysg_model* m)
-{
-    if (!h || !m || m->nknot < 2 || !m->r || !m->alpha || !m->beta) return YSG_ERR_ARG;
-    for (int p = 0; p < NPARAM; p++)
-        if (!m->val[p] || !m->cs[p]) return YSG_ERR_ARG;
-    const int n = m->nknot;
-    if ((size_t)(n + 2) * sizeof(Knot) > 200 * 1024) return YSG_ERR_LIMIT;   // fits shared memory
-    std::vector<Knot> rec((size_t)n + 2);
-    std::memset(rec.data(), 0, rec.size() * sizeof(Knot));
-    for (int i = 0; i < n; i++) {
-        Knot& k = rec[(size_t)i + 1];
-        k.r = m->r[i];
-        k.alpha = m->alpha[i];
-        k.beta = m->beta[i];
-        for (int p = 0; p < NPARAM; p++) {
-            k.v[p][0] = m->val[p][i];
-            k.v[p][1] = m->cs[p][i];
-        }
-    }
-    ModelHdr hd{};
-    hd.nknot = n;
-    hd.nic = m->nic;
-    hd.noc = m->noc;
-    hd.nsl = m->nsl;
-    hd.ocean = m->ocean;
-    hd.fic = m->fic;
-    // iminloc: first index of the minimum (nrutil.f90:392-399)
-    int ia = 1;
-    for (int i = 2; i <= n; i++)
-        if (m->alpha[i - 1] < m->alpha[ia - 1]) ia = i;
-    int ib = m->noc + 1;
-    for (int i = m->noc + 2; i <= m->nsl; i++)
-        if (m->beta[i - 1] < m->beta[ib - 1]) ib = i;
-    hd.imin_alpha = ia;
-    hd.imin_beta = ib;
-    hd.tref = m->tref;
-    hd.pibigg = m->pibigg;
-    hd.fre_norm = m->fre_norm;
-    cudaSetDevice(h->device);
-    CK(h->kn.ensure(rec.size() * sizeof(Knot)));
-    CK(cudaMemcpyAsync(h->kn.p, rec.data(), rec.size() * sizeof(Knot), cudaMemcpyHostToDevice, h->st));
-    CK(cudaStreamSynchronize(h->st));
-    h->hdr = hd;
-    h->grav_host.assign(m->val[P_GRAV], m->val[P_GRAV] + n);
-    h->has_model = true;
-    h->has_spectra = false;
-    return YSG_OK;
-}
-
-}  // extern "C"
 
 namespace {
 
@@ -207,6 +104,7 @@ int check_event(const ysg_handle* h, const ysg_event* ev)
     if (ev->is < 1 || ev->ir < 1 || ev->is >= h->hdr.nknot || ev->ir >= h->hdr.nknot) return YSG_ERR_ARG;
     if (ev->nr > 0 && (!ev->delta || !ev->azst)) return YSG_ERR_ARG;
     if (ev->grav < 0 || ev->grav > 2 || ev->out < 0 || ev->out > 2) return YSG_ERR_ARG;
+    if (!(ev->dw > 0.0) || !(ev->wmin > 0.0) || !(ev->ep > 0.0)) return YSG_ERR_ARG;
     return YSG_OK;
 }
 
@@ -254,50 +152,407 @@ cd cpowi(cd a, int m)
     return pw;
 }
 
-int run_solve_stage(ysg_handle* h, const EventDev& d)
+// Predicted relative cost of the pairs (l, omega_j .. omega_j+31) of an
+// event: Cash-Karp steps grow with omega times the radial path integrated
+// (start level below the turning radius up to the source, then the minor
+// continuation and four b-vector passes from source to receiver) plus a
+// per-interval floor.  Used only to order the work (longest first).
+double item_cost(const EventDev& ev, int li, int j0)
 {
-    const int L = d.lmax - d.lmin + 1;
-    const size_t ncoef = (size_t)L * NCOEF * d.nw;
-    CK(h->coef.ensure(ncoef * sizeof(cd)));
-    CK(cudaMemsetAsync(h->work.p, 0, 8 * sizeof(unsigned long long), h->st));
-    CK(cudaMemsetAsync(h->status.p, 0, sizeof(int), h->st));
-    CK(launch_solve_plain(h->kn.as<Knot>(), h->hdr, d, h->coef.as<cd>(),
-                          h->work.as<unsigned long long>(), h->status.as<int>(), h->st));
+    const int l = ev.lmin + li;
+    const double w = ev.wmin + (j0 + 16) * ev.dw;
+    const double vref = 1.0;                       // normalised wave speed scale
+    double rturn = (l + 0.5) * vref / w;
+    if (rturn > 1.0) rturn = 1.0;
+    double below = ev.rs - 0.6 * rturn;
+    if (below < 0.0) below = 0.0;
+    double above = std::fabs(ev.rr - ev.rs);
+    return 32.0 + w * (below + 5.0 * above) * 200.0;
+}
+
+struct Item {
+    int ev, li, j0;
+    double cost;
+};
+
+void build_items(std::vector<Item>& out, int e, const EventDev& ev)
+{
+    const int L = ev.lmax - ev.lmin + 1;
+    for (int li = 0; li < L; li++)
+        for (int j0 = 0; j0 < ev.nw; j0 += 32) out.push_back({e, li, j0, item_cost(ev, li, j0)});
+}
+
+int upload_items(ysg_handle* h, std::vector<Item>& items, const std::vector<EventDev>& evs,
+                 const std::vector<cd*>& coefs)
+{
+    std::stable_sort(items.begin(), items.end(),
+                     [](const Item& a, const Item& b) { return a.cost > b.cost; });
+    std::vector<int4> packed(items.size());
+    for (size_t i = 0; i < items.size(); i++) packed[i] = make_int4(items[i].ev, items[i].li, items[i].j0, 0);
+    CK(h->items.ensure(std::max<size_t>(packed.size(), 1) * sizeof(int4)));
+    CK(h->evdev.ensure(std::max<size_t>(evs.size(), 1) * sizeof(EventDev)));
+    CK(h->coefptr.ensure(std::max<size_t>(coefs.size(), 1) * sizeof(cd*)));
+    CK(h->counter.ensure(sizeof(int)));
+    if (!packed.empty())
+        CK(cudaMemcpyAsync(h->items.p, packed.data(), packed.size() * sizeof(int4), cudaMemcpyHostToDevice, h->st));
+    CK(cudaMemcpyAsync(h->evdev.p, evs.data(), evs.size() * sizeof(EventDev), cudaMemcpyHostToDevice, h->st));
+    CK(cudaMemcpyAsync(h->coefptr.p, coefs.data(), coefs.size() * sizeof(cd*), cudaMemcpyHostToDevice, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    h->h2d += (double)(packed.size() * sizeof(int4) + evs.size() * sizeof(EventDev) +
+                       coefs.size() * sizeof(cd*));
+    h->nitems = (int)packed.size();
+    if (h->solve_blocks == 0) h->solve_blocks = solve_batched_blocks(h->solve_block);
     return YSG_OK;
 }
 
-int finish_solve_stage(ysg_handle* h, const EventDev& d)
+// Event inputs to the device: cos/sin of delta and e^{i m azst}
+// (yspec.f90:173-174, :331, :414); buffers sized.  No kernel runs.
+int upload_event(ysg_handle* h, const ysg_event* ev)
 {
-    unsigned long long w[8];
-    int status = 0;
-    CK(cudaMemcpyAsync(w, h->work.p, sizeof w, cudaMemcpyDeviceToHost, h->st));
-    CK(cudaMemcpyAsync(&status, h->status.p, sizeof status, cudaMemcpyDeviceToHost, h->st));
+    const int nr = ev->nr, nw = ev->nw, n1 = std::max(nr, 1);
+    std::vector<double> ct(n1), stv(n1);
+    std::vector<cd> E((size_t)n1 * 5);
+    for (int k = 0; k < nr; k++) {
+        ct[k] = std::cos(ev->delta[k]);
+        stv[k] = std::sin(ev->delta[k]);
+        cd eia = mk(std::cos(ev->azst[k]), std::sin(ev->azst[k]));
+        for (int m = -2; m <= 2; m++) E[(size_t)k * 5 + (m + 2)] = cpowi(eia, m);
+    }
+    const int L = ev->lmax - ev->lmin + 1;
+    CK(h->coef.ensure((size_t)L * NCOEF * nw * sizeof(cd)));
+    CK(h->spec.ensure(3 * (size_t)nw * n1 * sizeof(cd)));
+    CK(h->delta.ensure((size_t)n1 * sizeof(double)));
+    CK(h->ct.ensure((size_t)n1 * sizeof(double)));
+    CK(h->stv.ensure((size_t)n1 * sizeof(double)));
+    CK(h->E.ensure((size_t)n1 * 5 * sizeof(cd)));
+    CK(h->leg.ensure((size_t)(ev->lmax + 1) * n1 * 8 * sizeof(double)));
+    if (nr > 0) {
+        CK(cudaMemcpyAsync(h->delta.p, ev->delta, (size_t)nr * sizeof(double), cudaMemcpyHostToDevice, h->st));
+        CK(cudaMemcpyAsync(h->ct.p, ct.data(), (size_t)nr * sizeof(double), cudaMemcpyHostToDevice, h->st));
+        CK(cudaMemcpyAsync(h->stv.p, stv.data(), (size_t)nr * sizeof(double), cudaMemcpyHostToDevice, h->st));
+        CK(cudaMemcpyAsync(h->E.p, E.data(), (size_t)nr * 5 * sizeof(cd), cudaMemcpyHostToDevice, h->st));
+        h->h2d += (double)nr * (3 * sizeof(double) + 5 * sizeof(cd));
+    }
+    CK(cudaStreamSynchronize(h->st));   // the host vectors go out of scope
+    h->pev = make_event(h, ev);
+    if (h->solver == 1) {
+        std::vector<Item> items;
+        build_items(items, 0, h->pev);
+        int rc = upload_items(h, items, {h->pev}, {h->coef.as<cd>()});
+        if (rc) return rc;
+    }
+    h->p_nr = nr;
+    h->p_lmax = ev->lmax;
+    h->ev_ready = true;
+    return YSG_OK;
+}
+
+// Time-stage inputs: taper (module_fourier.f90:96-116), twiddles with pi_d,
+// e^{eps t} (yspec.f90:439-444), cos/sin of azep (:466-473).
+int upload_time(ysg_handle* h, const ysg_time* tm, int nw)
+{
+    const int n = tm->nt, nr = tm->nr;
+    if (n < 4 || (n & (n - 1)) || n > (1 << 20)) return YSG_ERR_ARG;
+    if (tm->i2 - tm->i1 + 1 != nw || tm->i1 < 1 || tm->i2 > n) return YSG_ERR_ARG;
+    if (nr > 0 && !tm->azep) return YSG_ERR_ARG;
+    const int nout = ysg_trace_rows(tm);
+    int p = 0;
+    while ((1 << p) < n) p++;
+    const double pi_d = (double)3.14159265358979323846f;
+    std::vector<double> filt((size_t)n / 2 + 1, 1.0), expt(nout), cs(2 * (size_t)std::max(nr, 1));
+    const double w1 = tm->f11, w2 = tm->f12, w3 = tm->f21, w4 = tm->f22;
+    if (!(w1 == 0.0 && w2 == 0.0 && w3 == 0.0 && w4 == 0.0)) {
+        double f = 0.0;
+        for (int i = 1; i <= n / 2 + 1; i++) {
+            double w = (double)(i - 1) * tm->df;
+            if (w < w1) f = 0.0;
+            else if (w >= w1 && w < w2) f = 0.5 * (1.0 - std::cos(pi_d * (w - w1) / (w2 - w1)));
+            else if (w >= w2 && w < w3) f = 1.0;
+            else if (w >= w3 && w < w4) f = 0.5 * (1.0 - std::cos(pi_d * (w4 - w) / (w4 - w3)));
+            else if (w >= w4) f = 0.0;
+            filt[(size_t)i - 1] = f;
+        }
+    }
+    std::vector<cd> tw((size_t)n / 2);
+    const double dth = pi_d / (double)(n / 2);     // exact: n/2 is a power of two
+    for (int m = 0; m < n / 2; m++) {
+        double a = (double)m * dth;
+        tw[(size_t)m] = mk(std::cos(a), std::sin(a));
+    }
+    for (int i = 0; i < nout; i++) expt[(size_t)i] = std::exp(tm->ep * ((double)i * tm->dt));
+    for (int k = 0; k < nr; k++) {
+        cs[2 * (size_t)k] = std::cos(tm->azep[k]);
+        cs[2 * (size_t)k + 1] = std::sin(tm->azep[k]);
+    }
+    CK(h->filt.ensure(filt.size() * sizeof(double)));
+    CK(h->tw.ensure(tw.size() * sizeof(cd)));
+    CK(h->expt.ensure(expt.size() * sizeof(double)));
+    CK(h->cs.ensure(cs.size() * sizeof(double)));
+    CK(h->scratch.ensure(std::max<size_t>(ifft_scratch_bytes(n, nr), 16)));
+    CK(h->out.ensure(std::max<size_t>((size_t)nout * 4 * nr * sizeof(double), 16)));
+    CK(cudaMemcpyAsync(h->filt.p, filt.data(), filt.size() * sizeof(double), cudaMemcpyHostToDevice, h->st));
+    CK(cudaMemcpyAsync(h->tw.p, tw.data(), tw.size() * sizeof(cd), cudaMemcpyHostToDevice, h->st));
+    CK(cudaMemcpyAsync(h->expt.p, expt.data(), expt.size() * sizeof(double), cudaMemcpyHostToDevice, h->st));
+    CK(cudaMemcpyAsync(h->cs.p, cs.data(), cs.size() * sizeof(double), cudaMemcpyHostToDevice, h->st));
+    h->h2d += (double)((filt.size() + expt.size() + cs.size()) * sizeof(double) + tw.size() * sizeof(cd));
     CK(cudaStreamSynchronize(h->st));
-    double fl = 0.0;
-    for (int q = 0; q < 8; q++) fl += (double)w[q] * kStepFlops[q];
-    h->flops = fl;
-    h->pairs = (double)(d.lmax - d.lmin + 1) * d.nw;
+    TraceDev& td = h->ptd;
+    td = TraceDev{};
+    td.nt = n;
+    td.i1 = tm->i1;
+    td.i2 = tm->i2;
+    td.nw = nw;
+    td.nr = nr;
+    td.nout = nout;
+    td.log2n = p;
+    td.b1 = 1 << ((p + 1) / 2);
+    td.dt = tm->dt;
+    td.scale = tm->dt * (double)n;
+    td.t_norm = tm->t_norm;
+    td.amp_norm = tm->amp_norm;
+    h->tm_ready = true;
+    return YSG_OK;
+}
+
+int enqueue_solve(ysg_handle* h)
+{
+    const EventDev& d = h->pev;
+    CK(cudaMemsetAsync(h->work.p, 0, NSYS_COUNT * sizeof(unsigned long long), h->st));
+    CK(cudaMemsetAsync(h->status.p, 0, sizeof(int), h->st));
+    if (h->solver == 0) {
+        CK(launch_solve_plain(h->kn.as<Knot>(), h->hdr, d, h->coef.as<cd>(),
+                              h->work.as<unsigned long long>(), h->status.as<int>(), h->st));
+    } else {
+        (void)d;
+        CK(launch_solve_batched(h->kn.as<Knot>(), h->hdr, h->evdev.as<EventDev>(),
+                                h->coefptr.as<cd*>(), h->items.as<int4>(), h->nitems,
+                                h->counter.as<int>(), h->work.as<unsigned long long>(),
+                                h->solve_blocks, h->solve_block, h->st));
+    }
+    return YSG_OK;
+}
+
+// K2 -> K1 -> K3 on the stream, with timing events; no host synchronisation.
+int enqueue_spectra(ysg_handle* h)
+{
+    const EventDev& d = h->pev;
+    const int nr = h->p_nr, nw = d.nw;
+    const size_t nspec = (size_t)nw * std::max(nr, 1);
+    cd* d_ur = h->spec.as<cd>();
+    CK(cudaEventRecord(h->ev[0], h->st));
+    CK(launch_legendre(nr, h->p_lmax, h->delta.as<double>(), h->ct.as<double>(), h->stv.as<double>(),
+                       h->leg.as<double>(), h->st));
+    CK(cudaEventRecord(h->ev[1], h->st));
+    int rc = enqueue_solve(h);
+    if (rc) return rc;
+    CK(cudaEventRecord(h->ev[2], h->st));
+    CK(launch_lsum(nw, nr, d.lmin, d.lmax, h->coef.as<cd>(), h->leg.as<double>(), h->E.as<cd>(),
+                   d_ur, d_ur + nspec, d_ur + 2 * nspec, h->st));
+    CK(cudaEventRecord(h->ev[3], h->st));
+    return YSG_OK;
+}
+
+int enqueue_traces(ysg_handle* h)
+{
+    const TraceDev& td = h->ptd;
+    const size_t nspec = (size_t)td.nw * std::max(td.nr, 1);
+    const cd* d_ur = h->spec.as<cd>();
+    CK(cudaEventRecord(h->ev[3], h->st));
+    CK(launch_ifft(td, d_ur, d_ur + nspec, d_ur + 2 * nspec, h->filt.as<double>(), h->tw.as<cd>(),
+                   h->expt.as<double>(), h->cs.as<double>(), h->scratch.as<cd>(), h->out.as<double>(),
+                   h->st));
+    CK(cudaEventRecord(h->ev[4], h->st));
+    return YSG_OK;
+}
+
+// Wait for the stream, read the solve counters and the status word.
+int finish(ysg_handle* h, bool spectra, bool traces)
+{
+    unsigned long long w[NSYS_COUNT] = {};
+    int status = 0;
+    if (spectra) {
+        CK(cudaMemcpyAsync(w, h->work.p, sizeof w, cudaMemcpyDeviceToHost, h->st));
+        CK(cudaMemcpyAsync(&status, h->status.p, sizeof status, cudaMemcpyDeviceToHost, h->st));
+    }
+    CK(cudaStreamSynchronize(h->st));
+    if (spectra) {
+        double fl = 0.0;
+        for (int q = 0; q < NSYS_COUNT; q++) fl += (double)w[q] * kStepFlops[q];
+        h->flops = fl;
+        h->pairs = (double)(h->pev.lmax - h->pev.lmin + 1) * h->pev.nw;
+        cudaEventElapsedTime(&h->ms[0], h->ev[0], h->ev[1]);
+        cudaEventElapsedTime(&h->ms[1], h->ev[1], h->ev[2]);
+        cudaEventElapsedTime(&h->ms[2], h->ev[2], h->ev[3]);
+        h->has_spectra = status == 0;
+    }
+    if (traces) cudaEventElapsedTime(&h->ms[3], h->ev[3], h->ev[4]);
     return status ? YSG_ERR_DEVICE_WAIT : YSG_OK;
+}
+
+int copy_out(ysg_handle* h, double* out, int* nout)
+{
+    const TraceDev& td = h->ptd;
+    if (nout) *nout = td.nout;
+    if (out && td.nr > 0) {
+        CK(cudaMemcpyAsync(out, h->out.p, (size_t)td.nout * 4 * td.nr * sizeof(double),
+                           cudaMemcpyDeviceToHost, h->st));
+        h->d2h += (double)td.nout * 4 * td.nr * sizeof(double);
+    }
+    return YSG_OK;
 }
 
 }  // namespace
 
 extern "C" {
 
+const char* ysg_status_string(int s)
+{
+    switch (s) {
+        case YSG_OK: return "ok";
+        case YSG_ERR_ARG: return "bad argument";
+        case YSG_ERR_CUDA: return "CUDA runtime error";
+        case YSG_ERR_NO_MODEL: return "no model uploaded";
+        case YSG_ERR_NO_SPECTRA: return "traces requested before spectra";
+        case YSG_ERR_DEVICE_WAIT: return "a bounded device-side wait gave up";
+        case YSG_ERR_NO_DEVICE: return "no CUDA device";
+        case YSG_ERR_LIMIT: return "size beyond a fixed capacity";
+        default: return "unknown status";
+    }
+}
+
+int ysg_create(ysg_handle** out, int device)
+{
+    if (!out) return YSG_ERR_ARG;
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n <= 0) return YSG_ERR_NO_DEVICE;
+    if (device < 0 || device >= n) return YSG_ERR_ARG;
+    ysg_handle* h = new ysg_handle;
+    h->device = device;
+    if (cudaSetDevice(device) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking) != cudaSuccess) {
+        delete h;
+        return YSG_ERR_CUDA;
+    }
+    for (auto& e : h->ev) cudaEventCreate(&e);
+    if (h->status.ensure(sizeof(int)) != cudaSuccess ||
+        h->work.ensure(NSYS_COUNT * sizeof(unsigned long long)) != cudaSuccess) {
+        ysg_destroy(h);
+        return YSG_ERR_CUDA;
+    }
+    *out = h;
+    return YSG_OK;
+}
+
+void ysg_destroy(ysg_handle* h)
+{
+    if (!h) return;
+    cudaSetDevice(h->device);
+    if (h->st) cudaStreamSynchronize(h->st);
+    for (DevBuf* b : {&h->kn, &h->coef, &h->leg, &h->E, &h->delta, &h->ct, &h->stv, &h->spec,
+                      &h->filt, &h->tw, &h->expt, &h->cs, &h->scratch, &h->out, &h->work,
+                      &h->status, &h->items, &h->counter, &h->evdev, &h->coefptr})
+        b->release();
+    for (auto& e : h->ev)
+        if (e) cudaEventDestroy(e);
+    if (h->st) cudaStreamDestroy(h->st);
+    delete h;
+}
+
+int ysg_set_solver(ysg_handle* h, int which)
+{
+    if (!h || which < 0 || which > 1) return YSG_ERR_ARG;
+    h->solver = which;
+    return YSG_OK;
+}
+
+int ysg_get_stream(ysg_handle* h, void** stream)
+{
+    if (!h || !stream) return YSG_ERR_ARG;
+    *stream = (void*)h->st;
+    return YSG_OK;
+}
+
+int ysg_model_upload(ysg_handle* h, const ysg_model* m)
+{
+    if (!h || !m || m->nknot < 2 || !m->r || !m->alpha || !m->beta) return YSG_ERR_ARG;
+    for (int p = 0; p < NPARAM; p++)
+        if (!m->val[p] || !m->cs[p]) return YSG_ERR_ARG;
+    const int n = m->nknot;
+    if ((size_t)(n + 2) * sizeof(Knot) > 200 * 1024) return YSG_ERR_LIMIT;   // fits shared memory
+    if (m->nic < 1 || m->noc <= m->nic || m->nsl <= m->noc || m->nsl > n) return YSG_ERR_ARG;
+    std::vector<Knot> rec((size_t)n + 2);
+    std::memset(rec.data(), 0, rec.size() * sizeof(Knot));
+    for (int i = 0; i < n; i++) {
+        Knot& k = rec[(size_t)i + 1];
+        k.r = m->r[i];
+        k.alpha = m->alpha[i];
+        k.beta = m->beta[i];
+        for (int p = 0; p < NPARAM; p++) {
+            k.v[p][0] = m->val[p][i];
+            k.v[p][1] = m->cs[p][i];
+        }
+    }
+    ModelHdr hd{};
+    hd.nknot = n;
+    hd.nic = m->nic;
+    hd.noc = m->noc;
+    hd.nsl = m->nsl;
+    hd.ocean = m->ocean;
+    hd.fic = m->fic;
+    // iminloc: first index of the minimum (nrutil.f90:392-399)
+    int ia = 1;
+    for (int i = 2; i <= n; i++)
+        if (m->alpha[i - 1] < m->alpha[ia - 1]) ia = i;
+    int ib = m->noc + 1;
+    for (int i = m->noc + 2; i <= m->nsl; i++)
+        if (m->beta[i - 1] < m->beta[ib - 1]) ib = i;
+    hd.imin_alpha = ia;
+    hd.imin_beta = ib;
+    hd.tref = m->tref;
+    hd.pibigg = m->pibigg;
+    hd.fre_norm = m->fre_norm;
+    cudaSetDevice(h->device);
+    CK(h->kn.ensure(rec.size() * sizeof(Knot)));
+    CK(cudaMemcpyAsync(h->kn.p, rec.data(), rec.size() * sizeof(Knot), cudaMemcpyHostToDevice, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    h->hdr = hd;
+    h->grav_host.assign(m->val[P_GRAV], m->val[P_GRAV] + n);
+    h->has_model = true;
+    h->has_spectra = h->ev_ready = h->tm_ready = false;
+    return YSG_OK;
+}
+
+int ysg_trace_rows(const ysg_time* tm)
+{
+    if (!tm) return 0;
+    int nout = tm->nt;
+    for (int i = 1; i <= tm->nt; i++)
+        if ((double)(i - 1) * tm->dt > tm->tout) {
+            nout = i;
+            break;
+        }
+    return nout;
+}
+
 int ysg_event_coef(ysg_handle* h, const ysg_event* ev, double* coef)
 {
     int rc = check_event(h, ev);
     if (rc) return rc;
     cudaSetDevice(h->device);
-    EventDev d = make_event(h, ev);
-    CK(cudaEventRecord(h->ev[0], h->st));
-    rc = run_solve_stage(h, d);
+    h->has_spectra = h->tm_ready = false;
+    rc = upload_event(h, ev);
     if (rc) return rc;
+    CK(cudaEventRecord(h->ev[0], h->st));
     CK(cudaEventRecord(h->ev[1], h->st));
-    const size_t n = (size_t)(d.lmax - d.lmin + 1) * NCOEF * d.nw;
+    rc = enqueue_solve(h);
+    if (rc) return rc;
+    CK(cudaEventRecord(h->ev[2], h->st));
+    CK(cudaEventRecord(h->ev[3], h->st));
+    const size_t n = (size_t)(ev->lmax - ev->lmin + 1) * NCOEF * ev->nw;
     if (coef) CK(cudaMemcpyAsync(coef, h->coef.p, n * sizeof(cd), cudaMemcpyDeviceToHost, h->st));
-    rc = finish_solve_stage(h, d);
-    cudaEventElapsedTime(&h->ms[1], h->ev[0], h->ev[1]);
+    rc = finish(h, true, false);
+    h->has_spectra = false;
     return rc;
 }
 
@@ -319,6 +574,7 @@ int ysg_legendre_table(ysg_handle* h, int nr, int lmax, const double* delta, con
                        h->leg.as<double>(), h->st));
     CK(cudaMemcpyAsync(table, h->leg.p, nt * sizeof(double), cudaMemcpyDeviceToHost, h->st));
     CK(cudaStreamSynchronize(h->st));
+    h->has_spectra = h->ev_ready = false;
     return YSG_OK;
 }
 
@@ -327,154 +583,78 @@ int ysg_event_spectra(ysg_handle* h, const ysg_event* ev, double* ur, double* ut
     int rc = check_event(h, ev);
     if (rc) return rc;
     cudaSetDevice(h->device);
-    EventDev d = make_event(h, ev);
-    const int nr = ev->nr, nw = ev->nw;
-    h->has_spectra = false;
-    // host tables: cos/sin of delta, e^{i m azst} (yspec.f90:173-174, :331, :414)
-    std::vector<double> ct(std::max(nr, 1)), stv(std::max(nr, 1));
-    std::vector<cd> E((size_t)std::max(nr, 1) * 5);
-    for (int k = 0; k < nr; k++) {
-        ct[k] = std::cos(ev->delta[k]);
-        stv[k] = std::sin(ev->delta[k]);
-        cd eia = mk(std::cos(ev->azst[k]), std::sin(ev->azst[k]));
-        for (int m = -2; m <= 2; m++) E[(size_t)k * 5 + (m + 2)] = cpowi(eia, m);
-    }
-    const size_t nspec = (size_t)nw * std::max(nr, 1);
-    CK(h->spec.ensure(3 * nspec * sizeof(cd)));
-    cd* d_ur = h->spec.as<cd>();
-    cd* d_ut = d_ur + nspec;
-    cd* d_up = d_ut + nspec;
-    if (nr > 0) {
-        CK(h->delta.ensure((size_t)nr * sizeof(double)));
-        CK(h->ct.ensure((size_t)nr * sizeof(double)));
-        CK(h->stv.ensure((size_t)nr * sizeof(double)));
-        CK(h->E.ensure((size_t)nr * 5 * sizeof(cd)));
-        CK(h->leg.ensure((size_t)(ev->lmax + 1) * nr * 8 * sizeof(double)));
-        CK(cudaMemcpyAsync(h->delta.p, ev->delta, (size_t)nr * sizeof(double), cudaMemcpyHostToDevice, h->st));
-        CK(cudaMemcpyAsync(h->ct.p, ct.data(), (size_t)nr * sizeof(double), cudaMemcpyHostToDevice, h->st));
-        CK(cudaMemcpyAsync(h->stv.p, stv.data(), (size_t)nr * sizeof(double), cudaMemcpyHostToDevice, h->st));
-        CK(cudaMemcpyAsync(h->E.p, E.data(), (size_t)nr * 5 * sizeof(cd), cudaMemcpyHostToDevice, h->st));
-    }
-    CK(cudaEventRecord(h->ev[0], h->st));
-    CK(launch_legendre(nr, ev->lmax, h->delta.as<double>(), h->ct.as<double>(), h->stv.as<double>(),
-                       h->leg.as<double>(), h->st));
-    CK(cudaEventRecord(h->ev[1], h->st));
-    rc = run_solve_stage(h, d);
+    h->has_spectra = h->tm_ready = false;
+    rc = upload_event(h, ev);
     if (rc) return rc;
-    CK(cudaEventRecord(h->ev[2], h->st));
-    CK(launch_lsum(nw, nr, ev->lmin, ev->lmax, h->coef.as<cd>(), h->leg.as<double>(),
-                   h->E.as<cd>(), d_ur, d_ut, d_up, h->st));
-    CK(cudaEventRecord(h->ev[3], h->st));
+    rc = enqueue_spectra(h);
+    if (rc) return rc;
+    const int nr = ev->nr, nw = ev->nw;
+    const size_t nspec = (size_t)nw * std::max(nr, 1);
+    const cd* d_ur = h->spec.as<cd>();
     const size_t nb = (size_t)nw * nr * sizeof(cd);
     if (ur && nr > 0) CK(cudaMemcpyAsync(ur, d_ur, nb, cudaMemcpyDeviceToHost, h->st));
-    if (ut && nr > 0) CK(cudaMemcpyAsync(ut, d_ut, nb, cudaMemcpyDeviceToHost, h->st));
-    if (up && nr > 0) CK(cudaMemcpyAsync(up, d_up, nb, cudaMemcpyDeviceToHost, h->st));
-    rc = finish_solve_stage(h, d);
-    cudaEventElapsedTime(&h->ms[0], h->ev[0], h->ev[1]);
-    cudaEventElapsedTime(&h->ms[1], h->ev[1], h->ev[2]);
-    cudaEventElapsedTime(&h->ms[2], h->ev[2], h->ev[3]);
-    if (rc) return rc;
-    h->has_spectra = true;
-    h->last_nw = nw;
-    h->last_nr = nr;
-    return YSG_OK;
+    if (ut && nr > 0) CK(cudaMemcpyAsync(ut, d_ur + nspec, nb, cudaMemcpyDeviceToHost, h->st));
+    if (up && nr > 0) CK(cudaMemcpyAsync(up, d_ur + 2 * nspec, nb, cudaMemcpyDeviceToHost, h->st));
+    return finish(h, true, false);
 }
 
-int ysg_trace_rows(const ysg_time* tm)
-{
-    if (!tm) return 0;
-    int nout = tm->nt;
-    for (int i = 1; i <= tm->nt; i++)
-        if ((double)(i - 1) * tm->dt > tm->tout) {
-            nout = i;
-            break;
-        }
-    return nout;
-}
-
-int ysg_event_traces(ysg_handle* h, const ysg_time* tm, double* out, int* nout_p)
+int ysg_event_traces(ysg_handle* h, const ysg_time* tm, double* out, int* nout)
 {
     if (!h || !tm) return YSG_ERR_ARG;
-    if (!h->has_spectra) return YSG_ERR_NO_SPECTRA;
-    const int n = tm->nt, nr = tm->nr;
-    if (n < 4 || (n & (n - 1)) || n > (1 << 20)) return YSG_ERR_ARG;
-    if (nr != h->last_nr || tm->i2 - tm->i1 + 1 != h->last_nw || tm->i1 < 1) return YSG_ERR_ARG;
-    if (nr > 0 && (!tm->azep || !out)) return YSG_ERR_ARG;
+    if (!h->has_spectra || !h->ev_ready) return YSG_ERR_NO_SPECTRA;
+    if (tm->nr != h->p_nr) return YSG_ERR_ARG;
+    if (tm->nr > 0 && !out) return YSG_ERR_ARG;
     cudaSetDevice(h->device);
-    const int nout = ysg_trace_rows(tm);
-    if (nout_p) *nout_p = nout;
-    if (nr == 0) return YSG_OK;
-    int p = 0;
-    while ((1 << p) < n) p++;
-    // taper (module_fourier.f90:96-116), twiddles with pi_d, e^{eps t}, rotation
-    const double pi_d = (double)3.14159265358979323846f;
-    std::vector<double> filt((size_t)n / 2 + 1, 1.0), expt(nout), cs(2 * (size_t)nr);
-    const double w1 = tm->f11, w2 = tm->f12, w3 = tm->f21, w4 = tm->f22;
-    if (!(w1 == 0.0 && w2 == 0.0 && w3 == 0.0 && w4 == 0.0)) {
-        double f = 0.0;
-        for (int i = 1; i <= n / 2 + 1; i++) {
-            double w = (double)(i - 1) * tm->df;
-            if (w < w1) f = 0.0;
-            else if (w >= w1 && w < w2) f = 0.5 * (1.0 - std::cos(pi_d * (w - w1) / (w2 - w1)));
-            else if (w >= w2 && w < w3) f = 1.0;
-            else if (w >= w3 && w < w4) f = 0.5 * (1.0 - std::cos(pi_d * (w4 - w) / (w4 - w3)));
-            else if (w >= w4) f = 0.0;
-            filt[(size_t)i - 1] = f;
-        }
-    }
-    std::vector<cd> tw((size_t)n / 2);
-    const double dth = pi_d / (double)(n / 2);
-    for (int m = 0; m < n / 2; m++) {
-        double a = (double)m * dth;
-        tw[(size_t)m] = mk(std::cos(a), std::sin(a));
-    }
-    for (int i = 0; i < nout; i++) expt[(size_t)i] = std::exp(tm->ep * ((double)i * tm->dt));
-    for (int k = 0; k < nr; k++) {
-        cs[2 * (size_t)k] = std::cos(tm->azep[k]);
-        cs[2 * (size_t)k + 1] = std::sin(tm->azep[k]);
-    }
-    CK(h->filt.ensure(filt.size() * sizeof(double)));
-    CK(h->tw.ensure(tw.size() * sizeof(cd)));
-    CK(h->expt.ensure(expt.size() * sizeof(double)));
-    CK(h->cs.ensure(cs.size() * sizeof(double)));
-    CK(h->scratch.ensure(ifft_scratch_bytes(n, nr)));
-    const size_t nout_bytes = (size_t)nout * 4 * nr * sizeof(double);
-    CK(h->out.ensure(nout_bytes));
-    CK(cudaMemcpyAsync(h->filt.p, filt.data(), filt.size() * sizeof(double), cudaMemcpyHostToDevice, h->st));
-    CK(cudaMemcpyAsync(h->tw.p, tw.data(), tw.size() * sizeof(cd), cudaMemcpyHostToDevice, h->st));
-    CK(cudaMemcpyAsync(h->expt.p, expt.data(), expt.size() * sizeof(double), cudaMemcpyHostToDevice, h->st));
-    CK(cudaMemcpyAsync(h->cs.p, cs.data(), cs.size() * sizeof(double), cudaMemcpyHostToDevice, h->st));
-    TraceDev td{};
-    td.nt = n;
-    td.i1 = tm->i1;
-    td.i2 = tm->i2;
-    td.nw = h->last_nw;
-    td.nr = nr;
-    td.nout = nout;
-    td.log2n = p;
-    td.b1 = 1 << ((p + 1) / 2);
-    td.dt = tm->dt;
-    td.scale = tm->dt * (double)n;
-    td.t_norm = tm->t_norm;
-    td.amp_norm = tm->amp_norm;
-    const size_t nspec = (size_t)h->last_nw * nr;
-    const cd* d_ur = h->spec.as<cd>();
-    CK(cudaEventRecord(h->ev[3], h->st));
-    CK(launch_ifft(td, d_ur, d_ur + nspec, d_ur + 2 * nspec, h->filt.as<double>(), h->tw.as<cd>(),
-                   h->expt.as<double>(), h->cs.as<double>(), h->scratch.as<cd>(), h->out.as<double>(),
-                   h->st));
-    CK(cudaEventRecord(h->ev[4], h->st));
-    CK(cudaMemcpyAsync(out, h->out.p, nout_bytes, cudaMemcpyDeviceToHost, h->st));
-    CK(cudaStreamSynchronize(h->st));
-    cudaEventElapsedTime(&h->ms[3], h->ev[3], h->ev[4]);
-    return YSG_OK;
+    int rc = upload_time(h, tm, h->pev.nw);
+    if (rc) return rc;
+    rc = enqueue_traces(h);
+    if (rc) return rc;
+    rc = copy_out(h, out, nout);
+    if (rc) return rc;
+    return finish(h, false, true);
+}
+
+int ysg_event_prepare(ysg_handle* h, const ysg_event* ev, const ysg_time* tm)
+{
+    int rc = check_event(h, ev);
+    if (rc) return rc;
+    if (!tm || tm->nr != ev->nr) return YSG_ERR_ARG;
+    cudaSetDevice(h->device);
+    h->has_spectra = h->ev_ready = h->tm_ready = false;
+    h->h2d = h->d2h = 0.0;
+    rc = upload_event(h, ev);
+    if (rc) return rc;
+    return upload_time(h, tm, ev->nw);
+}
+
+int ysg_event_execute(ysg_handle* h)
+{
+    if (!h) return YSG_ERR_ARG;
+    if (!h->ev_ready || !h->tm_ready) return YSG_ERR_NO_SPECTRA;
+    cudaSetDevice(h->device);
+    int rc = enqueue_spectra(h);
+    if (rc) return rc;
+    return enqueue_traces(h);
+}
+
+int ysg_event_fetch(ysg_handle* h, double* out, int* nout)
+{
+    if (!h) return YSG_ERR_ARG;
+    if (!h->ev_ready || !h->tm_ready) return YSG_ERR_NO_SPECTRA;
+    cudaSetDevice(h->device);
+    int rc = copy_out(h, out, nout);
+    if (rc) return rc;
+    return finish(h, true, true);
 }
 
 int ysg_event_run(ysg_handle* h, const ysg_event* ev, const ysg_time* tm, double* out, int* nout)
 {
-    int rc = ysg_event_spectra(h, ev, nullptr, nullptr, nullptr);
+    int rc = ysg_event_prepare(h, ev, tm);
     if (rc) return rc;
-    return ysg_event_traces(h, tm, out, nout);
+    if (tm->nr > 0 && !out) return YSG_ERR_ARG;
+    rc = ysg_event_execute(h);
+    if (rc) return rc;
+    return ysg_event_fetch(h, out, nout);
 }
 
 int ysg_batch_run(ysg_handle* h, int nev, const ysg_event* evs, const ysg_time* tms, double** outs,
@@ -485,6 +665,14 @@ int ysg_batch_run(ysg_handle* h, int nev, const ysg_event* evs, const ysg_time* 
         int rc = ysg_event_run(h, &evs[e], &tms[e], outs[e], nouts ? &nouts[e] : nullptr);
         if (rc) return rc;
     }
+    return YSG_OK;
+}
+
+int ysg_last_bytes(ysg_handle* h, double* h2d, double* d2h)
+{
+    if (!h) return YSG_ERR_ARG;
+    if (h2d) *h2d = h->h2d;
+    if (d2h) *d2h = h->d2h;
     return YSG_OK;
 }
 

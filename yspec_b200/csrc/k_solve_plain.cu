@@ -28,6 +28,8 @@ __global__ void __launch_bounds__(128) k_solve_plain(const Knot* __restrict__ kn
     c.kn = kn;
     c.mh = mhs;
     c.ats = (double)ev.ats;
+    c.kb = nullptr;
+    c.ks = 0;
     for (int q = 0; q < NSYS; q++) c.nst[q] = 0;
     if (gid < total) {
         const int li = (int)(gid / ev.nw);

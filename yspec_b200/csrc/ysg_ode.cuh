@@ -15,7 +15,23 @@
 #pragma once
 #include "ysg_model.cuh"
 
+// Two builds of the solver code exist: the plain form keeps the Cash-Karp
+// stage vectors in per-thread arrays (the compiler places them in local
+// memory); with YSG_SMEM_STAGES the stage vectors live in a per-thread slab
+// of shared memory and only y and the stage input stay in registers.  Each
+// form gets its own inline namespace so the two translation units never
+// share a definition.
+#ifndef YSG_SMEM_STAGES
+#define YSG_SMEM_STAGES 0
+#endif
+#if YSG_SMEM_STAGES
+#define YSG_VARIANT v_smem
+#else
+#define YSG_VARIANT v_local
+#endif
+
 namespace ysg {
+inline namespace YSG_VARIANT {
 
 // nrtype.f90:18-27: pi_d and twopi_d are single-precision literals.
 constexpr double PI_D = (double)3.14159265358979323846f;
@@ -36,6 +52,8 @@ struct Ctx {
     const ModelHdr* mh;
     int ll, llp1, il;
     unsigned nst[NSYS];
+    cd* kb;          // shared-memory stage slab of this thread (smem form)
+    int ks;          // stride between slab entries, in complex elements
     double zeta, zeta2, zeta2m2, szeta2m2, nu, dr, ats;
     cd omega, omega2, omegai, omegai2, lno;
 };
@@ -225,7 +243,8 @@ __device__ __forceinline__ FluidCoef fluid_amat(const Ctx& c, double rr)
 // ---------------------------------------------------------------------------
 struct TorSys {
     static constexpr int N = 2, CLS = 0;
-    __device__ static __forceinline__ void f(const Ctx& c, double r, const cd* y, cd* d)
+    template <class Out>
+    __device__ static __forceinline__ void f(const Ctx& c, double r, const cd* y, Out d)
     {
         TorCoef a = tor_amat(c, r);       // module_int.f90:168-184
         d[0] = a.t * y[0] + a.k * y[1];
@@ -235,7 +254,8 @@ struct TorSys {
 
 struct RadSys {
     static constexpr int N = 2, CLS = 1;
-    __device__ static __forceinline__ void f(const Ctx& c, double r, const cd* y, cd* d)
+    template <class Out>
+    __device__ static __forceinline__ void f(const Ctx& c, double r, const cd* y, Out d)
     {
         RadCoef a = rad_amat(c, r);       // module_int.f90:357-392
         d[0] = a.t * y[0] + a.k * y[1];
@@ -246,7 +266,8 @@ struct RadSys {
 // module_int.f90:818-871 sph_minors_solid_derivs
 struct MinorSolidG {
     static constexpr int N = 14, CLS = 6;
-    __device__ static __forceinline__ void f(const Ctx& c, double r, const cd* m, cd* d)
+    template <class Out>
+    __device__ static __forceinline__ void f(const Ctx& c, double r, const cd* m, Out d)
     {
         SolidCoef a = solid_amat<2>(c, r);
         cd a123 = a.t11 + (a.t22 + a.t33), a126 = a.t11 + (a.t22 - a.t33);
@@ -282,7 +303,8 @@ struct MinorSolidG {
 template <int KIND>
 struct MinorSolidNC {
     static constexpr int N = 5, CLS = 4;
-    __device__ static __forceinline__ void f(const Ctx& c, double r, const cd* m, cd* d)
+    template <class Out>
+    __device__ static __forceinline__ void f(const Ctx& c, double r, const cd* m, Out d)
     {
         SolidCoef a = solid_amat<KIND>(c, r);
         cd a11 = a.t11 + a.t22, a22 = a.t11 - a.t22;
@@ -297,7 +319,8 @@ struct MinorSolidNC {
 // module_int.f90:941-967 sph_minors_fluid_derivs
 struct MinorFluidG {
     static constexpr int N = 5, CLS = 5;
-    __device__ static __forceinline__ void f(const Ctx& c, double r, const cd* m, cd* d)
+    template <class Out>
+    __device__ static __forceinline__ void f(const Ctx& c, double r, const cd* m, Out d)
     {
         FluidCoef a = fluid_amat<2>(c, r);
         cd tp = a.t11 + a.t22, tm = a.t11 - a.t22;
@@ -313,7 +336,8 @@ struct MinorFluidG {
 template <int KIND>
 struct MinorFluidNC {
     static constexpr int N = 2, CLS = 2;
-    __device__ static __forceinline__ void f(const Ctx& c, double r, const cd* m, cd* d)
+    template <class Out>
+    __device__ static __forceinline__ void f(const Ctx& c, double r, const cd* m, Out d)
     {
         FluidCoef a = fluid_amat<KIND>(c, r);
         d[0] = a.t11 * m[0] + a.k11 * m[1];
@@ -324,7 +348,8 @@ struct MinorFluidNC {
 // module_int.f90:1016-1057 sph_bvec_solid_derivs
 struct BvecSolidG {
     static constexpr int N = 14, CLS = 7;
-    __device__ static __forceinline__ void f(const Ctx& c, double r, const cd* b, cd* d)
+    template <class Out>
+    __device__ static __forceinline__ void f(const Ctx& c, double r, const cd* b, Out d)
     {
         SolidCoef a = solid_amat<2>(c, r);
         const cd t11 = a.t11, t12 = a.t12, k11 = a.k11, k22 = a.k22;
@@ -358,7 +383,8 @@ struct BvecSolidG {
 template <int KIND>
 struct BvecSolidNC {
     static constexpr int N = 4, CLS = 3;
-    __device__ static __forceinline__ void f(const Ctx& c, double r, const cd* b, cd* d)
+    template <class Out>
+    __device__ static __forceinline__ void f(const Ctx& c, double r, const cd* b, Out d)
     {
         SolidCoef a = solid_amat<KIND>(c, r);
         d[0] = -(a.s11 * b[2]) - a.s12 * b[3] - a.t11 * b[0] - a.t21 * b[1];
@@ -409,6 +435,97 @@ __device__ __forceinline__ void rkck_step(const Ctx& c, cd* y, double x, double 
         y[i] = y[i] + h * (c1 * k1[i] + c3 * k3[i] + c4 * k4[i] + c6 * k2[i]);
 }
 
+// Shared-memory form of the same step: stage vectors go to the thread's
+// slab (entry (s*N + i) at kb[(s*N + i) * ks]) as the right-hand side
+// produces them, so only y and the stage input are held in registers.
+struct SlabOut {
+    cd* p;
+    int ks;
+    __device__ __forceinline__ cd& operator[](int i) const { return p[i * ks]; }
+};
+
+// Cash-Karp tableau (module_int.f90:2039-2049) for the looped step.
+__constant__ double ck_a[6] = {0.0, 0.2, 0.3, 0.6, 1.0, 0.875};
+__constant__ double ck_b[6][5] = {
+    {0.0, 0.0, 0.0, 0.0, 0.0},
+    {0.2, 0.0, 0.0, 0.0, 0.0},
+    {3.0 / 40.0, 9.0 / 40.0, 0.0, 0.0, 0.0},
+    {0.3, -0.9, 1.2, 0.0, 0.0},
+    {-11.0 / 54.0, 2.5, -70.0 / 27.0, 35.0 / 27.0, 0.0},
+    {1631.0 / 55296.0, 175.0 / 512.0, 575.0 / 13824.0, 44275.0 / 110592.0, 253.0 / 4096.0}};
+
+// The step as a runtime loop over the six stages with one copy of the
+// right-hand side: the unrolled form inlines six 14-component RHS bodies,
+// which overflows the instruction cache and leaves warps waiting on
+// instruction fetch.  Stage vectors live in the thread's shared-memory slab;
+// the sixth stage reuses the second stage's entries.
+template <class Sys>
+__device__ __forceinline__ void rkck_step_loop(const Ctx& c, cd* y, double x, double h)
+{
+    constexpr int N = Sys::N;
+    constexpr double c1 = 37.0 / 378.0, c3 = 250.0 / 621.0, c4 = 125.0 / 594.0,
+                     c6 = 512.0 / 1771.0;
+    cd* const kb = c.kb;
+    const int ks = c.ks;
+    cd yt[N];
+#pragma unroll 1
+    for (int s = 0; s < 6; s++) {
+#pragma unroll
+        for (int i = 0; i < N; i++) yt[i] = y[i];
+        for (int j = 0; j < s; j++) {
+            const double hb = h * ck_b[s][j];
+            const cd* kj = kb + j * N * ks;
+#pragma unroll
+            for (int i = 0; i < N; i++) yt[i] += hb * kj[i * ks];
+        }
+        const int slot = (s == 5) ? 1 : s;
+        Sys::f(c, x + ck_a[s] * h, yt, SlabOut{kb + slot * N * ks, ks});
+    }
+#pragma unroll
+    for (int i = 0; i < N; i++)
+        y[i] = y[i] + h * (c1 * kb[i * ks] + c3 * kb[(2 * N + i) * ks] + c4 * kb[(3 * N + i) * ks] +
+                           c6 * kb[(N + i) * ks]);
+}
+
+template <class Sys>
+__device__ __forceinline__ void rkck_step_smem(const Ctx& c, cd* y, double x, double h)
+{
+    constexpr int N = Sys::N;
+    constexpr double a2 = 0.2, a3 = 0.3, a4 = 0.6, a5 = 1.0, a6 = 0.875;
+    constexpr double b21 = 0.2, b31 = 3.0 / 40.0, b32 = 9.0 / 40.0;
+    constexpr double b41 = 0.3, b42 = -0.9, b43 = 1.2;
+    constexpr double b51 = -11.0 / 54.0, b52 = 2.5, b53 = -70.0 / 27.0, b54 = 35.0 / 27.0;
+    constexpr double b61 = 1631.0 / 55296.0, b62 = 175.0 / 512.0, b63 = 575.0 / 13824.0,
+                     b64 = 44275.0 / 110592.0, b65 = 253.0 / 4096.0;
+    constexpr double c1 = 37.0 / 378.0, c3 = 250.0 / 621.0, c4 = 125.0 / 594.0,
+                     c6 = 512.0 / 1771.0;
+    cd* const kb = c.kb;
+    const int ks = c.ks;
+    const SlabOut K0{kb, ks}, K1{kb + N * ks, ks}, K2{kb + 2 * N * ks, ks};
+    const SlabOut K3{kb + 3 * N * ks, ks}, K4{kb + 4 * N * ks, ks};
+    cd yt[N];
+    Sys::f(c, x, y, K0);
+#pragma unroll
+    for (int i = 0; i < N; i++) yt[i] = y[i] + (b21 * h) * K0[i];
+    Sys::f(c, x + a2 * h, yt, K1);
+#pragma unroll
+    for (int i = 0; i < N; i++) yt[i] = y[i] + h * (b31 * K0[i] + b32 * K1[i]);
+    Sys::f(c, x + a3 * h, yt, K2);
+#pragma unroll
+    for (int i = 0; i < N; i++) yt[i] = y[i] + h * (b41 * K0[i] + b42 * K1[i] + b43 * K2[i]);
+    Sys::f(c, x + a4 * h, yt, K3);
+#pragma unroll
+    for (int i = 0; i < N; i++)
+        yt[i] = y[i] + h * (b51 * K0[i] + b52 * K1[i] + b53 * K2[i] + b54 * K3[i]);
+    Sys::f(c, x + a5 * h, yt, K4);
+#pragma unroll
+    for (int i = 0; i < N; i++)
+        yt[i] = y[i] + h * (b61 * K0[i] + b62 * K1[i] + b63 * K2[i] + b64 * K3[i] + b65 * K4[i]);
+    Sys::f(c, x + a6 * h, yt, K1);   // the sixth stage reuses k2's entries
+#pragma unroll
+    for (int i = 0; i < N; i++) y[i] = y[i] + h * (c1 * K0[i] + c3 * K2[i] + c4 * K3[i] + c6 * K1[i]);
+}
+
 template <int N>
 __device__ __forceinline__ void rescale(cd* y, int* scale)
 {
@@ -430,10 +547,23 @@ __device__ __forceinline__ void rescale(cd* y, int* scale)
 }
 
 // module_int.f90:1847-1968 yint
+#if YSG_SMEM_STAGES
+#define YSG_YINT_ATTR __noinline__
+#else
+#define YSG_YINT_ATTR
+#endif
+
 template <class Sys>
-__device__ void yint(Ctx& c, int i1, int i2, double r1, double r2, cd* y, int* scale)
+__device__ YSG_YINT_ATTR void yint(Ctx& c, int i1, int i2, double r1, double r2, cd* yio, int* scale)
 {
     if (r2 == r1) return;
+#if YSG_SMEM_STAGES
+    cd y[Sys::N];
+#pragma unroll
+    for (int k = 0; k < Sys::N; k++) y[k] = yio[k];
+#else
+    cd* y = yio;
+#endif
     const bool up = r2 > r1;
     const Knot* kn = c.kn;
     const int di = up ? 1 : -1;
@@ -456,10 +586,18 @@ __device__ void yint(Ctx& c, int i1, int i2, double r1, double r2, cd* y, int* s
         c.nst[Sys::CLS] += (unsigned)(n - 1);
         for (int j = 1; j <= n - 1; j++) {
             double rr = __dadd_rn(rr1, __dmul_rn((double)(j - 1), drr));
+#if YSG_SMEM_STAGES
+            rkck_step_loop<Sys>(c, y, rr, drr);
+#else
             rkck_step<Sys>(c, y, rr, drr);
+#endif
             if (scale) rescale<Sys::N>(y, scale);
         }
     }
+#if YSG_SMEM_STAGES
+#pragma unroll
+    for (int k = 0; k < Sys::N; k++) yio[k] = y[k];
+#endif
 }
 
 // ---------------------------------------------------------------------------
@@ -867,4 +1005,5 @@ __device__ __forceinline__ void sph_ysol_ngcow(const cd* m, const cd* b, cd* y)
 #undef YS
 #undef YB
 
+}  // inline namespace
 }  // namespace ysg

@@ -9,6 +9,7 @@
 #include "ysg_ode.cuh"
 
 namespace ysg {
+inline namespace YSG_VARIANT {
 
 __device__ __forceinline__ double huge_pow(int k)
 {
@@ -565,4 +566,5 @@ __device__ inline void pair_spheroidal(Ctx& c, const EventDev& ev, int l, int j,
     }
 }
 
+}  // inline namespace
 }  // namespace ysg

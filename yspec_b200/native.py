@@ -72,8 +72,10 @@ class YshNorms(C.Structure):
 # Symbols declared in include/*.h, checked by the CPU test suite.
 EXPORTS = [
     "ysg_create", "ysg_model_upload", "ysg_event_spectra", "ysg_event_traces", "ysg_trace_rows",
-    "ysg_event_run", "ysg_batch_run", "ysg_event_coef", "ysg_legendre_table", "ysg_set_solver",
-    "ysg_last_timings", "ysg_last_work", "ysg_status_string", "ysg_destroy",
+    "ysg_event_run", "ysg_event_prepare", "ysg_event_execute", "ysg_event_fetch", "ysg_get_stream",
+    "ysg_batch_run", "ysg_event_coef", "ysg_legendre_table", "ysg_set_solver",
+    "ysg_last_timings", "ysg_last_work", "ysg_last_bytes", "ysg_fp64_peak", "ysg_status_string",
+    "ysg_destroy",
     "ysh_norms_get", "ysh_read_params", "ysh_free_params", "ysh_read_model", "ysh_model_view",
     "ysh_model_nknot", "ysh_model_array", "ysh_free_model", "ysh_event_setup", "ysh_free_event",
     "ysh_write_traces", "ysh_run", "ysh_free", "ysh_status_string",
@@ -104,6 +106,10 @@ def lib() -> C.CDLL:
     L.ysg_event_traces.argtypes = [vp, C.POINTER(YsgTime), _dp, C.POINTER(C.c_int)]
     L.ysg_trace_rows.argtypes = [C.POINTER(YsgTime)]
     L.ysg_event_run.argtypes = [vp, C.POINTER(YsgEvent), C.POINTER(YsgTime), _dp, C.POINTER(C.c_int)]
+    L.ysg_event_prepare.argtypes = [vp, C.POINTER(YsgEvent), C.POINTER(YsgTime)]
+    L.ysg_event_execute.argtypes = [vp]
+    L.ysg_event_fetch.argtypes = [vp, _dp, C.POINTER(C.c_int)]
+    L.ysg_get_stream.argtypes = [vp, C.POINTER(vp)]
     L.ysg_batch_run.argtypes = [vp, C.c_int, C.POINTER(YsgEvent), C.POINTER(YsgTime),
                                 C.POINTER(_dp), C.POINTER(C.c_int)]
     L.ysg_event_coef.argtypes = [vp, C.POINTER(YsgEvent), _dp]
@@ -111,6 +117,8 @@ def lib() -> C.CDLL:
     L.ysg_set_solver.argtypes = [vp, C.c_int]
     L.ysg_last_timings.argtypes = [vp, C.POINTER(C.c_float)]
     L.ysg_last_work.argtypes = [vp, _dp, _dp]
+    L.ysg_last_bytes.argtypes = [vp, _dp, _dp]
+    L.ysg_fp64_peak.argtypes = [C.c_int, _dp]
     L.ysg_status_string.argtypes = [C.c_int]
     L.ysg_status_string.restype = C.c_char_p
     L.ysg_destroy.argtypes = [vp]
