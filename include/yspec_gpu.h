@@ -125,6 +125,24 @@ int ysg_event_fetch(ysg_handle *h, double *out, int *nout);
 /* The handle's cudaStream_t, as a void pointer. */
 int ysg_get_stream(ysg_handle *h, void **stream);
 
+/* Time series from device-resident spectra without any device allocation.
+ * No counterpart in the reference: it exists for callers that cannot let
+ * the library call cudaMalloc (a host that owns the whole GPU memory
+ * through its own pool, or code where an allocation would synchronise the
+ * device).  Same result as ysg_event_traces; d_ur/d_ut/d_up are complex
+ * (nw, nr) device arrays, d_azep has nr entries, d_out receives
+ * (nout, 4, nr); tm->azep is not used.  Work is enqueued on `stream`
+ * (a cudaStream_t, or NULL) and the call returns without waiting.
+ * Intermediate rows live in one 16 MiB array compiled into the library and
+ * held by every GPU that loads it until exit; nt is limited to 262144
+ * (YSG_ERR_LIMIT beyond).  All calls share that array: calls that overlap
+ * on the GPU race and must be serialised.  The first call on each device
+ * looks up the array's device address and should come before any stream
+ * capture. */
+int ysg_traces_noalloc(const ysg_time *tm, const double *d_ur, const double *d_ut,
+                       const double *d_up, const double *d_azep, double *d_out, int *nout,
+                       void *stream);
+
 /* Several events through the batched persistent solver: one launch per
  * stage for all events, CUDA-graph captured.  outs[e] receives the traces of
  * event e as ysg_event_traces does; nouts[e] its row count.  Events share

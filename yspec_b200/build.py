@@ -41,6 +41,7 @@ SOURCES = [
     CSRC / "k_lsum.cu",
     CSRC / "k_ifft.cu",
     CSRC / "k_peak.cu",
+    CSRC / "k_ifft_noalloc.cu",
     CSRC / "host" / "ysh_host.cpp",
 ]
 
