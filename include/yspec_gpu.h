@@ -66,7 +66,10 @@ typedef struct {
     int is, ir;                      /* find_radius_index of source, receiver */
     int ats, grav, out, cor;         /* switches, yspec.f90:100-103 */
     int nr;                          /* receivers */
-    double wmin, dw, ep;             /* omega_j = wmin + (j-1) dw - i ep */
+    int jofs, jstride;               /* frequency shard: the event's j-th frequency is
+                                        omega at index jofs + (j-1) jstride of the full
+                                        band (0 and 1 for the whole band) */
+    double wmin, dw, ep;             /* omega_k = wmin + k dw - i ep, k = jofs + (j-1) jstride */
     double rs, rr;                   /* normalised source / receiver radius */
     double mm[6];                    /* moment tensor / moment_norm */
     const double *delta;             /* nr epicentral angles (delaz), rad */

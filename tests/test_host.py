@@ -1,0 +1,155 @@
+"""Host side of the yspec program (C++ mirror of the Fortran host) on CPU.
+
+The host code that stays on the CPU (parameter file, model deck with its
+normalisation, splines and gravity, event set-up, writer) must agree bit for
+bit with the oracle, and the library must export every C-ABI symbol the
+headers declare.  No GPU is needed; device entry points report NO_DEVICE.
+"""
+import ctypes as C
+import re
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import yo
+from conftest import ROOT, has_gpu
+from yspec_b200 import Event, Model, Params, native as N, workloads as W
+
+DECKS = ["model200.deck", "model400.deck", "model200_ocean.deck", "model200_fic.deck"]
+ARRAYS = ["r", "rho", "rho_cs", "acon", "acon_cs", "ccon", "ccon_cs", "fcon", "fcon_cs", "lcon",
+          "lcon_cs", "ncon", "ncon_cs", "kappa", "kappa_cs", "mu", "mu_cs", "qkappa", "qkappa_cs",
+          "qmu", "qmu_cs", "grav", "grav_cs", "xlam", "xlam_cs", "xa2", "xa2_cs", "alpha", "beta"]
+
+
+def test_library_exports_every_declared_symbol():
+    names = set()
+    for h in (ROOT / "include").glob("*.h"):
+        txt = re.sub(r"/\*.*?\*/", "", h.read_text(), flags=re.S)
+        names |= set(re.findall(r"\b(ys[gh]_[a-z0-9_]+)\s*\(", txt))
+    assert len(names) > 30
+    L = N.lib()
+    missing = [n for n in sorted(names) if not hasattr(L, n)]
+    assert not missing, missing
+
+
+@pytest.mark.parametrize("deck", DECKS)
+def test_model_bit_identical_to_oracle(workdir, deck):
+    p = W.config("c1", seed=2, model_file=str(W.GOLDEN / deck), depth_r=3.0)[0]
+    P = yo.Problem(p.write(workdir / "m.in"))
+    m = Model(p.model_file)
+    for name in ARRAYS:
+        np.testing.assert_array_equal(m.array(name), P.array(name), err_msg=name)
+    v = m.view()
+    assert (v.nknot, v.nic, v.noc, v.nsl, v.ocean, v.fic) == (
+        P.model.nknot, P.model.nic, P.model.noc, P.model.nsl, P.model.ocean, P.model.fic)
+    assert v.tref == P.model.tref
+
+
+@pytest.mark.parametrize("cfg", ["c1", "c2", "c4"])
+def test_event_setup_bit_identical_to_oracle(workdir, cfg):
+    p = W.config(cfg, seed=9)[0]
+    pf = p.write(workdir / "e.in")
+    P = yo.Problem(pf)
+    ev = Event(Model(p.model_file), Params(pf))
+    g = P.grid
+    e, t = ev.ev, ev.tm
+    assert (e.nw, e.is_, e.ir, t.nt, t.i1, t.i2) == (g.nw, g.is_, g.ir, g.nt, g.i1, g.i2)
+    assert (e.wmin, e.dw, e.ep, e.rs, e.rr) == (g.wmin, g.dw, g.ep, g.rs, g.rr)
+    assert (t.df, t.dt, t.tout, t.f11, t.f12, t.f21, t.f22) == (g.df, g.dt, g.tout, g.f11, g.f12, g.f21, g.f22)
+    assert list(e.mm) == list(g.mm)
+    d, azep, azst = P.geometry()
+    nr = ev.nr
+    np.testing.assert_array_equal(np.ctypeslib.as_array(ev.raw.delta, (nr,)), d)
+    np.testing.assert_array_equal(np.ctypeslib.as_array(ev.raw.azep, (nr,)), azep)
+    np.testing.assert_array_equal(np.ctypeslib.as_array(ev.raw.azst, (nr,)), azst)
+
+
+def _param_text_variants(model):
+    """Parameter files exercising list-directed reads: comment lines are
+    skipped positionally, a value may sit after blank records, quoted
+    strings may hold '/', an unquoted '/' ends the read."""
+    p = W.Params(model_file=str(model), receivers=[(0.0, 10.0), (-20.5, 33.0), (45.0, -170.0)])
+    base = p.text()
+    blank_before_receivers = base.replace("# receiver latitudes and longitudes\n",
+                                          "# receiver latitudes and longitudes\n \n")
+    return {"plain": base, "blank_records": blank_before_receivers,
+            "slash_prefix": base.replace("  yspec.out", "  run/out.x")}
+
+
+@pytest.mark.parametrize("variant", ["plain", "blank_records", "slash_prefix"])
+def test_params_match_oracle(workdir, variant):
+    txt = _param_text_variants(W.MODEL200)[variant]
+    pf = workdir / "p.in"
+    pf.write_text(txt)
+    P = yo.Problem(pf)
+    got = Params(pf)
+    o = P.params
+    for f in ("ats", "grav", "out", "cor", "lmin", "lmax", "f1", "f2", "tout", "dt", "f11", "f12",
+              "f21", "f22", "depth_s", "lat_s", "lon_s", "depth_r", "nr"):
+        assert getattr(got, f) == getattr(o, f), f
+    assert got.pref_out == o.pref_out.decode() and got.model_file == o.model_file.decode()
+    assert list(got.raw.mm) == list(o.mm)
+    nr = o.nr
+    assert np.ctypeslib.as_array(got.raw.lat_r, (nr,)).tolist() == np.ctypeslib.as_array(o.lat_r, (nr,)).tolist()
+    if variant == "slash_prefix":
+        assert got.pref_out == "run"            # '/' ends a list-directed read
+
+
+def _status(model_file, **over):
+    p = W.Params(model_file=str(model_file), **over)
+    return p
+
+
+@pytest.mark.parametrize("case,status", [
+    (dict(model_file=str(W.GOLDEN / "model200_ocean.deck"), depth_r=0.0), 110),   # receiver in ocean
+    (dict(model_file=str(W.GOLDEN / "model200_ocean.deck"), depth_s=1.0), 108),   # source in ocean
+    (dict(depth_s=7000.0), 107),                                                  # source not in model
+    (dict(fmax=60.0, dt=10.0), 105),                                              # Nyquist below fmax
+])
+def test_stop_conditions(workdir, case, status):
+    p = W.Params(**case)
+    pf = p.write(workdir / "s.in")
+    m = Model(p.model_file)
+    with pytest.raises(N.YspecError) as ei:
+        Event(m, Params(pf))
+    assert ei.value.status == status
+
+
+def test_missing_files(workdir):
+    with pytest.raises(N.YspecError) as ei:
+        Params(workdir / "nope.in")
+    assert ei.value.status == 101
+    with pytest.raises(N.YspecError) as ei:
+        Model(workdir / "nope.deck")
+    assert ei.value.status == 103
+
+
+def test_writer_byte_identical_to_oracle(workdir):
+    rng = np.random.default_rng(0)
+    nout, nr = 7, 12
+    out = rng.normal(size=(nr, 4, nout)) * 10.0 ** rng.integers(-120, 120, size=(nr, 4, nout))
+    out[0, 1, 0] = -0.0
+    out[0, 2, 1] = 0.0
+    out[1, 3, 2] = 9.9999995e-8          # rounds up across a decade
+    out = np.ascontiguousarray(out)
+    (workdir / "a").mkdir()
+    (workdir / "b").mkdir()
+    assert N.lib().ysh_write_traces(str(workdir / "a" / "syn").encode(), N.dptr(out), nout, nr) == 0
+    assert yo.lib().yo_write_traces(str(workdir / "b" / "syn").encode(), yo._p(out), nout, nr) == 0
+    names = sorted(x.name for x in (workdir / "a").iterdir())
+    assert names == sorted(x.name for x in (workdir / "b").iterdir())
+    assert "syn.1" in names and "syn.10" in names and "syn.12" in names
+    for n in names:
+        assert (workdir / "a" / n).read_bytes() == (workdir / "b" / n).read_bytes(), n
+    line = (workdir / "a" / "syn.1").read_text().splitlines()[0]
+    assert len(line) == 60 and line[15:30].strip().startswith("-0.000000E+00")
+
+
+@pytest.mark.skipif(has_gpu(), reason="checks the no-device error path")
+def test_no_device_fails_loudly():
+    from yspec_b200 import Engine
+
+    with pytest.raises(N.YspecError) as ei:
+        Engine(0)
+    assert ei.value.status == 6               # YSG_ERR_NO_DEVICE: no CPU fallback

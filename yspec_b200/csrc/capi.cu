@@ -105,6 +105,7 @@ int check_event(const ysg_handle* h, const ysg_event* ev)
     if (ev->nr > 0 && (!ev->delta || !ev->azst)) return YSG_ERR_ARG;
     if (ev->grav < 0 || ev->grav > 2 || ev->out < 0 || ev->out > 2) return YSG_ERR_ARG;
     if (!(ev->dw > 0.0) || !(ev->wmin > 0.0) || !(ev->ep > 0.0)) return YSG_ERR_ARG;
+    if (ev->jofs < 0 || ev->jstride < 1) return YSG_ERR_ARG;
     return YSG_OK;
 }
 
@@ -121,6 +122,8 @@ EventDev make_event(const ysg_handle* h, const ysg_event* ev)
     d.out = ev->out;
     d.cor = ev->cor;
     d.nr = ev->nr;
+    d.jofs = ev->jofs;
+    d.jstride = ev->jstride;
     d.rs = ev->rs;
     d.rr = ev->rr;
     d.ep = ev->ep;
@@ -160,7 +163,7 @@ cd cpowi(cd a, int m)
 double item_cost(const EventDev& ev, int li, int j0)
 {
     const int l = ev.lmin + li;
-    const double w = ev.wmin + (j0 + 16) * ev.dw;
+    const double w = ev.wmin + (ev.jofs + (j0 + 16) * ev.jstride) * ev.dw;
     const double vref = 1.0;                       // normalised wave speed scale
     double rturn = (l + 0.5) * vref / w;
     if (rturn > 1.0) rturn = 1.0;

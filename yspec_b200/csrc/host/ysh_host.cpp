@@ -529,6 +529,8 @@ int ysh_event_setup(const ysh_model* m, const ysh_params* p, ysh_event* e)
     ev.out = p->out;
     ev.cor = p->cor;
     ev.nr = nr;
+    ev.jofs = 0;
+    ev.jstride = 1;
     ev.wmin = (double)(i1 - 1) * dw;
     ev.dw = dw;
     ev.ep = ep;

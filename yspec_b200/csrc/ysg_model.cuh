@@ -37,7 +37,7 @@ struct ModelHdr {
 // Per-event constants of the (omega,l) loop (yspec.f90:176-261).
 struct EventDev {
     int lmin, lmax, nw, is, ir, ats, grav, out, cor, nr;
-    int pad0, pad1;
+    int jofs, jstride;   // frequency shard: local j -> full-band index jofs + (j-1) jstride
     double rs, rr, ep, wmin, dw, grav_ir;
     double mm[6];
 };

@@ -471,7 +471,8 @@ __device__ inline void source_vector_sph(const Ctx& c, int is, double rs, const 
 __device__ __forceinline__ cd omega_of(const EventDev& ev, int j)
 {
     // w = wmin + (j-1)*dw - i*ep, formed without contraction (yspec.f90:261)
-    return mk(__dadd_rn(ev.wmin, __dmul_rn((double)(j - 1), ev.dw)), -ev.ep);
+    const int k = ev.jofs + (j - 1) * ev.jstride;       // index in the full band
+    return mk(__dadd_rn(ev.wmin, __dmul_rn((double)k, ev.dw)), -ev.ep);
 }
 
 __device__ __forceinline__ cd out_factor(int out, cd w)

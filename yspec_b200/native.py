@@ -28,6 +28,7 @@ class YsgEvent(C.Structure):
     _fields_ = [
         ("lmin", C.c_int), ("lmax", C.c_int), ("nw", C.c_int), ("is_", C.c_int), ("ir", C.c_int),
         ("ats", C.c_int), ("grav", C.c_int), ("out", C.c_int), ("cor", C.c_int), ("nr", C.c_int),
+        ("jofs", C.c_int), ("jstride", C.c_int),
         ("wmin", C.c_double), ("dw", C.c_double), ("ep", C.c_double),
         ("rs", C.c_double), ("rr", C.c_double), ("mm", C.c_double * 6),
         ("delta", _dp), ("azst", _dp),
