@@ -70,7 +70,7 @@ struct ysg_handle {
     cudaEvent_t ev[5] = {};
     int solver = 1;
     // model
-    DevBuf kn;
+    DevBuf kn, sg;
     ModelHdr hdr{};
     std::vector<double> grav_host;   // knot gravity for the tilt correction
     bool has_model = false;
@@ -323,11 +323,11 @@ int enqueue_solve(ysg_handle* h)
     CK(cudaMemsetAsync(h->work.p, 0, NSYS_COUNT * sizeof(unsigned long long), h->st));
     CK(cudaMemsetAsync(h->status.p, 0, sizeof(int), h->st));
     if (h->solver == 0) {
-        CK(launch_solve_plain(h->kn.as<Knot>(), h->hdr, d, h->coef.as<cd>(),
+        CK(launch_solve_plain(h->kn.as<Knot>(), h->sg.as<Seg>(), h->hdr, d, h->coef.as<cd>(),
                               h->work.as<unsigned long long>(), h->status.as<int>(), h->st));
     } else {
         (void)d;
-        CK(launch_solve_batched(h->kn.as<Knot>(), h->hdr, h->evdev.as<EventDev>(),
+        CK(launch_solve_batched(h->kn.as<Knot>(), h->sg.as<Seg>(), h->hdr, h->evdev.as<EventDev>(),
                                 h->coefptr.as<cd*>(), h->items.as<int4>(), h->nitems,
                                 h->counter.as<int>(), h->work.as<unsigned long long>(),
                                 h->solve_blocks, h->solve_block, h->st));
@@ -452,7 +452,7 @@ void ysg_destroy(ysg_handle* h)
     if (!h) return;
     cudaSetDevice(h->device);
     if (h->st) cudaStreamSynchronize(h->st);
-    for (DevBuf* b : {&h->kn, &h->coef, &h->leg, &h->E, &h->delta, &h->ct, &h->stv, &h->spec,
+    for (DevBuf* b : {&h->kn, &h->sg, &h->coef, &h->leg, &h->E, &h->delta, &h->ct, &h->stv, &h->spec,
                       &h->filt, &h->tw, &h->expt, &h->cs, &h->scratch, &h->out, &h->work,
                       &h->status, &h->items, &h->counter, &h->evdev, &h->coefptr})
         b->release();
@@ -515,9 +515,29 @@ int ysg_model_upload(ysg_handle* h, const ysg_model* m)
     hd.tref = m->tref;
     hd.pibigg = m->pibigg;
     hd.fre_norm = m->fre_norm;
+    // power-form segments of the same splines (ysg_model.cuh, Seg)
+    std::vector<Seg> seg((size_t)n + 1);
+    std::memset(seg.data(), 0, seg.size() * sizeof(Seg));
+    for (int i = 1; i < n; i++) {
+        Seg& s = seg[(size_t)i];
+        const Knot &a = rec[(size_t)i], &b = rec[(size_t)i + 1];
+        const double hh = b.r - a.r;
+        s.r0 = a.r;
+        for (int p = 0; p < NPARAM; p++) {
+            s.c[p][0] = a.v[p][0];
+            if (hh == 0.0) continue;
+            s.c[p][1] = (b.v[p][0] - a.v[p][0]) / hh - hh * (2.0 * a.v[p][1] + b.v[p][1]) / 6.0;
+            s.c[p][2] = 0.5 * a.v[p][1];
+            s.c[p][3] = (b.v[p][1] - a.v[p][1]) / (6.0 * hh);
+        }
+    }
+    seg[(size_t)n].r0 = rec[(size_t)n].r;
+    for (int p = 0; p < NPARAM; p++) seg[(size_t)n].c[p][0] = rec[(size_t)n].v[p][0];
     cudaSetDevice(h->device);
     CK(h->kn.ensure(rec.size() * sizeof(Knot)));
     CK(cudaMemcpyAsync(h->kn.p, rec.data(), rec.size() * sizeof(Knot), cudaMemcpyHostToDevice, h->st));
+    CK(h->sg.ensure(seg.size() * sizeof(Seg)));
+    CK(cudaMemcpyAsync(h->sg.p, seg.data(), seg.size() * sizeof(Seg), cudaMemcpyHostToDevice, h->st));
     CK(cudaStreamSynchronize(h->st));
     h->hdr = hd;
     h->grav_host.assign(m->val[P_GRAV], m->val[P_GRAV] + n);

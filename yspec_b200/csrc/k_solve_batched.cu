@@ -4,10 +4,10 @@
 // (omega_j, l)), organised for the B200:
 //   * one thread per pair, but the five Cash-Karp stage vectors of the
 //     14-component minor / b-vector systems live in a per-thread slab of
-//     shared memory (70 complex entries, thread-interleaved so a warp's
-//     accesses are bank-conflict free); y and the stage input stay in
-//     registers.  The plain form keeps them in local memory, which spills
-//     through L1 into L2.
+//     shared memory (70 complex entries, interleaved across the lanes of a
+//     warp so accesses are bank-conflict free and every offset is a
+//     constant); y and the stage input stay in registers.  The plain form
+//     keeps them in local memory, which spills through L1 into L2.
 //   * a persistent grid (resident blocks only) pulls work items from an
 //     atomic counter.  An item is (event, l, 32 consecutive frequencies):
 //     the lanes of a warp share l and step through nearly identical radial
@@ -25,7 +25,7 @@ namespace ysg {
 constexpr int SLAB = 5 * 14;     // complex entries per thread
 
 __global__ void __launch_bounds__(64) k_solve_batched(const Knot* __restrict__ kn,
-                                                      ModelHdr mh_in,
+                                                      const Seg* __restrict__ sg, ModelHdr mh_in,
                                                       const EventDev* __restrict__ evs,
                                                       cd* const* __restrict__ coefs,
                                                       const int4* __restrict__ items, int nitems,
@@ -40,8 +40,8 @@ __global__ void __launch_bounds__(64) k_solve_batched(const Knot* __restrict__ k
     Ctx c;
     c.kn = kn;
     c.mh = &mh;
-    c.kb = slab + threadIdx.x;
-    c.ks = blockDim.x;
+    c.sg = sg;
+    c.kb = slab + (threadIdx.x >> 5) * (SLAB * KS) + lane;
     for (int q = 0; q < NSYS; q++) c.nst[q] = 0;
     for (;;) {
         int it = 0;
@@ -89,7 +89,8 @@ int solve_batched_blocks(int block)
     return nsm * per;
 }
 
-cudaError_t launch_solve_batched(const Knot* kn, const ModelHdr& mh, const EventDev* evs_dev,
+cudaError_t launch_solve_batched(const Knot* kn, const Seg* sg, const ModelHdr& mh,
+                                 const EventDev* evs_dev,
                                  cd* const* coefs_dev, const int4* items, int nitems, int* counter,
                                  unsigned long long* work, int nblocks, int block, cudaStream_t st)
 {
@@ -100,8 +101,8 @@ cudaError_t launch_solve_batched(const Knot* kn, const ModelHdr& mh, const Event
     if (e != cudaSuccess) return e;
     e = cudaMemsetAsync(counter, 0, sizeof(int), st);
     if (e != cudaSuccess) return e;
-    k_solve_batched<<<nblocks, block, smem, st>>>(kn, mh, evs_dev, coefs_dev, items, nitems, counter,
-                                                 work);
+    k_solve_batched<<<nblocks, block, smem, st>>>(kn, sg, mh, evs_dev, coefs_dev, items, nitems,
+                                                 counter, work);
     return cudaGetLastError();
 }
 

@@ -8,7 +8,8 @@
 
 namespace ysg {
 
-__global__ void __launch_bounds__(128) k_solve_plain(const Knot* __restrict__ kn_g, ModelHdr mh,
+__global__ void __launch_bounds__(128) k_solve_plain(const Knot* __restrict__ kn_g,
+                                                     const Seg* __restrict__ sg, ModelHdr mh,
                                                      EventDev ev, cd* __restrict__ coef,
                                                      unsigned long long* __restrict__ work,
                                                      int* status)
@@ -28,8 +29,8 @@ __global__ void __launch_bounds__(128) k_solve_plain(const Knot* __restrict__ kn
     c.kn = kn;
     c.mh = mhs;
     c.ats = (double)ev.ats;
+    c.sg = sg;
     c.kb = nullptr;
-    c.ks = 0;
     for (int q = 0; q < NSYS; q++) c.nst[q] = 0;
     if (gid < total) {
         const int li = (int)(gid / ev.nw);
@@ -60,7 +61,8 @@ size_t solve_plain_smem(int nknot)
     return (size_t)(nknot + 2) * sizeof(Knot) + sizeof(ModelHdr) + 16;
 }
 
-cudaError_t launch_solve_plain(const Knot* kn, const ModelHdr& mh, const EventDev& ev, cd* coef,
+cudaError_t launch_solve_plain(const Knot* kn, const Seg* sg, const ModelHdr& mh, const EventDev& ev,
+                               cd* coef,
                                unsigned long long* work, int* status, cudaStream_t st)
 {
     const long long total = (long long)(ev.lmax - ev.lmin + 1) * ev.nw;
@@ -71,7 +73,7 @@ cudaError_t launch_solve_plain(const Knot* kn, const ModelHdr& mh, const EventDe
     cudaError_t e = cudaFuncSetAttribute(k_solve_plain, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     if (e != cudaSuccess) return e;
-    k_solve_plain<<<(unsigned)nb, bs, smem, st>>>(kn, mh, ev, coef, work, status);
+    k_solve_plain<<<(unsigned)nb, bs, smem, st>>>(kn, sg, mh, ev, coef, work, status);
     return cudaGetLastError();
 }
 

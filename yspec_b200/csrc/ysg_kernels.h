@@ -10,15 +10,16 @@ constexpr int NSYS_COUNT = 8;
 
 // K1 plain: one thread per (omega,l) pair of one event.
 size_t solve_plain_smem(int nknot);
-cudaError_t launch_solve_plain(const Knot* kn, const ModelHdr& mh, const EventDev& ev, cd* coef,
-                               unsigned long long* work, int* status, cudaStream_t st);
+cudaError_t launch_solve_plain(const Knot* kn, const Seg* sg, const ModelHdr& mh, const EventDev& ev,
+                               cd* coef, unsigned long long* work, int* status, cudaStream_t st);
 
 // K1 batched persistent: work items (event, l index, first frequency - 1)
 // of one or more events, one thread per (omega,l) pair, stage vectors in
 // shared memory.  counter must be device memory (reset by the launcher).
 size_t solve_batched_smem(int block);
 int solve_batched_blocks(int block);
-cudaError_t launch_solve_batched(const Knot* kn, const ModelHdr& mh, const EventDev* evs_dev,
+cudaError_t launch_solve_batched(const Knot* kn, const Seg* sg, const ModelHdr& mh,
+                                 const EventDev* evs_dev,
                                  cd* const* coefs_dev, const int4* items, int nitems, int* counter,
                                  unsigned long long* work, int nblocks, int block, cudaStream_t st);
 

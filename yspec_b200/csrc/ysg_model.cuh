@@ -77,4 +77,25 @@ __device__ __forceinline__ double spl(const Knot* kn, const SplPt& s, int p)
     return s.A * a.v[p][0] + s.B * b.v[p][0] + (s.A3 * a.v[p][1] + s.B3 * b.v[p][1]) * s.h26;
 }
 
+// The same cubic on knot interval i in power form, value = c0 + t (c1 +
+// t (c2 + t c3)) with t = r - r_i.  Expanding A y_i + B y_i+1 + ((A^3-A) y''_i
+// + (B^3-B) y''_i+1) h^2/6 in t = B h gives
+//   c0 = y_i,  c1 = (y_i+1 - y_i)/h - h (2 y''_i + y''_i+1)/6,
+//   c2 = y''_i / 2,  c3 = (y''_i+1 - y''_i) / (6 h),
+// and c1 = c2 = c3 = 0 on a zero-length interval.  The right-hand sides
+// evaluate the model with it: three fused multiply-adds per parameter and
+// no division, equal to the form above to rounding.  Record i covers
+// [r_i, r_i+1] (1-based like the knots); 432 bytes, 16-byte aligned.
+struct __align__(16) Seg {
+    double r0, pad;
+    double c[NPARAM][4];
+};
+static_assert(sizeof(Seg) == 432, "segment record size");
+
+__device__ __forceinline__ double seg(const Seg& s, double t, int p)
+{
+    const double* c = s.c[p];
+    return fma(fma(fma(c[3], t, c[2]), t, c[1]), t, c[0]);
+}
+
 }  // namespace ysg

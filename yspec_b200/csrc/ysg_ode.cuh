@@ -52,8 +52,8 @@ struct Ctx {
     const ModelHdr* mh;
     int ll, llp1, il;
     unsigned nst[NSYS];
+    const Seg* sg;   // power-form spline segments (right-hand sides)
     cd* kb;          // shared-memory stage slab of this thread (smem form)
-    int ks;          // stride between slab entries, in complex elements
     double zeta, zeta2, zeta2m2, szeta2m2, nu, dr, ats;
     cd omega, omega2, omegai, omegai2, lno;
 };
@@ -99,22 +99,34 @@ __device__ __forceinline__ void alpha_steps(Ctx& c)
 
 // ---------------------------------------------------------------------------
 // Coefficient matrices
+//
+// The model is evaluated from the power-form segments of the current layer
+// (c.il, set by yint).  The reference's separate divisions (1/r and the
+// complex reciprocals 1/(C(1 + qa lno)), 1/(L(1 + qmu lno))) are formed from
+// one real division: for a real c and complex q, 1/(c q) = conj(q) / (c |q|^2),
+// and the real denominators are multiplied together and split back out.
+// The moduli are O(1) after normalisation, so this stays far from overflow
+// and agrees with the separate divisions to a few ulps.
 // ---------------------------------------------------------------------------
+__device__ __forceinline__ double norm2(cd a) { return a.x * a.x + a.y * a.y; }
 
 // module_int.f90:134-164 tor_amat (t real, k and s complex)
 struct TorCoef { double t; cd k, s; };
 
 __device__ __forceinline__ TorCoef tor_amat(const Ctx& c, double rr)
 {
-    SplPt s = spl_at(c.kn, c.il, rr);
-    double rrho = spl(c.kn, s, P_RHO), rlcon = spl(c.kn, s, P_LCON);
-    double rncon = spl(c.kn, s, P_NCON), rqmu = spl(c.kn, s, P_QMU);
+    const Seg& g = c.sg[c.il];
+    const double u = rr - g.r0;
+    double rrho = seg(g, u, P_RHO), rlcon = seg(g, u, P_LCON);
+    double rncon = seg(g, u, P_NCON), rqmu = seg(g, u, P_QMU);
     cd qll = 1.0 + rqmu * c.lno;
-    cd clcon = rlcon * qll, cncon = rncon * qll;
-    double ri = 1.0 / rr;
+    cd cncon = rncon * qll;
+    const double dl = rlcon * norm2(qll);
+    const double inv = 1.0 / (rr * dl);
+    double ri = dl * inv;
     TorCoef a;
     a.t = 2.0 * ri;
-    a.k = 1.0 / clcon;
+    a.k = conj(qll) * (rr * inv);     // 1 / (L (1 + qmu lno))
     a.s = -(c.omega2 * rrho) + (ri * ri * c.zeta2m2) * cncon;
     return a;
 }
@@ -125,16 +137,18 @@ struct RadCoef { cd t, k, s; };
 
 __device__ __forceinline__ RadCoef rad_amat(const Ctx& c, double rr)
 {
-    SplPt s = spl_at(c.kn, c.il, rr);
-    const Knot* kn = c.kn;
-    double rrho = spl(kn, s, P_RHO), racon = spl(kn, s, P_ACON), rccon = spl(kn, s, P_CCON);
-    double rfcon = spl(kn, s, P_FCON), rncon = spl(kn, s, P_NCON), gg = spl(kn, s, P_GRAV);
-    double rqmu = spl(kn, s, P_QMU), rxlam = spl(kn, s, P_XLAM), rxa2 = spl(kn, s, P_XA2);
+    const Seg& g = c.sg[c.il];
+    const double u = rr - g.r0;
+    double rrho = seg(g, u, P_RHO), racon = seg(g, u, P_ACON), rccon = seg(g, u, P_CCON);
+    double rfcon = seg(g, u, P_FCON), rncon = seg(g, u, P_NCON), gg = seg(g, u, P_GRAV);
+    double rqmu = seg(g, u, P_QMU), rxlam = seg(g, u, P_XLAM), rxa2 = seg(g, u, P_XA2);
     cd qaa = 1.0 + rxa2 * c.lno, qff = 1.0 + rxlam * c.lno, qll = 1.0 + rqmu * c.lno;
     cd cacon = racon * qaa, cfcon = rfcon * qff, cncon = rncon * qll;
-    cd cccon = 1.0 / (rccon * qaa);
+    const double dc = rccon * norm2(qaa);
+    const double inv = 1.0 / (rr * dc);
+    cd cccon = conj(qaa) * (rr * inv);     // 1 / (C (1 + qa lno))
     cd gamma = cacon - cncon - cfcon * cfcon * cccon;
-    double ri = 1.0 / rr;
+    double ri = dc * inv;
     RadCoef a;
     a.t = (1.0 - 2.0 * cfcon * cccon) * ri;
     a.k = cccon;
@@ -154,31 +168,33 @@ struct SolidCoef {
 template <int KIND>
 __device__ __forceinline__ SolidCoef solid_amat(const Ctx& c, double rr)
 {
-    SplPt s = spl_at(c.kn, c.il, rr);
-    const Knot* kn = c.kn;
-    double rrho = spl(kn, s, P_RHO), racon = spl(kn, s, P_ACON), rccon = spl(kn, s, P_CCON);
-    double rfcon = spl(kn, s, P_FCON), rncon = spl(kn, s, P_NCON), rlcon = spl(kn, s, P_LCON);
-    double rqmu = spl(kn, s, P_QMU), rxlam = spl(kn, s, P_XLAM), rxa2 = spl(kn, s, P_XA2);
+    const Seg& g = c.sg[c.il];
+    const double u = rr - g.r0;
+    double rrho = seg(g, u, P_RHO), racon = seg(g, u, P_ACON), rccon = seg(g, u, P_CCON);
+    double rfcon = seg(g, u, P_FCON), rncon = seg(g, u, P_NCON), rlcon = seg(g, u, P_LCON);
+    double rqmu = seg(g, u, P_QMU), rxlam = seg(g, u, P_XLAM), rxa2 = seg(g, u, P_XA2);
     cd qaa = 1.0 + rxa2 * c.lno, qff = 1.0 + rxlam * c.lno, qll = 1.0 + rqmu * c.lno;
-    cd cacon = racon * qaa, cfcon = rfcon * qff, cncon = rncon * qll, clcon = rlcon * qll;
-    cd cccon = 1.0 / (rccon * qaa);
+    cd cacon = racon * qaa, cfcon = rfcon * qff, cncon = rncon * qll;
+    const double dc = rccon * norm2(qaa), dl = rlcon * norm2(qll);
+    const double inv = 1.0 / (rr * (dc * dl));
+    cd cccon = conj(qaa) * ((rr * dl) * inv);     // 1 / (C (1 + qa lno))
     cd fc = cfcon * cccon;
     cd gamma = cacon - cncon - cfcon * fc;
-    double ri = 1.0 / rr, ri2 = ri * ri;
+    double ri = (dc * dl) * inv, ri2 = ri * ri;
     SolidCoef a;
     a.t11 = (1.0 - 2.0 * fc) * ri;
     a.t12 = (c.zeta * ri) * fc;
     a.t21 = -(c.zeta * ri);
     a.t22 = 2.0 * ri;
     a.k11 = cccon;
-    a.k22 = 1.0 / clcon;
+    a.k22 = conj(qll) * ((rr * dc) * inv);       // 1 / (L (1 + qmu lno))
     cd mw2r = -(c.omega2 * rrho);
     a.s22 = mw2r + (c.zeta2 * (gamma + cncon) - 2.0 * cncon) * ri2;
     if (KIND == 0) {
         a.s11 = mw2r + (4.0 * gamma) * ri2;
         a.s12 = (-2.0 * c.zeta) * gamma * ri2;
     } else {
-        double gg = spl(kn, s, P_GRAV);
+        double gg = seg(g, u, P_GRAV);
         double rgr = rrho * gg * rr;
         a.s11 = mw2r + (4.0 * (gamma - rgr)) * ri2;
         a.s12 = (c.zeta * (rgr - 2.0 * gamma)) * ri2;
@@ -204,14 +220,17 @@ struct FluidCoef {
 template <int KIND>
 __device__ __forceinline__ FluidCoef fluid_amat(const Ctx& c, double rr)
 {
-    SplPt s = spl_at(c.kn, c.il, rr);
-    const Knot* kn = c.kn;
-    double rrho = spl(kn, s, P_RHO), rccon = spl(kn, s, P_CCON), rxa2 = spl(kn, s, P_XA2);
+    const Seg& g = c.sg[c.il];
+    const double u = rr - g.r0;
+    double rrho = seg(g, u, P_RHO), rccon = seg(g, u, P_CCON), rxa2 = seg(g, u, P_XA2);
     cd qaa = 1.0 + rxa2 * c.lno;
-    cd cccon = 1.0 / (rccon * qaa);
-    double ri = 1.0 / rr;
+    const double dc = rccon * norm2(qaa);
+    const double inv = 1.0 / (rr * rrho * dc);
+    cd cccon = conj(qaa) * ((rr * rrho) * inv);  // 1 / (C (1 + qa lno))
+    double ri = (rrho * dc) * inv;
+    const double irho = (rr * dc) * inv;          // 1 / rho
     FluidCoef a;
-    a.k11 = cccon - ((c.zeta2 * c.omegai2) * (ri * ri)) / rrho;
+    a.k11 = cccon - (c.zeta2 * c.omegai2) * ((ri * ri) * irho);
     if (KIND == 0) {
         a.t11 = mk(-ri);
         a.s11 = -(c.omega2 * rrho);
@@ -219,7 +238,7 @@ __device__ __forceinline__ FluidCoef fluid_amat(const Ctx& c, double rr)
         a.t21 = a.t22 = a.k22 = 0.0;
         return a;
     }
-    double gg = spl(kn, s, P_GRAV);
+    double gg = seg(g, u, P_GRAV);
     cd gzw = (gg * c.zeta2) * c.omegai2;
     a.t11 = (gzw * ri - 1.0) * ri;
     a.s11 = -(c.omega2 * rrho) + (rrho * gg) * ((gzw * ri - 4.0) * ri);
@@ -436,12 +455,15 @@ __device__ __forceinline__ void rkck_step(const Ctx& c, cd* y, double x, double 
 }
 
 // Shared-memory form of the same step: stage vectors go to the thread's
-// slab (entry (s*N + i) at kb[(s*N + i) * ks]) as the right-hand side
-// produces them, so only y and the stage input are held in registers.
+// slab as the right-hand side produces them, so only y and the stage input
+// are held in registers.  A warp's slabs are interleaved lane by lane: entry
+// e of a lane sits at kb[e * KS], so a warp touches 32 consecutive complex
+// values per entry (no bank conflicts) and every offset is a constant.
+constexpr int KS = 32;
+
 struct SlabOut {
     cd* p;
-    int ks;
-    __device__ __forceinline__ cd& operator[](int i) const { return p[i * ks]; }
+    __device__ __forceinline__ cd& operator[](int i) const { return p[i * KS]; }
 };
 
 // Cash-Karp tableau (module_int.f90:2039-2049) for the looped step.
@@ -466,7 +488,6 @@ __device__ __forceinline__ void rkck_step_loop(const Ctx& c, cd* y, double x, do
     constexpr double c1 = 37.0 / 378.0, c3 = 250.0 / 621.0, c4 = 125.0 / 594.0,
                      c6 = 512.0 / 1771.0;
     cd* const kb = c.kb;
-    const int ks = c.ks;
     cd yt[N];
 #pragma unroll 1
     for (int s = 0; s < 6; s++) {
@@ -474,17 +495,17 @@ __device__ __forceinline__ void rkck_step_loop(const Ctx& c, cd* y, double x, do
         for (int i = 0; i < N; i++) yt[i] = y[i];
         for (int j = 0; j < s; j++) {
             const double hb = h * ck_b[s][j];
-            const cd* kj = kb + j * N * ks;
+            const cd* kj = kb + j * N * KS;
 #pragma unroll
-            for (int i = 0; i < N; i++) yt[i] += hb * kj[i * ks];
+            for (int i = 0; i < N; i++) yt[i] += hb * kj[i * KS];
         }
         const int slot = (s == 5) ? 1 : s;
-        Sys::f(c, x + ck_a[s] * h, yt, SlabOut{kb + slot * N * ks, ks});
+        Sys::f(c, x + ck_a[s] * h, yt, SlabOut{kb + slot * N * KS});
     }
 #pragma unroll
     for (int i = 0; i < N; i++)
-        y[i] = y[i] + h * (c1 * kb[i * ks] + c3 * kb[(2 * N + i) * ks] + c4 * kb[(3 * N + i) * ks] +
-                           c6 * kb[(N + i) * ks]);
+        y[i] = y[i] + h * (c1 * kb[i * KS] + c3 * kb[(2 * N + i) * KS] + c4 * kb[(3 * N + i) * KS] +
+                           c6 * kb[(N + i) * KS]);
 }
 
 template <class Sys>
@@ -500,9 +521,8 @@ __device__ __forceinline__ void rkck_step_smem(const Ctx& c, cd* y, double x, do
     constexpr double c1 = 37.0 / 378.0, c3 = 250.0 / 621.0, c4 = 125.0 / 594.0,
                      c6 = 512.0 / 1771.0;
     cd* const kb = c.kb;
-    const int ks = c.ks;
-    const SlabOut K0{kb, ks}, K1{kb + N * ks, ks}, K2{kb + 2 * N * ks, ks};
-    const SlabOut K3{kb + 3 * N * ks, ks}, K4{kb + 4 * N * ks, ks};
+    const SlabOut K0{kb}, K1{kb + N * KS}, K2{kb + 2 * N * KS};
+    const SlabOut K3{kb + 3 * N * KS}, K4{kb + 4 * N * KS};
     cd yt[N];
     Sys::f(c, x, y, K0);
 #pragma unroll
@@ -526,19 +546,24 @@ __device__ __forceinline__ void rkck_step_smem(const Ctx& c, cd* y, double x, do
     for (int i = 0; i < N; i++) y[i] = y[i] + h * (c1 * K0[i] + c3 * K2[i] + c4 * K3[i] + c6 * K1[i]);
 }
 
+// yint's rescaling (module_int.f90:1910-1919, 1952-1961).  |y| is compared through
+// |y|^2 against the squared bounds (1e-40, 1e40, both normal doubles): the
+// decision can differ from the reference only within rounding of a bound,
+// where either choice scales y exactly as the scale count records.
 template <int N>
 __device__ __forceinline__ void rescale(cd* y, int* scale)
 {
+    constexpr double TINY2 = SC_TINY * SC_TINY, HUGE2 = SC_HUGE * SC_HUGE;
     bool all_small = true, any_big = false;
 #pragma unroll
-    for (int k = 0; k < N; k++) all_small = all_small && (cabs(y[k]) < SC_TINY);
+    for (int k = 0; k < N; k++) all_small = all_small && (norm2(y[k]) < TINY2);
     if (all_small) {
         (*scale)++;
 #pragma unroll
         for (int k = 0; k < N; k++) y[k] = y[k] * SC_HUGE;
     }
 #pragma unroll
-    for (int k = 0; k < N; k++) any_big = any_big || (cabs(y[k]) > SC_HUGE);
+    for (int k = 0; k < N; k++) any_big = any_big || (norm2(y[k]) > HUGE2);
     if (any_big) {
         (*scale)--;
 #pragma unroll

@@ -1,0 +1,61 @@
+"""Time the device stages of a synthetic workload configuration.
+
+    python -m yspec_b200.stages c2 [--solver batched|plain] [--reps 3]
+                                   [--seed 0] [--set lmax=300 --set fmax=20.0]
+
+Runs the configuration's first event through `Engine.run` `reps` times and
+prints, per run, the device time of each stage (Legendre table, solves,
+l-sum, filter + inverse FFT) measured with CUDA events on the engine's
+stream, the number of (omega,l) solves and the counted FP64 work of the
+solve stage.  It is also the small, self-contained command used for ncu
+captures of one kernel.
+"""
+from __future__ import annotations
+
+import argparse
+import tempfile
+import time
+from pathlib import Path
+
+from . import Engine, Event, Model, Params, workloads as W
+
+
+def _parse_set(items: list[str]) -> dict:
+    out = {}
+    for kv in items:
+        k, v = kv.split("=", 1)
+        out[k] = type(getattr(W.Params(), k))(v)
+    return out
+
+
+def main(argv=None) -> None:
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("config", help="c1 .. c5")
+    ap.add_argument("--solver", default="batched", choices=["batched", "plain"])
+    ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--event", type=int, default=0, help="event index within the configuration")
+    ap.add_argument("--set", action="append", default=[], metavar="KEY=VALUE",
+                    help="override a parameter of the configuration")
+    a = ap.parse_args(argv)
+    p = W.config(a.config, seed=a.seed, **_parse_set(a.set))[a.event]
+    eng = Engine(0, solver=a.solver)
+    with tempfile.TemporaryDirectory() as tmp:
+        pf = p.write(Path(tmp) / f"{a.config}.in")
+        m = Model(p.model_file)
+        eng.upload(m)
+        ev = Event(m, Params(pf))
+        for rep in range(a.reps):
+            t = time.perf_counter()
+            eng.run(ev)
+            wall = time.perf_counter() - t
+            ms = eng.timings()
+            pairs, fl = eng.work()
+            print(f"{a.config} {a.solver} rep{rep}: wall {wall:.3f} s  stages (ms) "
+                  f"legendre {ms[0]:.3f} solve {ms[1]:.3f} lsum {ms[2]:.3f} ifft {ms[3]:.3f}  "
+                  f"pairs {pairs:.0f}  solves/s {pairs / (ms[1] / 1e3):.4g}  "
+                  f"solve FP64 {fl / (ms[1] / 1e3) / 1e12:.3f} TFLOP/s", flush=True)
+
+
+if __name__ == "__main__":
+    main()
