@@ -187,6 +187,10 @@ int ysg_last_bytes(ysg_handle *h, double *h2d, double *d2h);
 int ysg_fp64_peak(int device, double *tflops);
 
 const char *ysg_status_string(int status);
+
+/* The CUDA runtime error behind the calling thread's last YSG_ERR_CUDA
+ * (error name, message and the failing call), or "" if there was none. */
+const char *ysg_last_cuda_error(void);
 void ysg_destroy(ysg_handle *h);
 
 #ifdef __cplusplus

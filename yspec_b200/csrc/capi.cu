@@ -62,6 +62,22 @@ const double kStepFlops[NSYS_COUNT] = {
     6 * 700.0 + 88.0 * 14,   // b-vector, self-gravitation
 };
 
+// Device buffers and uploaded state of one event.  Slot 0 serves the
+// single-event calls; a batch uses slots 0..nev-1.
+struct Slot {
+    DevBuf coef, leg, E, delta, ct, stv, spec, filt, tw, expt, cs, out;
+    EventDev pev{};
+    TraceDev ptd{};
+    int nr = 0, lmax = 0;
+    bool ev_ready = false, tm_ready = false;
+    void release()
+    {
+        for (DevBuf* b : {&coef, &leg, &E, &delta, &ct, &stv, &spec, &filt, &tw, &expt, &cs, &out})
+            b->release();
+        ev_ready = tm_ready = false;
+    }
+};
+
 }  // namespace
 
 struct ysg_handle {
@@ -74,27 +90,48 @@ struct ysg_handle {
     ModelHdr hdr{};
     std::vector<double> grav_host;   // knot gravity for the tilt correction
     bool has_model = false;
-    // event buffers
-    DevBuf coef, leg, E, delta, ct, stv, spec, filt, tw, expt, cs, scratch, out;
+    // events
+    std::vector<Slot> slots;
+    int nactive = 0;                 // slots of the last prepare / batch
+    DevBuf scratch;                  // inverse-FFT rows, shared by the slots (stages run in order)
     DevBuf work, status, items, counter, evdev, coefptr;
     int nitems = 0, solve_blocks = 0, solve_block = 64;
-    // uploaded event / time stage
-    bool ev_ready = false, tm_ready = false, has_spectra = false;
-    EventDev pev{};
-    TraceDev ptd{};
-    int p_nr = 0, p_lmax = 0;
+    bool has_spectra = false;
+    // CUDA graph of the last batch (updated in place when the shape repeats)
+    cudaGraphExec_t gexec = nullptr;
+    bool capturing = false;          // enqueue_* run under stream capture
     float ms[4] = {0, 0, 0, 0};
     double h2d = 0.0, d2h = 0.0;     // bytes moved since the last prepare
     double pairs = 0.0, flops = 0.0;
 };
 
-#define CK(x)                                       \
-    do {                                            \
-        cudaError_t e_ = (x);                       \
-        if (e_ != cudaSuccess) return YSG_ERR_CUDA; \
+// CUDA failures return YSG_ERR_CUDA and leave the runtime's error name and
+// the failing call's source line for ysg_last_cuda_error().
+thread_local char g_cuda_err[160] = "";
+
+int cuda_fail(cudaError_t e, int line)
+{
+    std::snprintf(g_cuda_err, sizeof g_cuda_err, "%s (%s) at capi.cu:%d", cudaGetErrorName(e),
+                  cudaGetErrorString(e), line);
+    return YSG_ERR_CUDA;
+}
+
+#define CK(x)                                                  \
+    do {                                                       \
+        cudaError_t e_ = (x);                                  \
+        if (e_ != cudaSuccess) return cuda_fail(e_, __LINE__); \
     } while (0)
 
 namespace {
+
+// Stage timing event i.  Under stream capture a plain record only orders the
+// captured work; cudaEventRecordExternal makes it an event-record node of the
+// graph, so the stage times of a batch are measured like a single event's.
+cudaError_t record(ysg_handle* h, int i)
+{
+    return cudaEventRecordWithFlags(h->ev[i], h->st,
+                                    h->capturing ? cudaEventRecordExternal : cudaEventRecordDefault);
+}
 
 int check_event(const ysg_handle* h, const ysg_event* ev)
 {
@@ -208,9 +245,23 @@ int upload_items(ysg_handle* h, std::vector<Item>& items, const std::vector<Even
     return YSG_OK;
 }
 
+// Work items of the batched solver for slots 0..nev-1, longest first.
+int upload_batch_items(ysg_handle* h, int nev)
+{
+    std::vector<Item> items;
+    std::vector<EventDev> evs((size_t)nev);
+    std::vector<cd*> coefs((size_t)nev);
+    for (int e = 0; e < nev; e++) {
+        evs[(size_t)e] = h->slots[(size_t)e].pev;
+        coefs[(size_t)e] = h->slots[(size_t)e].coef.as<cd>();
+        build_items(items, e, evs[(size_t)e]);
+    }
+    return upload_items(h, items, evs, coefs);
+}
+
 // Event inputs to the device: cos/sin of delta and e^{i m azst}
 // (yspec.f90:173-174, :331, :414); buffers sized.  No kernel runs.
-int upload_event(ysg_handle* h, const ysg_event* ev)
+int upload_event(ysg_handle* h, Slot& s, const ysg_event* ev)
 {
     const int nr = ev->nr, nw = ev->nw, n1 = std::max(nr, 1);
     std::vector<double> ct(n1), stv(n1);
@@ -222,37 +273,32 @@ int upload_event(ysg_handle* h, const ysg_event* ev)
         for (int m = -2; m <= 2; m++) E[(size_t)k * 5 + (m + 2)] = cpowi(eia, m);
     }
     const int L = ev->lmax - ev->lmin + 1;
-    CK(h->coef.ensure((size_t)L * NCOEF * nw * sizeof(cd)));
-    CK(h->spec.ensure(3 * (size_t)nw * n1 * sizeof(cd)));
-    CK(h->delta.ensure((size_t)n1 * sizeof(double)));
-    CK(h->ct.ensure((size_t)n1 * sizeof(double)));
-    CK(h->stv.ensure((size_t)n1 * sizeof(double)));
-    CK(h->E.ensure((size_t)n1 * 5 * sizeof(cd)));
-    CK(h->leg.ensure((size_t)(ev->lmax + 1) * n1 * 8 * sizeof(double)));
+    s.ev_ready = s.tm_ready = false;
+    CK(s.coef.ensure((size_t)L * NCOEF * nw * sizeof(cd)));
+    CK(s.spec.ensure(3 * (size_t)nw * n1 * sizeof(cd)));
+    CK(s.delta.ensure((size_t)n1 * sizeof(double)));
+    CK(s.ct.ensure((size_t)n1 * sizeof(double)));
+    CK(s.stv.ensure((size_t)n1 * sizeof(double)));
+    CK(s.E.ensure((size_t)n1 * 5 * sizeof(cd)));
+    CK(s.leg.ensure((size_t)(ev->lmax + 1) * n1 * 8 * sizeof(double)));
     if (nr > 0) {
-        CK(cudaMemcpyAsync(h->delta.p, ev->delta, (size_t)nr * sizeof(double), cudaMemcpyHostToDevice, h->st));
-        CK(cudaMemcpyAsync(h->ct.p, ct.data(), (size_t)nr * sizeof(double), cudaMemcpyHostToDevice, h->st));
-        CK(cudaMemcpyAsync(h->stv.p, stv.data(), (size_t)nr * sizeof(double), cudaMemcpyHostToDevice, h->st));
-        CK(cudaMemcpyAsync(h->E.p, E.data(), (size_t)nr * 5 * sizeof(cd), cudaMemcpyHostToDevice, h->st));
+        CK(cudaMemcpyAsync(s.delta.p, ev->delta, (size_t)nr * sizeof(double), cudaMemcpyHostToDevice, h->st));
+        CK(cudaMemcpyAsync(s.ct.p, ct.data(), (size_t)nr * sizeof(double), cudaMemcpyHostToDevice, h->st));
+        CK(cudaMemcpyAsync(s.stv.p, stv.data(), (size_t)nr * sizeof(double), cudaMemcpyHostToDevice, h->st));
+        CK(cudaMemcpyAsync(s.E.p, E.data(), (size_t)nr * 5 * sizeof(cd), cudaMemcpyHostToDevice, h->st));
         h->h2d += (double)nr * (3 * sizeof(double) + 5 * sizeof(cd));
     }
     CK(cudaStreamSynchronize(h->st));   // the host vectors go out of scope
-    h->pev = make_event(h, ev);
-    if (h->solver == 1) {
-        std::vector<Item> items;
-        build_items(items, 0, h->pev);
-        int rc = upload_items(h, items, {h->pev}, {h->coef.as<cd>()});
-        if (rc) return rc;
-    }
-    h->p_nr = nr;
-    h->p_lmax = ev->lmax;
-    h->ev_ready = true;
+    s.pev = make_event(h, ev);
+    s.nr = nr;
+    s.lmax = ev->lmax;
+    s.ev_ready = true;
     return YSG_OK;
 }
 
 // Time-stage inputs: taper (module_fourier.f90:96-116), twiddles with pi_d,
 // e^{eps t} (yspec.f90:439-444), cos/sin of azep (:466-473).
-int upload_time(ysg_handle* h, const ysg_time* tm, int nw)
+int upload_time(ysg_handle* h, Slot& s, const ysg_time* tm, int nw)
 {
     const int n = tm->nt, nr = tm->nr;
     if (n < 4 || (n & (n - 1)) || n > (1 << 20)) return YSG_ERR_ARG;
@@ -287,19 +333,20 @@ int upload_time(ysg_handle* h, const ysg_time* tm, int nw)
         cs[2 * (size_t)k] = std::cos(tm->azep[k]);
         cs[2 * (size_t)k + 1] = std::sin(tm->azep[k]);
     }
-    CK(h->filt.ensure(filt.size() * sizeof(double)));
-    CK(h->tw.ensure(tw.size() * sizeof(cd)));
-    CK(h->expt.ensure(expt.size() * sizeof(double)));
-    CK(h->cs.ensure(cs.size() * sizeof(double)));
+    s.tm_ready = false;
+    CK(s.filt.ensure(filt.size() * sizeof(double)));
+    CK(s.tw.ensure(tw.size() * sizeof(cd)));
+    CK(s.expt.ensure(expt.size() * sizeof(double)));
+    CK(s.cs.ensure(cs.size() * sizeof(double)));
     CK(h->scratch.ensure(std::max<size_t>(ifft_scratch_bytes(n, nr), 16)));
-    CK(h->out.ensure(std::max<size_t>((size_t)nout * 4 * nr * sizeof(double), 16)));
-    CK(cudaMemcpyAsync(h->filt.p, filt.data(), filt.size() * sizeof(double), cudaMemcpyHostToDevice, h->st));
-    CK(cudaMemcpyAsync(h->tw.p, tw.data(), tw.size() * sizeof(cd), cudaMemcpyHostToDevice, h->st));
-    CK(cudaMemcpyAsync(h->expt.p, expt.data(), expt.size() * sizeof(double), cudaMemcpyHostToDevice, h->st));
-    CK(cudaMemcpyAsync(h->cs.p, cs.data(), cs.size() * sizeof(double), cudaMemcpyHostToDevice, h->st));
+    CK(s.out.ensure(std::max<size_t>((size_t)nout * 4 * nr * sizeof(double), 16)));
+    CK(cudaMemcpyAsync(s.filt.p, filt.data(), filt.size() * sizeof(double), cudaMemcpyHostToDevice, h->st));
+    CK(cudaMemcpyAsync(s.tw.p, tw.data(), tw.size() * sizeof(cd), cudaMemcpyHostToDevice, h->st));
+    CK(cudaMemcpyAsync(s.expt.p, expt.data(), expt.size() * sizeof(double), cudaMemcpyHostToDevice, h->st));
+    CK(cudaMemcpyAsync(s.cs.p, cs.data(), cs.size() * sizeof(double), cudaMemcpyHostToDevice, h->st));
     h->h2d += (double)((filt.size() + expt.size() + cs.size()) * sizeof(double) + tw.size() * sizeof(cd));
     CK(cudaStreamSynchronize(h->st));
-    TraceDev& td = h->ptd;
+    TraceDev& td = s.ptd;
     td = TraceDev{};
     td.nt = n;
     td.i1 = tm->i1;
@@ -313,20 +360,23 @@ int upload_time(ysg_handle* h, const ysg_time* tm, int nw)
     td.scale = tm->dt * (double)n;
     td.t_norm = tm->t_norm;
     td.amp_norm = tm->amp_norm;
-    h->tm_ready = true;
+    s.tm_ready = true;
     return YSG_OK;
 }
 
-int enqueue_solve(ysg_handle* h)
+// K1 for slots 0..nev-1: one batched launch over all their items, or one
+// plain launch per event.
+int enqueue_solve(ysg_handle* h, int nev)
 {
-    const EventDev& d = h->pev;
     CK(cudaMemsetAsync(h->work.p, 0, NSYS_COUNT * sizeof(unsigned long long), h->st));
     CK(cudaMemsetAsync(h->status.p, 0, sizeof(int), h->st));
     if (h->solver == 0) {
-        CK(launch_solve_plain(h->kn.as<Knot>(), h->sg.as<Seg>(), h->hdr, d, h->coef.as<cd>(),
-                              h->work.as<unsigned long long>(), h->status.as<int>(), h->st));
+        for (int e = 0; e < nev; e++) {
+            const Slot& s = h->slots[(size_t)e];
+            CK(launch_solve_plain(h->kn.as<Knot>(), h->sg.as<Seg>(), h->hdr, s.pev, s.coef.as<cd>(),
+                                  h->work.as<unsigned long long>(), h->status.as<int>(), h->st));
+        }
     } else {
-        (void)d;
         CK(launch_solve_batched(h->kn.as<Knot>(), h->sg.as<Seg>(), h->hdr, h->evdev.as<EventDev>(),
                                 h->coefptr.as<cd*>(), h->items.as<int4>(), h->nitems,
                                 h->counter.as<int>(), h->work.as<unsigned long long>(),
@@ -335,41 +385,51 @@ int enqueue_solve(ysg_handle* h)
     return YSG_OK;
 }
 
-// K2 -> K1 -> K3 on the stream, with timing events; no host synchronisation.
-int enqueue_spectra(ysg_handle* h)
+// K2 (all slots) -> K1 -> K3 (all slots) on the stream, with timing events
+// between the stage groups; no host synchronisation.
+int enqueue_spectra(ysg_handle* h, int nev)
 {
-    const EventDev& d = h->pev;
-    const int nr = h->p_nr, nw = d.nw;
-    const size_t nspec = (size_t)nw * std::max(nr, 1);
-    cd* d_ur = h->spec.as<cd>();
-    CK(cudaEventRecord(h->ev[0], h->st));
-    CK(launch_legendre(nr, h->p_lmax, h->delta.as<double>(), h->ct.as<double>(), h->stv.as<double>(),
-                       h->leg.as<double>(), h->st));
-    CK(cudaEventRecord(h->ev[1], h->st));
-    int rc = enqueue_solve(h);
+    CK(record(h, 0));
+    for (int e = 0; e < nev; e++) {
+        Slot& s = h->slots[(size_t)e];
+        CK(launch_legendre(s.nr, s.lmax, s.delta.as<double>(), s.ct.as<double>(), s.stv.as<double>(),
+                           s.leg.as<double>(), h->st));
+    }
+    CK(record(h, 1));
+    int rc = enqueue_solve(h, nev);
     if (rc) return rc;
-    CK(cudaEventRecord(h->ev[2], h->st));
-    CK(launch_lsum(nw, nr, d.lmin, d.lmax, h->coef.as<cd>(), h->leg.as<double>(), h->E.as<cd>(),
-                   d_ur, d_ur + nspec, d_ur + 2 * nspec, h->st));
-    CK(cudaEventRecord(h->ev[3], h->st));
+    CK(record(h, 2));
+    for (int e = 0; e < nev; e++) {
+        Slot& s = h->slots[(size_t)e];
+        const EventDev& d = s.pev;
+        const size_t nspec = (size_t)d.nw * std::max(s.nr, 1);
+        cd* d_ur = s.spec.as<cd>();
+        CK(launch_lsum(d.nw, s.nr, d.lmin, d.lmax, s.coef.as<cd>(), s.leg.as<double>(), s.E.as<cd>(),
+                       d_ur, d_ur + nspec, d_ur + 2 * nspec, h->st));
+    }
+    CK(record(h, 3));
     return YSG_OK;
 }
 
-int enqueue_traces(ysg_handle* h)
+// K4 for slots 0..nev-1.  They share the scratch rows, so they run in order.
+int enqueue_traces(ysg_handle* h, int nev)
 {
-    const TraceDev& td = h->ptd;
-    const size_t nspec = (size_t)td.nw * std::max(td.nr, 1);
-    const cd* d_ur = h->spec.as<cd>();
-    CK(cudaEventRecord(h->ev[3], h->st));
-    CK(launch_ifft(td, d_ur, d_ur + nspec, d_ur + 2 * nspec, h->filt.as<double>(), h->tw.as<cd>(),
-                   h->expt.as<double>(), h->cs.as<double>(), h->scratch.as<cd>(), h->out.as<double>(),
-                   h->st));
-    CK(cudaEventRecord(h->ev[4], h->st));
+    CK(record(h, 3));
+    for (int e = 0; e < nev; e++) {
+        Slot& s = h->slots[(size_t)e];
+        const TraceDev& td = s.ptd;
+        const size_t nspec = (size_t)td.nw * std::max(td.nr, 1);
+        const cd* d_ur = s.spec.as<cd>();
+        CK(launch_ifft(td, d_ur, d_ur + nspec, d_ur + 2 * nspec, s.filt.as<double>(), s.tw.as<cd>(),
+                       s.expt.as<double>(), s.cs.as<double>(), h->scratch.as<cd>(), s.out.as<double>(),
+                       h->st));
+    }
+    CK(record(h, 4));
     return YSG_OK;
 }
 
 // Wait for the stream, read the solve counters and the status word.
-int finish(ysg_handle* h, bool spectra, bool traces)
+int finish(ysg_handle* h, int nev, bool spectra, bool traces)
 {
     unsigned long long w[NSYS_COUNT] = {};
     int status = 0;
@@ -382,31 +442,94 @@ int finish(ysg_handle* h, bool spectra, bool traces)
         double fl = 0.0;
         for (int q = 0; q < NSYS_COUNT; q++) fl += (double)w[q] * kStepFlops[q];
         h->flops = fl;
-        h->pairs = (double)(h->pev.lmax - h->pev.lmin + 1) * h->pev.nw;
-        cudaEventElapsedTime(&h->ms[0], h->ev[0], h->ev[1]);
-        cudaEventElapsedTime(&h->ms[1], h->ev[1], h->ev[2]);
-        cudaEventElapsedTime(&h->ms[2], h->ev[2], h->ev[3]);
+        double pairs = 0.0;
+        for (int e = 0; e < nev; e++) {
+            const EventDev& d = h->slots[(size_t)e].pev;
+            pairs += (double)(d.lmax - d.lmin + 1) * d.nw;
+        }
+        h->pairs = pairs;
+        CK(cudaEventElapsedTime(&h->ms[0], h->ev[0], h->ev[1]));
+        CK(cudaEventElapsedTime(&h->ms[1], h->ev[1], h->ev[2]));
+        CK(cudaEventElapsedTime(&h->ms[2], h->ev[2], h->ev[3]));
         h->has_spectra = status == 0;
     }
-    if (traces) cudaEventElapsedTime(&h->ms[3], h->ev[3], h->ev[4]);
+    if (traces) CK(cudaEventElapsedTime(&h->ms[3], h->ev[3], h->ev[4]));
     return status ? YSG_ERR_DEVICE_WAIT : YSG_OK;
 }
 
-int copy_out(ysg_handle* h, double* out, int* nout)
+int copy_out(ysg_handle* h, const Slot& s, double* out, int* nout)
 {
-    const TraceDev& td = h->ptd;
+    const TraceDev& td = s.ptd;
     if (nout) *nout = td.nout;
     if (out && td.nr > 0) {
-        CK(cudaMemcpyAsync(out, h->out.p, (size_t)td.nout * 4 * td.nr * sizeof(double),
+        CK(cudaMemcpyAsync(out, s.out.p, (size_t)td.nout * 4 * td.nr * sizeof(double),
                            cudaMemcpyDeviceToHost, h->st));
         h->d2h += (double)td.nout * 4 * td.nr * sizeof(double);
     }
     return YSG_OK;
 }
 
+Slot& slot0(ysg_handle* h)
+{
+    if (h->slots.empty()) h->slots.resize(1);
+    return h->slots[0];
+}
+
+// Upload one event into slot 0 (and its work items for the batched solver).
+int prepare_single(ysg_handle* h, const ysg_event* ev)
+{
+    Slot& s = slot0(h);
+    int rc = upload_event(h, s, ev);
+    if (rc) return rc;
+    h->nactive = 1;
+    if (h->solver == 1) return upload_batch_items(h, 1);
+    return YSG_OK;
+}
+
+// Capture the whole batch (K2, K1, K3, K4 of slots 0..nev-1) into a CUDA
+// graph and launch it.  A graph of the same shape as the previous batch
+// updates the instantiated one in place.
+int launch_batch_graph(ysg_handle* h, int nev)
+{
+    CK(cudaStreamBeginCapture(h->st, cudaStreamCaptureModeRelaxed));
+    h->capturing = true;
+    int rc = enqueue_spectra(h, nev);
+    if (!rc) rc = enqueue_traces(h, nev);
+    h->capturing = false;
+    cudaGraph_t g = nullptr;
+    cudaError_t ce = cudaStreamEndCapture(h->st, &g);
+    if (rc || ce != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        return rc ? rc : YSG_ERR_CUDA;
+    }
+    bool updated = false;
+    if (h->gexec) {
+        cudaGraphExecUpdateResultInfo info;
+        updated = cudaGraphExecUpdate(h->gexec, g, &info) == cudaSuccess;
+        if (!updated) {
+            cudaGetLastError();
+            cudaGraphExecDestroy(h->gexec);
+            h->gexec = nullptr;
+        }
+    }
+    if (!updated) {
+        ce = cudaGraphInstantiate(&h->gexec, g, 0);
+        if (ce != cudaSuccess) {
+            h->gexec = nullptr;
+            cudaGraphDestroy(g);
+            return YSG_ERR_CUDA;
+        }
+    }
+    cudaGraphDestroy(g);
+    CK(cudaGraphLaunch(h->gexec, h->st));
+    return YSG_OK;
+}
+
 }  // namespace
 
 extern "C" {
+
+const char* ysg_last_cuda_error(void) { return g_cuda_err; }
 
 const char* ysg_status_string(int s)
 {
@@ -452,9 +575,10 @@ void ysg_destroy(ysg_handle* h)
     if (!h) return;
     cudaSetDevice(h->device);
     if (h->st) cudaStreamSynchronize(h->st);
-    for (DevBuf* b : {&h->kn, &h->sg, &h->coef, &h->leg, &h->E, &h->delta, &h->ct, &h->stv, &h->spec,
-                      &h->filt, &h->tw, &h->expt, &h->cs, &h->scratch, &h->out, &h->work,
-                      &h->status, &h->items, &h->counter, &h->evdev, &h->coefptr})
+    if (h->gexec) cudaGraphExecDestroy(h->gexec);
+    for (Slot& s : h->slots) s.release();
+    for (DevBuf* b : {&h->kn, &h->sg, &h->scratch, &h->work, &h->status, &h->items, &h->counter,
+                      &h->evdev, &h->coefptr})
         b->release();
     for (auto& e : h->ev)
         if (e) cudaEventDestroy(e);
@@ -466,6 +590,8 @@ int ysg_set_solver(ysg_handle* h, int which)
 {
     if (!h || which < 0 || which > 1) return YSG_ERR_ARG;
     h->solver = which;
+    h->nactive = 0;          // work items depend on the solver: prepare again
+    h->has_spectra = false;
     return YSG_OK;
 }
 
@@ -542,7 +668,8 @@ int ysg_model_upload(ysg_handle* h, const ysg_model* m)
     h->hdr = hd;
     h->grav_host.assign(m->val[P_GRAV], m->val[P_GRAV] + n);
     h->has_model = true;
-    h->has_spectra = h->ev_ready = h->tm_ready = false;
+    h->has_spectra = false;
+    for (Slot& s : h->slots) s.ev_ready = s.tm_ready = false;
     return YSG_OK;
 }
 
@@ -563,18 +690,18 @@ int ysg_event_coef(ysg_handle* h, const ysg_event* ev, double* coef)
     int rc = check_event(h, ev);
     if (rc) return rc;
     cudaSetDevice(h->device);
-    h->has_spectra = h->tm_ready = false;
-    rc = upload_event(h, ev);
+    h->has_spectra = false;
+    rc = prepare_single(h, ev);
     if (rc) return rc;
-    CK(cudaEventRecord(h->ev[0], h->st));
-    CK(cudaEventRecord(h->ev[1], h->st));
-    rc = enqueue_solve(h);
+    CK(record(h, 0));
+    CK(record(h, 1));
+    rc = enqueue_solve(h, 1);
     if (rc) return rc;
-    CK(cudaEventRecord(h->ev[2], h->st));
-    CK(cudaEventRecord(h->ev[3], h->st));
+    CK(record(h, 2));
+    CK(record(h, 3));
     const size_t n = (size_t)(ev->lmax - ev->lmin + 1) * NCOEF * ev->nw;
-    if (coef) CK(cudaMemcpyAsync(coef, h->coef.p, n * sizeof(cd), cudaMemcpyDeviceToHost, h->st));
-    rc = finish(h, true, false);
+    if (coef) CK(cudaMemcpyAsync(coef, slot0(h).coef.p, n * sizeof(cd), cudaMemcpyDeviceToHost, h->st));
+    rc = finish(h, 1, true, false);
     h->has_spectra = false;
     return rc;
 }
@@ -585,19 +712,21 @@ int ysg_legendre_table(ysg_handle* h, int nr, int lmax, const double* delta, con
     if (!h || nr < 0 || lmax < 0 || (nr > 0 && (!delta || !ct || !st || !table))) return YSG_ERR_ARG;
     if (nr == 0) return YSG_OK;
     cudaSetDevice(h->device);
-    CK(h->delta.ensure((size_t)nr * sizeof(double)));
-    CK(h->ct.ensure((size_t)nr * sizeof(double)));
-    CK(h->stv.ensure((size_t)nr * sizeof(double)));
+    Slot& s = slot0(h);
+    s.ev_ready = s.tm_ready = false;
+    h->has_spectra = false;
+    CK(s.delta.ensure((size_t)nr * sizeof(double)));
+    CK(s.ct.ensure((size_t)nr * sizeof(double)));
+    CK(s.stv.ensure((size_t)nr * sizeof(double)));
     const size_t nt = (size_t)(lmax + 1) * nr * 8;
-    CK(h->leg.ensure(nt * sizeof(double)));
-    CK(cudaMemcpyAsync(h->delta.p, delta, (size_t)nr * sizeof(double), cudaMemcpyHostToDevice, h->st));
-    CK(cudaMemcpyAsync(h->ct.p, ct, (size_t)nr * sizeof(double), cudaMemcpyHostToDevice, h->st));
-    CK(cudaMemcpyAsync(h->stv.p, st, (size_t)nr * sizeof(double), cudaMemcpyHostToDevice, h->st));
-    CK(launch_legendre(nr, lmax, h->delta.as<double>(), h->ct.as<double>(), h->stv.as<double>(),
-                       h->leg.as<double>(), h->st));
-    CK(cudaMemcpyAsync(table, h->leg.p, nt * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+    CK(s.leg.ensure(nt * sizeof(double)));
+    CK(cudaMemcpyAsync(s.delta.p, delta, (size_t)nr * sizeof(double), cudaMemcpyHostToDevice, h->st));
+    CK(cudaMemcpyAsync(s.ct.p, ct, (size_t)nr * sizeof(double), cudaMemcpyHostToDevice, h->st));
+    CK(cudaMemcpyAsync(s.stv.p, st, (size_t)nr * sizeof(double), cudaMemcpyHostToDevice, h->st));
+    CK(launch_legendre(nr, lmax, s.delta.as<double>(), s.ct.as<double>(), s.stv.as<double>(),
+                       s.leg.as<double>(), h->st));
+    CK(cudaMemcpyAsync(table, s.leg.p, nt * sizeof(double), cudaMemcpyDeviceToHost, h->st));
     CK(cudaStreamSynchronize(h->st));
-    h->has_spectra = h->ev_ready = false;
     return YSG_OK;
 }
 
@@ -606,35 +735,36 @@ int ysg_event_spectra(ysg_handle* h, const ysg_event* ev, double* ur, double* ut
     int rc = check_event(h, ev);
     if (rc) return rc;
     cudaSetDevice(h->device);
-    h->has_spectra = h->tm_ready = false;
-    rc = upload_event(h, ev);
+    h->has_spectra = false;
+    rc = prepare_single(h, ev);
     if (rc) return rc;
-    rc = enqueue_spectra(h);
+    rc = enqueue_spectra(h, 1);
     if (rc) return rc;
     const int nr = ev->nr, nw = ev->nw;
     const size_t nspec = (size_t)nw * std::max(nr, 1);
-    const cd* d_ur = h->spec.as<cd>();
+    const cd* d_ur = slot0(h).spec.as<cd>();
     const size_t nb = (size_t)nw * nr * sizeof(cd);
     if (ur && nr > 0) CK(cudaMemcpyAsync(ur, d_ur, nb, cudaMemcpyDeviceToHost, h->st));
     if (ut && nr > 0) CK(cudaMemcpyAsync(ut, d_ur + nspec, nb, cudaMemcpyDeviceToHost, h->st));
     if (up && nr > 0) CK(cudaMemcpyAsync(up, d_ur + 2 * nspec, nb, cudaMemcpyDeviceToHost, h->st));
-    return finish(h, true, false);
+    return finish(h, 1, true, false);
 }
 
 int ysg_event_traces(ysg_handle* h, const ysg_time* tm, double* out, int* nout)
 {
     if (!h || !tm) return YSG_ERR_ARG;
-    if (!h->has_spectra || !h->ev_ready) return YSG_ERR_NO_SPECTRA;
-    if (tm->nr != h->p_nr) return YSG_ERR_ARG;
+    if (!h->has_spectra || h->nactive != 1 || !slot0(h).ev_ready) return YSG_ERR_NO_SPECTRA;
+    Slot& s = slot0(h);
+    if (tm->nr != s.nr) return YSG_ERR_ARG;
     if (tm->nr > 0 && !out) return YSG_ERR_ARG;
     cudaSetDevice(h->device);
-    int rc = upload_time(h, tm, h->pev.nw);
+    int rc = upload_time(h, s, tm, s.pev.nw);
     if (rc) return rc;
-    rc = enqueue_traces(h);
+    rc = enqueue_traces(h, 1);
     if (rc) return rc;
-    rc = copy_out(h, out, nout);
+    rc = copy_out(h, s, out, nout);
     if (rc) return rc;
-    return finish(h, false, true);
+    return finish(h, 1, false, true);
 }
 
 int ysg_event_prepare(ysg_handle* h, const ysg_event* ev, const ysg_time* tm)
@@ -643,31 +773,31 @@ int ysg_event_prepare(ysg_handle* h, const ysg_event* ev, const ysg_time* tm)
     if (rc) return rc;
     if (!tm || tm->nr != ev->nr) return YSG_ERR_ARG;
     cudaSetDevice(h->device);
-    h->has_spectra = h->ev_ready = h->tm_ready = false;
+    h->has_spectra = false;
     h->h2d = h->d2h = 0.0;
-    rc = upload_event(h, ev);
+    rc = prepare_single(h, ev);
     if (rc) return rc;
-    return upload_time(h, tm, ev->nw);
+    return upload_time(h, slot0(h), tm, ev->nw);
 }
 
 int ysg_event_execute(ysg_handle* h)
 {
     if (!h) return YSG_ERR_ARG;
-    if (!h->ev_ready || !h->tm_ready) return YSG_ERR_NO_SPECTRA;
+    if (h->nactive != 1 || !slot0(h).ev_ready || !slot0(h).tm_ready) return YSG_ERR_NO_SPECTRA;
     cudaSetDevice(h->device);
-    int rc = enqueue_spectra(h);
+    int rc = enqueue_spectra(h, 1);
     if (rc) return rc;
-    return enqueue_traces(h);
+    return enqueue_traces(h, 1);
 }
 
 int ysg_event_fetch(ysg_handle* h, double* out, int* nout)
 {
     if (!h) return YSG_ERR_ARG;
-    if (!h->ev_ready || !h->tm_ready) return YSG_ERR_NO_SPECTRA;
+    if (h->nactive != 1 || !slot0(h).ev_ready || !slot0(h).tm_ready) return YSG_ERR_NO_SPECTRA;
     cudaSetDevice(h->device);
-    int rc = copy_out(h, out, nout);
+    int rc = copy_out(h, slot0(h), out, nout);
     if (rc) return rc;
-    return finish(h, true, true);
+    return finish(h, 1, true, true);
 }
 
 int ysg_event_run(ysg_handle* h, const ysg_event* ev, const ysg_time* tm, double* out, int* nout)
@@ -685,10 +815,34 @@ int ysg_batch_run(ysg_handle* h, int nev, const ysg_event* evs, const ysg_time* 
 {
     if (!h || nev < 0 || (nev > 0 && (!evs || !tms || !outs))) return YSG_ERR_ARG;
     for (int e = 0; e < nev; e++) {
-        int rc = ysg_event_run(h, &evs[e], &tms[e], outs[e], nouts ? &nouts[e] : nullptr);
+        int rc = check_event(h, &evs[e]);
+        if (rc) return rc;
+        if (tms[e].nr != evs[e].nr || (evs[e].nr > 0 && !outs[e])) return YSG_ERR_ARG;
+    }
+    if (nev == 0) return YSG_OK;
+    cudaSetDevice(h->device);
+    h->has_spectra = false;
+    h->nactive = 0;
+    h->h2d = h->d2h = 0.0;
+    if (h->slots.size() < (size_t)nev) h->slots.resize((size_t)nev);
+    for (int e = 0; e < nev; e++) {
+        Slot& s = h->slots[(size_t)e];
+        int rc = upload_event(h, s, &evs[e]);
+        if (!rc) rc = upload_time(h, s, &tms[e], evs[e].nw);
         if (rc) return rc;
     }
-    return YSG_OK;
+    if (h->solver == 1) {
+        int rc = upload_batch_items(h, nev);
+        if (rc) return rc;
+    }
+    h->nactive = nev;
+    int rc = launch_batch_graph(h, nev);
+    if (rc) return rc;
+    for (int e = 0; e < nev; e++) {
+        rc = copy_out(h, h->slots[(size_t)e], outs[e], nouts ? &nouts[e] : nullptr);
+        if (rc) return rc;
+    }
+    return finish(h, nev, true, true);
 }
 
 int ysg_last_bytes(ysg_handle* h, double* h2d, double* d2h)

@@ -76,7 +76,7 @@ EXPORTS = [
     "ysg_event_run", "ysg_event_prepare", "ysg_event_execute", "ysg_event_fetch", "ysg_get_stream",
     "ysg_batch_run", "ysg_event_coef", "ysg_legendre_table", "ysg_set_solver",
     "ysg_last_timings", "ysg_last_work", "ysg_last_bytes", "ysg_fp64_peak", "ysg_status_string",
-    "ysg_destroy",
+    "ysg_last_cuda_error", "ysg_destroy", "ysg_traces_noalloc",
     "ysh_norms_get", "ysh_read_params", "ysh_free_params", "ysh_read_model", "ysh_model_view",
     "ysh_model_nknot", "ysh_model_array", "ysh_free_model", "ysh_event_setup", "ysh_free_event",
     "ysh_write_traces", "ysh_run", "ysh_free", "ysh_status_string",
@@ -88,6 +88,8 @@ _lib = None
 class YspecError(RuntimeError):
     def __init__(self, status: int, where: str):
         msg = lib().ysh_status_string(status).decode()
+        if status == 2:
+            msg += ": " + lib().ysg_last_cuda_error().decode()
         super().__init__(f"{where}: status {status}: {msg}")
         self.status = status
 
@@ -122,6 +124,8 @@ def lib() -> C.CDLL:
     L.ysg_fp64_peak.argtypes = [C.c_int, _dp]
     L.ysg_status_string.argtypes = [C.c_int]
     L.ysg_status_string.restype = C.c_char_p
+    L.ysg_last_cuda_error.argtypes = []
+    L.ysg_last_cuda_error.restype = C.c_char_p
     L.ysg_destroy.argtypes = [vp]
     L.ysg_destroy.restype = None
     L.ysh_norms_get.argtypes = [C.POINTER(YshNorms)]
