@@ -169,6 +169,11 @@ int ysg_legendre_table(ysg_handle *h, int nr, int lmax, const double *delta, con
  * event per launch), 1 = batched persistent (default). */
 int ysg_set_solver(ysg_handle *h, int which);
 
+/* Schedule of the batched solver: 0 = four 64-thread blocks per SM with the
+ * full register budget (default), 1 = five blocks per SM with a tighter
+ * register budget. */
+int ysg_set_schedule(ysg_handle *h, int variant);
+
 /* Device times in ms of the last event's stages, measured with CUDA events
  * on the handle's stream: [0] Legendre table, [1] solves, [2] l-sum,
  * [3] filter + inverse FFT + post-processing. */

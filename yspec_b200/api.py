@@ -133,6 +133,10 @@ class Engine:
     def set_solver(self, which: str) -> None:
         N.check(N.lib().ysg_set_solver(self.h, {"plain": 0, "batched": 1}[which]), "set_solver")
 
+    def set_schedule(self, variant: int) -> None:
+        """Batched-solver schedule (0: 4 blocks/SM, full registers; 1: 5 blocks/SM)."""
+        N.check(N.lib().ysg_set_schedule(self.h, variant), "set_schedule")
+
     def upload(self, model: Model) -> None:
         v = model.view()
         N.check(N.lib().ysg_model_upload(self.h, C.byref(v)), "model_upload")

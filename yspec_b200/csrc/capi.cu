@@ -86,7 +86,7 @@ struct ysg_handle {
     cudaEvent_t ev[5] = {};
     int solver = 1;
     // model
-    DevBuf kn, sg;
+    DevBuf kn, sg, hdr_dev;
     ModelHdr hdr{};
     std::vector<double> grav_host;   // knot gravity for the tilt correction
     bool has_model = false;
@@ -95,7 +95,9 @@ struct ysg_handle {
     int nactive = 0;                 // slots of the last prepare / batch
     DevBuf scratch;                  // inverse-FFT rows, shared by the slots (stages run in order)
     DevBuf work, status, items, counter, evdev, coefptr;
-    int nitems = 0, solve_blocks = 0, solve_block = 64;
+    int nitems = 0;
+    int variant = 0;                 // batched-solver register budget (launch_solve_batched)
+    int solve_blocks[2] = {0, 0};    // resident grid per variant
     bool has_spectra = false;
     // CUDA graph of the last batch (updated in place when the shape repeats)
     cudaGraphExec_t gexec = nullptr;
@@ -241,7 +243,9 @@ int upload_items(ysg_handle* h, std::vector<Item>& items, const std::vector<Even
     h->h2d += (double)(packed.size() * sizeof(int4) + evs.size() * sizeof(EventDev) +
                        coefs.size() * sizeof(cd*));
     h->nitems = (int)packed.size();
-    if (h->solve_blocks == 0) h->solve_blocks = solve_batched_blocks(h->solve_block);
+    for (int v = 0; v < solve_batched_variants() && v < 2; v++)
+        if (h->solve_blocks[v] == 0) h->solve_blocks[v] = solve_batched_blocks(v);
+    if (h->solve_blocks[h->variant] == 0) return YSG_ERR_CUDA;
     return YSG_OK;
 }
 
@@ -377,10 +381,10 @@ int enqueue_solve(ysg_handle* h, int nev)
                                   h->work.as<unsigned long long>(), h->status.as<int>(), h->st));
         }
     } else {
-        CK(launch_solve_batched(h->kn.as<Knot>(), h->sg.as<Seg>(), h->hdr, h->evdev.as<EventDev>(),
-                                h->coefptr.as<cd*>(), h->items.as<int4>(), h->nitems,
-                                h->counter.as<int>(), h->work.as<unsigned long long>(),
-                                h->solve_blocks, h->solve_block, h->st));
+        CK(launch_solve_batched(h->variant, h->kn.as<Knot>(), h->sg.as<Seg>(), h->hdr_dev.as<ModelHdr>(),
+                                h->evdev.as<EventDev>(), h->coefptr.as<cd*>(), h->items.as<int4>(),
+                                h->nitems, h->counter.as<int>(), h->work.as<unsigned long long>(),
+                                h->solve_blocks[h->variant], h->st));
     }
     return YSG_OK;
 }
@@ -577,7 +581,7 @@ void ysg_destroy(ysg_handle* h)
     if (h->st) cudaStreamSynchronize(h->st);
     if (h->gexec) cudaGraphExecDestroy(h->gexec);
     for (Slot& s : h->slots) s.release();
-    for (DevBuf* b : {&h->kn, &h->sg, &h->scratch, &h->work, &h->status, &h->items, &h->counter,
+    for (DevBuf* b : {&h->kn, &h->sg, &h->hdr_dev, &h->scratch, &h->work, &h->status, &h->items, &h->counter,
                       &h->evdev, &h->coefptr})
         b->release();
     for (auto& e : h->ev)
@@ -592,6 +596,13 @@ int ysg_set_solver(ysg_handle* h, int which)
     h->solver = which;
     h->nactive = 0;          // work items depend on the solver: prepare again
     h->has_spectra = false;
+    return YSG_OK;
+}
+
+int ysg_set_schedule(ysg_handle* h, int variant)
+{
+    if (!h || variant < 0 || variant >= solve_batched_variants()) return YSG_ERR_ARG;
+    h->variant = variant;
     return YSG_OK;
 }
 
@@ -664,6 +675,8 @@ int ysg_model_upload(ysg_handle* h, const ysg_model* m)
     CK(cudaMemcpyAsync(h->kn.p, rec.data(), rec.size() * sizeof(Knot), cudaMemcpyHostToDevice, h->st));
     CK(h->sg.ensure(seg.size() * sizeof(Seg)));
     CK(cudaMemcpyAsync(h->sg.p, seg.data(), seg.size() * sizeof(Seg), cudaMemcpyHostToDevice, h->st));
+    CK(h->hdr_dev.ensure(sizeof(ModelHdr)));
+    CK(cudaMemcpyAsync(h->hdr_dev.p, &hd, sizeof(ModelHdr), cudaMemcpyHostToDevice, h->st));
     CK(cudaStreamSynchronize(h->st));
     h->hdr = hd;
     h->grav_host.assign(m->val[P_GRAV], m->val[P_GRAV] + n);

@@ -4,10 +4,13 @@
 // (omega_j, l)), organised for the B200:
 //   * one thread per pair, but the five Cash-Karp stage vectors of the
 //     14-component minor / b-vector systems live in a per-thread slab of
-//     shared memory (70 complex entries, interleaved across the lanes of a
-//     warp so accesses are bank-conflict free and every offset is a
-//     constant); y and the stage input stay in registers.  The plain form
-//     keeps them in local memory, which spills through L1 into L2.
+//     shared memory (70 complex values, 1120 bytes), interleaved across the
+//     lanes of a warp so accesses are bank-conflict free and every offset is
+//     a constant; y and the stage input stay in registers.  Three 64-thread
+//     blocks share an SM.  (Folding the stages into partial sums needs only
+//     four slots and fits a fourth block, but the extra stage code overflows
+//     the instruction cache: measured slower.)  The plain form keeps all
+//     stage vectors in local memory, which spills through L1 into L2.
 //   * a persistent grid (resident blocks only) pulls work items from an
 //     atomic counter.  An item is (event, l, 32 consecutive frequencies):
 //     the lanes of a warp share l and step through nearly identical radial
@@ -22,24 +25,26 @@
 
 namespace ysg {
 
-constexpr int SLAB = 5 * 14;     // complex entries per thread
+constexpr int SLAB = 5 * 14;     // complex entries per thread (five stage slots)
 
-__global__ void __launch_bounds__(64) k_solve_batched(const Knot* __restrict__ kn,
-                                                      const Seg* __restrict__ sg, ModelHdr mh_in,
+// MINB = resident blocks per SM the registers are budgeted for (the shared
+// memory admits three): 3 keeps the full 255 registers per thread.
+template <int MINB>
+__global__ void __launch_bounds__(64, MINB) k_solve_batched(const Knot* __restrict__ kn,
+                                                      const Seg* __restrict__ sg,
+                                                      const ModelHdr* __restrict__ mh,
                                                       const EventDev* __restrict__ evs,
                                                       cd* const* __restrict__ coefs,
                                                       const int4* __restrict__ items, int nitems,
                                                       int* counter,
                                                       unsigned long long* __restrict__ work)
 {
+    // the slab is all the shared memory a block has: four blocks fill the SM
     extern __shared__ cd slab[];
-    __shared__ ModelHdr mh;
-    if (threadIdx.x == 0) mh = mh_in;
-    __syncthreads();
     const int lane = threadIdx.x & 31;
     Ctx c;
     c.kn = kn;
-    c.mh = &mh;
+    c.mh = mh;
     c.sg = sg;
     c.kb = slab + (threadIdx.x >> 5) * (SLAB * KS) + lane;
     for (int q = 0; q < NSYS; q++) c.nst[q] = 0;
@@ -74,35 +79,49 @@ __global__ void __launch_bounds__(64) k_solve_batched(const Knot* __restrict__ k
     }
 }
 
-size_t solve_batched_smem(int block) { return (size_t)block * SLAB * sizeof(cd); }
+namespace {
 
-int solve_batched_blocks(int block)
+constexpr int kBlock = 64;
+
+using SolveFn = void (*)(const Knot*, const Seg*, const ModelHdr*, const EventDev*, cd* const*,
+                         const int4*, int, int*, unsigned long long*);
+
+SolveFn solve_fn(int) { return k_solve_batched<3>; }
+
+size_t solve_smem() { return (size_t)kBlock * SLAB * sizeof(cd); }
+
+}  // namespace
+
+int solve_batched_variants() { return 1; }
+
+int solve_batched_blocks(int variant)
 {
     int dev = 0, nsm = 0, per = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    cudaFuncSetAttribute(k_solve_batched, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)solve_batched_smem(block));
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_solve_batched, block,
-                                                  solve_batched_smem(block));
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        return 0;
+    SolveFn f = solve_fn(variant);
+    if (cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)solve_smem()) !=
+            cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, f, kBlock, solve_smem()) != cudaSuccess)
+        return 0;
     if (per < 1) per = 1;
     return nsm * per;
 }
 
-cudaError_t launch_solve_batched(const Knot* kn, const Seg* sg, const ModelHdr& mh,
-                                 const EventDev* evs_dev,
-                                 cd* const* coefs_dev, const int4* items, int nitems, int* counter,
-                                 unsigned long long* work, int nblocks, int block, cudaStream_t st)
+cudaError_t launch_solve_batched(int variant, const Knot* kn, const Seg* sg, const ModelHdr* mh,
+                                 const EventDev* evs_dev, cd* const* coefs_dev, const int4* items,
+                                 int nitems, int* counter, unsigned long long* work, int nblocks,
+                                 cudaStream_t st)
 {
     if (nitems <= 0) return cudaSuccess;
-    size_t smem = solve_batched_smem(block);
-    cudaError_t e = cudaFuncSetAttribute(k_solve_batched, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
+    SolveFn f = solve_fn(variant);
+    cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)solve_smem());
     if (e != cudaSuccess) return e;
     e = cudaMemsetAsync(counter, 0, sizeof(int), st);
     if (e != cudaSuccess) return e;
-    k_solve_batched<<<nblocks, block, smem, st>>>(kn, sg, mh, evs_dev, coefs_dev, items, nitems,
-                                                 counter, work);
+    f<<<nblocks, kBlock, solve_smem(), st>>>(kn, sg, mh, evs_dev, coefs_dev, items, nitems, counter,
+                                             work);
     return cudaGetLastError();
 }
 

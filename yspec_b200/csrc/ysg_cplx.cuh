@@ -11,7 +11,9 @@
 
 namespace ysg {
 
-struct cd {
+// 16-byte aligned so that a complex value moves with one 128-bit load or
+// store (shared, global and local memory alike).
+struct __align__(16) cd {
     double x, y;
 };
 

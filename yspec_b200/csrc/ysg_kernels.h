@@ -16,12 +16,14 @@ cudaError_t launch_solve_plain(const Knot* kn, const Seg* sg, const ModelHdr& mh
 // K1 batched persistent: work items (event, l index, first frequency - 1)
 // of one or more events, one thread per (omega,l) pair, stage vectors in
 // shared memory.  counter must be device memory (reset by the launcher).
-size_t solve_batched_smem(int block);
-int solve_batched_blocks(int block);
-cudaError_t launch_solve_batched(const Knot* kn, const Seg* sg, const ModelHdr& mh,
-                                 const EventDev* evs_dev,
-                                 cd* const* coefs_dev, const int4* items, int nitems, int* counter,
-                                 unsigned long long* work, int nblocks, int block, cudaStream_t st);
+// `variant` selects the register budget (0: four 64-thread blocks per SM,
+// 1: five); solve_batched_blocks gives the resident grid of a variant.
+int solve_batched_variants();
+int solve_batched_blocks(int variant);
+cudaError_t launch_solve_batched(int variant, const Knot* kn, const Seg* sg, const ModelHdr* mh,
+                                 const EventDev* evs_dev, cd* const* coefs_dev, const int4* items,
+                                 int nitems, int* counter, unsigned long long* work, int nblocks,
+                                 cudaStream_t st);
 
 // K2: Legendre table, T[((l * nr) + k) * 8 + q].
 cudaError_t launch_legendre(int nr, int lmax, const double* delta, const double* ct,

@@ -1,9 +1,10 @@
 """Time the device stages of a synthetic workload configuration.
 
-    python -m yspec_b200.stages c2 [--solver batched|plain] [--reps 3]
-                                   [--seed 0] [--set lmax=300 --set fmax=20.0]
+    python -m yspec_b200.stages c2 [--solver batched|plain] [--schedule 0|1] [--reps 3]
+                                   [--seed 0] [--set lmax=300 --set fmax=20.0] [--batch]
 
-Runs the configuration's first event through `Engine.run` `reps` times and
+Runs the configuration's first event through `Engine.run` (or, with
+--batch, all its events through one `Engine.batch_run`) `reps` times and
 prints, per run, the device time of each stage (Legendre table, solves,
 l-sum, filter + inverse FFT) measured with CUDA events on the engine's
 stream, the number of (omega,l) solves and the counted FP64 work of the
@@ -35,19 +36,26 @@ def main(argv=None) -> None:
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--event", type=int, default=0, help="event index within the configuration")
+    ap.add_argument("--schedule", type=int, default=0, help="batched-solver schedule variant")
+    ap.add_argument("--batch", action="store_true", help="run every event of the configuration as one batch")
     ap.add_argument("--set", action="append", default=[], metavar="KEY=VALUE",
                     help="override a parameter of the configuration")
     a = ap.parse_args(argv)
-    p = W.config(a.config, seed=a.seed, **_parse_set(a.set))[a.event]
+    ps = W.config(a.config, seed=a.seed, **_parse_set(a.set))
+    if not a.batch:
+        ps = [ps[a.event]]
     eng = Engine(0, solver=a.solver)
+    eng.set_schedule(a.schedule)
     with tempfile.TemporaryDirectory() as tmp:
-        pf = p.write(Path(tmp) / f"{a.config}.in")
-        m = Model(p.model_file)
+        m = Model(ps[0].model_file)
         eng.upload(m)
-        ev = Event(m, Params(pf))
+        evs = [Event(m, Params(p.write(Path(tmp) / f"{a.config}_{i}.in"))) for i, p in enumerate(ps)]
         for rep in range(a.reps):
             t = time.perf_counter()
-            eng.run(ev)
+            if a.batch:
+                eng.batch_run(evs)
+            else:
+                eng.run(evs[0])
             wall = time.perf_counter() - t
             ms = eng.timings()
             pairs, fl = eng.work()
