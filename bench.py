@@ -74,21 +74,26 @@ def batch_compare(local: int, reps: int = 2) -> dict:
         for _ in range(reps):
             t0 = time.perf_counter()
             solve = dev = 0.0
+            launches = 0
             if solver == "batched":
                 eng.batch_run(evs)
                 ms = eng.timings()
                 solve, dev = ms[1], sum(ms)
+                launches = eng.launches()
             else:
                 for e in evs:
                     eng.run(e)
                     ms = eng.timings()
                     solve += ms[1]
                     dev += sum(ms)
+                    launches += eng.launches()
             wall = time.perf_counter() - t0
-            r = {"solve_ms": solve, "device_ms": dev, "wall_ms": 1e3 * wall,
+            r = {"solve_ms": solve, "device_ms": dev, "wall_ms": 1e3 * wall, "gpu_launches": launches,
                  "solves_per_s": pairs / (solve / 1e3),
                  "pipeline_solves_per_s": pairs / (dev / 1e3),
                  "e2e_solves_per_s": pairs / wall, "traces_per_s": traces / (dev / 1e3)}
+            if solver == "batched":
+                r["schedule"], r["autotune_solve_ms"] = eng.last_schedule()
             if best is None or r["device_ms"] < best["device_ms"]:
                 best = r
         res[solver] = best
@@ -261,6 +266,7 @@ def run_b200(args) -> None:
     clocks = Clocks(local)
     barrier()
     torch.cuda.synchronize()
+    launches0 = eng.launches()
     clocks.start()
     for k in range(args.steps):
         with torch.cuda.stream(stream):
@@ -274,6 +280,8 @@ def run_b200(args) -> None:
         flops = eng.work()[1]
     torch.cuda.synchronize()
     clk = clocks.stop()
+    launches = eng.launches() - launches0
+    sched = eng.last_schedule()[0] if args.solver == "batched" else None
     barrier()
     dev_ms = sum(a.elapsed_time(b) for a, b in zip(ev0, ev1))
     dev_ms = allmax(dev_ms)
@@ -308,13 +316,14 @@ def run_b200(args) -> None:
             "data": "synthetic (seeded PREM-like model, receivers, moment tensor)",
             "config": {"workload": WORKLOAD, "pairs_per_event": int(pairs), "receivers": nr,
                        "nt": ev.tm.nt, "trace_rows": nout, "solver": args.solver,
+                       "schedule": sched,
                        "l2": "flushed between timed steps (256 MB write, untimed)",
                        "parallelism": f"replicas x{world}"},
             "traces_per_s": world * nr * args.steps / (dev_ms / 1e3),
             "stage_ms": dict(zip(["legendre", "solve", "lsum", "ifft"], eng.timings())),
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h), "ms_per_step": e_ms / args.steps},
-            "gpu_launches": 6 * args.steps,
+            "gpu_launches": launches,
             "roofline": {"bound": "tensor", "pipe": "fp64 (CUDA-core FMA rate = FP64 tensor rate on B200)",
                          "kernel": "k_solve_batched" if args.solver == "batched" else "k_solve_plain",
                          "achieved": achieved, "peak": peak, "unit": "TFLOP/s",

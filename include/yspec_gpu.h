@@ -169,10 +169,17 @@ int ysg_legendre_table(ysg_handle *h, int nr, int lmax, const double *delta, con
  * event per launch), 1 = batched persistent (default). */
 int ysg_set_solver(ysg_handle *h, int which);
 
-/* Schedule of the batched solver: 0 = four 64-thread blocks per SM with the
- * full register budget (default), 1 = five blocks per SM with a tighter
- * register budget. */
-int ysg_set_schedule(ysg_handle *h, int variant);
+/* Work schedule of the batched solver: 0 = tiles of (event, l, 32
+ * consecutive frequencies) ordered by estimated cost; 1 = lists of 32 pairs
+ * of equal code path and near-equal exact step-count cost (a count-only
+ * pass and a sort before the solve); -1 (default) = autotuned: the first
+ * time a workload signature is seen, the solve stage runs once with each
+ * schedule and the faster is kept.  Results do not depend on the schedule. */
+int ysg_set_schedule(ysg_handle *h, int sched);
+
+/* Schedule of the last batched solve, and the solve-stage times in ms of
+ * each schedule from the last autotuning run (tune_ms may be NULL). */
+int ysg_last_schedule(ysg_handle *h, int *sched, float tune_ms[2]);
 
 /* Device times in ms of the last event's stages, measured with CUDA events
  * on the handle's stream: [0] Legendre table, [1] solves, [2] l-sum,
@@ -182,6 +189,10 @@ int ysg_last_timings(ysg_handle *h, float ms[4]);
 /* Counters of the last solve stage: number of (omega,l) pairs and the
  * algorithmic FP64 flop count of the stepping work actually performed. */
 int ysg_last_work(ysg_handle *h, double *pairs, double *flops);
+
+/* Kernels of this library enqueued since the last ysg_event_prepare (or
+ * ysg_event_run / ysg_batch_run), autotuning runs excluded. */
+int ysg_last_launches(ysg_handle *h, long long *n);
 
 /* Host<->device bytes moved by the last ysg_event_run / prepare+fetch:
  * event inputs and tables copied in, traces copied out. */

@@ -133,9 +133,16 @@ class Engine:
     def set_solver(self, which: str) -> None:
         N.check(N.lib().ysg_set_solver(self.h, {"plain": 0, "batched": 1}[which]), "set_solver")
 
-    def set_schedule(self, variant: int) -> None:
-        """Batched-solver schedule (0: 4 blocks/SM, full registers; 1: 5 blocks/SM)."""
-        N.check(N.lib().ysg_set_schedule(self.h, variant), "set_schedule")
+    def set_schedule(self, sched: int) -> None:
+        """Batched-solver schedule: 0 tiles, 1 cost-sorted pair lists, -1 autotuned."""
+        N.check(N.lib().ysg_set_schedule(self.h, sched), "set_schedule")
+
+    def last_schedule(self) -> tuple[int, list[float]]:
+        """Schedule of the last batched solve and the last autotuning times (ms)."""
+        s = C.c_int()
+        ms = (C.c_float * 2)()
+        N.check(N.lib().ysg_last_schedule(self.h, C.byref(s), ms), "last_schedule")
+        return s.value, list(ms)
 
     def upload(self, model: Model) -> None:
         v = model.view()
@@ -216,6 +223,12 @@ class Engine:
         a, b = C.c_double(), C.c_double()
         N.check(N.lib().ysg_last_bytes(self.h, C.byref(a), C.byref(b)), "bytes")
         return a.value, b.value
+
+    def launches(self) -> int:
+        """Kernels of this library enqueued since the last prepare / run."""
+        n = C.c_longlong()
+        N.check(N.lib().ysg_last_launches(self.h, C.byref(n)), "launches")
+        return n.value
 
     def work(self) -> tuple[float, float]:
         p, f = C.c_double(), C.c_double()

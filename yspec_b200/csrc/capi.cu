@@ -13,9 +13,11 @@
 // ysg_event_prepare / _execute / _fetch expose the three phases so a caller
 // can time the device work alone.
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <vector>
 
 #include "yspec_gpu.h"
@@ -58,9 +60,17 @@ const double kStepFlops[NSYS_COUNT] = {
     6 * 290.0 + 88.0 * 4,    // b-vector, no gravity / Cowling
     6 * 300.0 + 88.0 * 5,    // solid minors, no gravity / Cowling
     6 * 240.0 + 88.0 * 5,    // fluid minors, self-gravitation
-    6 * 700.0 + 88.0 * 14,   // solid minors, self-gravitation
-    6 * 700.0 + 88.0 * 14,   // b-vector, self-gravitation
+    6 * 666.0 + 88.0 * 14,   // solid minors, self-gravitation
+    6 * 666.0 + 88.0 * 14,   // b-vector, self-gravitation
 };
+
+// Work of a pair outside the stepping (start level, start vectors, minor
+// algebra, source vectors), for the scheduler's cost model only.
+constexpr double kPairBaseFlops = 2.0e4;
+
+// Workload signature of the autotuner: events, pairs (to 1%), largest
+// degree and band, gravity switch of the first event, knots.
+using Signature = std::array<long long, 6>;
 
 // Device buffers and uploaded state of one event.  Slot 0 serves the
 // single-event calls; a batch uses slots 0..nev-1.
@@ -95,9 +105,16 @@ struct ysg_handle {
     int nactive = 0;                 // slots of the last prepare / batch
     DevBuf scratch;                  // inverse-FFT rows, shared by the slots (stages run in order)
     DevBuf work, status, items, counter, evdev, coefptr;
-    int nitems = 0;
-    int variant = 0;                 // batched-solver register budget (launch_solve_batched)
-    int solve_blocks[2] = {0, 0};    // resident grid per variant
+    int nitems = 0;                  // schedule-0 tiles
+    long long npairs = 0;            // pairs of the active slots
+    int nev_items = 0;               // slots the items were built for
+    DevBuf offs, keys0, keys1, vals0, vals1, sort_tmp;
+    int sched = -1;                  // batched-solver schedule; -1 = autotuned
+    int cur_sched = 0;               // schedule of the next solve launch
+    std::map<Signature, int> tuned;  // autotuner choices
+    float tune_ms[NSCHED] = {};      // solve times of the last tuning run
+    long long launches = 0;          // this library's kernels enqueued since the last prepare
+    int solve_blocks[NSCHED] = {};   // resident grid per schedule
     bool has_spectra = false;
     // CUDA graph of the last batch (updated in place when the shape repeats)
     cudaGraphExec_t gexec = nullptr;
@@ -239,13 +256,29 @@ int upload_items(ysg_handle* h, std::vector<Item>& items, const std::vector<Even
         CK(cudaMemcpyAsync(h->items.p, packed.data(), packed.size() * sizeof(int4), cudaMemcpyHostToDevice, h->st));
     CK(cudaMemcpyAsync(h->evdev.p, evs.data(), evs.size() * sizeof(EventDev), cudaMemcpyHostToDevice, h->st));
     CK(cudaMemcpyAsync(h->coefptr.p, coefs.data(), coefs.size() * sizeof(cd*), cudaMemcpyHostToDevice, h->st));
+    // flat pair offsets of the events and buffers of the pair schedule
+    std::vector<long long> off(evs.size() + 1, 0);
+    for (size_t e = 0; e < evs.size(); e++)
+        off[e + 1] = off[e] + (long long)(evs[e].lmax - evs[e].lmin + 1) * evs[e].nw;
+    const long long np = off.back();
+    CK(h->offs.ensure(off.size() * sizeof(long long)));
+    CK(cudaMemcpyAsync(h->offs.p, off.data(), off.size() * sizeof(long long), cudaMemcpyHostToDevice, h->st));
+    const size_t pb = (size_t)std::max<long long>(np, 1) * sizeof(unsigned long long);
+    CK(h->keys0.ensure(pb));
+    CK(h->keys1.ensure(pb));
+    CK(h->vals0.ensure(pb));
+    CK(h->vals1.ensure(pb));
+    CK(h->sort_tmp.ensure(std::max<size_t>(pair_sort_tmp_bytes(np), 16)));
     CK(cudaStreamSynchronize(h->st));
     h->h2d += (double)(packed.size() * sizeof(int4) + evs.size() * sizeof(EventDev) +
-                       coefs.size() * sizeof(cd*));
+                       coefs.size() * sizeof(cd*) + off.size() * sizeof(long long));
     h->nitems = (int)packed.size();
-    for (int v = 0; v < solve_batched_variants() && v < 2; v++)
+    h->npairs = np;
+    h->nev_items = (int)evs.size();
+    for (int v = 0; v < NSCHED; v++) {
         if (h->solve_blocks[v] == 0) h->solve_blocks[v] = solve_batched_blocks(v);
-    if (h->solve_blocks[h->variant] == 0) return YSG_ERR_CUDA;
+        if (h->solve_blocks[v] == 0) return YSG_ERR_CUDA;
+    }
     return YSG_OK;
 }
 
@@ -377,15 +410,81 @@ int enqueue_solve(ysg_handle* h, int nev)
     if (h->solver == 0) {
         for (int e = 0; e < nev; e++) {
             const Slot& s = h->slots[(size_t)e];
+            h->launches += 1;
             CK(launch_solve_plain(h->kn.as<Knot>(), h->sg.as<Seg>(), h->hdr, s.pev, s.coef.as<cd>(),
                                   h->work.as<unsigned long long>(), h->status.as<int>(), h->st));
         }
     } else {
-        CK(launch_solve_batched(h->variant, h->kn.as<Knot>(), h->sg.as<Seg>(), h->hdr_dev.as<ModelHdr>(),
+        const int s = h->cur_sched;
+        const unsigned long long* pairs = nullptr;
+        int nitems = h->nitems;
+        if (s == 1) {
+            StepCost sc;
+            for (int q = 0; q < NSYS_COUNT; q++) sc.flops[q] = kStepFlops[q];
+            sc.base = kPairBaseFlops;
+            unsigned long long* keys[2] = {h->keys0.as<unsigned long long>(), h->keys1.as<unsigned long long>()};
+            unsigned long long* vals[2] = {h->vals0.as<unsigned long long>(), h->vals1.as<unsigned long long>()};
+            unsigned long long* sorted = nullptr;
+            h->launches += 1;        // k_pair_cost (the radix sort is CUB's)
+            CK(launch_pair_schedule(h->kn.as<Knot>(), h->sg.as<Seg>(), h->hdr_dev.as<ModelHdr>(),
+                                    h->evdev.as<EventDev>(), h->offs.as<long long>(), h->nev_items,
+                                    h->npairs, sc, keys, vals, h->sort_tmp.p, h->sort_tmp.cap, &sorted,
+                                    h->st));
+            pairs = sorted;
+            nitems = (int)((h->npairs + 31) / 32);
+        }
+        h->launches += 1;
+        CK(launch_solve_batched(s, h->kn.as<Knot>(), h->sg.as<Seg>(), h->hdr_dev.as<ModelHdr>(),
                                 h->evdev.as<EventDev>(), h->coefptr.as<cd*>(), h->items.as<int4>(),
-                                h->nitems, h->counter.as<int>(), h->work.as<unsigned long long>(),
-                                h->solve_blocks[h->variant], h->st));
+                                pairs, h->npairs, nitems, h->counter.as<int>(),
+                                h->work.as<unsigned long long>(), h->solve_blocks[s], h->st));
     }
+    return YSG_OK;
+}
+
+// Choose the batched solver's schedule for the active slots.  A fixed
+// schedule (ysg_set_schedule) is used as is; otherwise the autotuner looks
+// up the workload signature and, the first time it is seen, runs the solve
+// stage once with each schedule (timed with CUDA events on the stream) and
+// keeps the faster.  Every schedule computes every pair with the same
+// per-thread arithmetic, so the coefficients do not depend on the choice.
+int resolve_schedule(ysg_handle* h, int nev)
+{
+    if (h->solver != 1) return YSG_OK;
+    if (h->sched >= 0) {
+        h->cur_sched = h->sched;
+        return YSG_OK;
+    }
+    long long maxl = 0, maxw = 0;
+    for (int e = 0; e < nev; e++) {
+        maxl = std::max<long long>(maxl, h->slots[(size_t)e].pev.lmax);
+        maxw = std::max<long long>(maxw, h->slots[(size_t)e].pev.nw);
+    }
+    long long q = h->npairs;                   // two significant digits
+    long long scale = 1;
+    while (q >= 100) {
+        q /= 10;
+        scale *= 10;
+    }
+    const Signature sig = {nev, q * scale, maxl, maxw, h->slots[0].pev.grav, h->hdr.nknot};
+    auto it = h->tuned.find(sig);
+    if (it != h->tuned.end()) {
+        h->cur_sched = it->second;
+        return YSG_OK;
+    }
+    int best = 0;
+    for (int s = 0; s < NSCHED; s++) {
+        h->cur_sched = s;
+        CK(record(h, 1));
+        int rc = enqueue_solve(h, nev);
+        if (rc) return rc;
+        CK(record(h, 2));
+        CK(cudaStreamSynchronize(h->st));
+        CK(cudaEventElapsedTime(&h->tune_ms[s], h->ev[1], h->ev[2]));
+        if (h->tune_ms[s] < h->tune_ms[best]) best = s;
+    }
+    h->tuned[sig] = best;
+    h->cur_sched = best;
     return YSG_OK;
 }
 
@@ -396,6 +495,7 @@ int enqueue_spectra(ysg_handle* h, int nev)
     CK(record(h, 0));
     for (int e = 0; e < nev; e++) {
         Slot& s = h->slots[(size_t)e];
+        h->launches += s.nr > 0 ? 1 : 0;
         CK(launch_legendre(s.nr, s.lmax, s.delta.as<double>(), s.ct.as<double>(), s.stv.as<double>(),
                            s.leg.as<double>(), h->st));
     }
@@ -408,6 +508,7 @@ int enqueue_spectra(ysg_handle* h, int nev)
         const EventDev& d = s.pev;
         const size_t nspec = (size_t)d.nw * std::max(s.nr, 1);
         cd* d_ur = s.spec.as<cd>();
+        h->launches += s.nr > 0 ? 1 : 0;
         CK(launch_lsum(d.nw, s.nr, d.lmin, d.lmax, s.coef.as<cd>(), s.leg.as<double>(), s.E.as<cd>(),
                        d_ur, d_ur + nspec, d_ur + 2 * nspec, h->st));
     }
@@ -424,6 +525,7 @@ int enqueue_traces(ysg_handle* h, int nev)
         const TraceDev& td = s.ptd;
         const size_t nspec = (size_t)td.nw * std::max(td.nr, 1);
         const cd* d_ur = s.spec.as<cd>();
+        h->launches += td.nr > 0 ? 3 : 0;   // pass A, pass B, rotation
         CK(launch_ifft(td, d_ur, d_ur + nspec, d_ur + 2 * nspec, s.filt.as<double>(), s.tw.as<cd>(),
                        s.expt.as<double>(), s.cs.as<double>(), h->scratch.as<cd>(), s.out.as<double>(),
                        h->st));
@@ -486,7 +588,11 @@ int prepare_single(ysg_handle* h, const ysg_event* ev)
     int rc = upload_event(h, s, ev);
     if (rc) return rc;
     h->nactive = 1;
-    if (h->solver == 1) return upload_batch_items(h, 1);
+    if (h->solver == 1) {
+        rc = upload_batch_items(h, 1);
+        if (!rc) rc = resolve_schedule(h, 1);
+        return rc;
+    }
     return YSG_OK;
 }
 
@@ -581,7 +687,8 @@ void ysg_destroy(ysg_handle* h)
     if (h->st) cudaStreamSynchronize(h->st);
     if (h->gexec) cudaGraphExecDestroy(h->gexec);
     for (Slot& s : h->slots) s.release();
-    for (DevBuf* b : {&h->kn, &h->sg, &h->hdr_dev, &h->scratch, &h->work, &h->status, &h->items, &h->counter,
+    for (DevBuf* b : {&h->kn, &h->sg, &h->hdr_dev, &h->offs, &h->keys0, &h->keys1, &h->vals0,
+                      &h->vals1, &h->sort_tmp, &h->scratch, &h->work, &h->status, &h->items, &h->counter,
                       &h->evdev, &h->coefptr})
         b->release();
     for (auto& e : h->ev)
@@ -599,10 +706,21 @@ int ysg_set_solver(ysg_handle* h, int which)
     return YSG_OK;
 }
 
-int ysg_set_schedule(ysg_handle* h, int variant)
+int ysg_set_schedule(ysg_handle* h, int sched)
 {
-    if (!h || variant < 0 || variant >= solve_batched_variants()) return YSG_ERR_ARG;
-    h->variant = variant;
+    if (!h || sched < -1 || sched >= NSCHED) return YSG_ERR_ARG;
+    h->sched = sched;
+    h->nactive = 0;          // prepare again
+    h->has_spectra = false;
+    return YSG_OK;
+}
+
+int ysg_last_schedule(ysg_handle* h, int* sched, float* tune_ms)
+{
+    if (!h || !sched) return YSG_ERR_ARG;
+    *sched = h->cur_sched;
+    if (tune_ms)
+        for (int s = 0; s < NSCHED; s++) tune_ms[s] = h->tune_ms[s];
     return YSG_OK;
 }
 
@@ -789,6 +907,7 @@ int ysg_event_prepare(ysg_handle* h, const ysg_event* ev, const ysg_time* tm)
     h->has_spectra = false;
     h->h2d = h->d2h = 0.0;
     rc = prepare_single(h, ev);
+    h->launches = 0;          // count the execute's kernels only (not autotuning)
     if (rc) return rc;
     return upload_time(h, slot0(h), tm, ev->nw);
 }
@@ -846,9 +965,11 @@ int ysg_batch_run(ysg_handle* h, int nev, const ysg_event* evs, const ysg_time* 
     }
     if (h->solver == 1) {
         int rc = upload_batch_items(h, nev);
+        if (!rc) rc = resolve_schedule(h, nev);
         if (rc) return rc;
     }
     h->nactive = nev;
+    h->launches = 0;
     int rc = launch_batch_graph(h, nev);
     if (rc) return rc;
     for (int e = 0; e < nev; e++) {
@@ -856,6 +977,13 @@ int ysg_batch_run(ysg_handle* h, int nev, const ysg_event* evs, const ysg_time* 
         if (rc) return rc;
     }
     return finish(h, nev, true, true);
+}
+
+int ysg_last_launches(ysg_handle* h, long long* n)
+{
+    if (!h || !n) return YSG_ERR_ARG;
+    *n = h->launches;
+    return YSG_OK;
 }
 
 int ysg_last_bytes(ysg_handle* h, double* h2d, double* d2h)

@@ -1,0 +1,114 @@
+// k_schedule.cu -- cost model and ordering of the pair schedule.
+//
+// The batched solver can take its work as (event, l, 32 consecutive
+// frequencies) tiles, or as lists of 32 pairs of near-equal cost and the
+// same code path.  The second needs every pair's cost before the solve:
+// k_pair_cost runs each pair's driver (yspec.f90:259-400) in the
+// count-only build of the solver code, where yint makes every integer
+// decision a real solve makes (start level, layers, steps per layer,
+// module_int.f90:1847-1968) but steps no state, so the counts are exact.
+// The cost is the counted FP64 work, sum over systems of steps x flops per
+// step; the path class is the set of systems a pair integrates.  Pairs are
+// then sorted (CUB radix sort, descending) by
+//   key = log-cost bucket (1.1% wide) | path class | flat pair index,
+// so a warp's 32 lanes take the same yint sequence with nearly the same
+// number of steps, and the persistent kernel takes the costliest first.
+#define YSG_COUNT_ONLY 1
+#include "ysg_kernels.h"
+#include "ysg_solvers.cuh"
+
+#include <cub/device/device_radix_sort.cuh>
+
+namespace ysg {
+
+namespace {
+
+__device__ __forceinline__ int event_of(const long long* __restrict__ off, int nev, long long p)
+{
+    int lo = 0, hi = nev;                  // off[lo] <= p < off[hi]
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (off[mid] <= p) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+__global__ void __launch_bounds__(128) k_pair_cost(const Knot* __restrict__ kn, const Seg* __restrict__ sg,
+                                                   const ModelHdr* __restrict__ mh,
+                                                   const EventDev* __restrict__ evs,
+                                                   const long long* __restrict__ off, int nev,
+                                                   StepCost sc, unsigned long long* __restrict__ keys,
+                                                   unsigned long long* __restrict__ vals)
+{
+    const long long np = off[nev];
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < np;
+         p += (long long)gridDim.x * blockDim.x) {
+        const int e = event_of(off, nev, p);
+        const EventDev& ev = evs[e];
+        const long long local = p - off[e];
+        const int li = (int)(local / ev.nw);
+        const int j = (int)(local - (long long)li * ev.nw) + 1;
+        const int l = ev.lmin + li;
+        Ctx c;
+        c.kn = kn;
+        c.mh = mh;
+        c.sg = sg;
+        c.kb = nullptr;
+        c.ats = (double)ev.ats;
+        for (int q = 0; q < NSYS; q++) c.nst[q] = 0;
+        cd out[NCOEF];
+        if (l == 0) {
+            pair_radial(c, ev, j, out);
+        } else {
+            if (l > 1) pair_toroidal(c, ev, l, j, out + 10);
+            pair_spheroidal(c, ev, l, j, out, out + 5);
+        }
+        double cost = sc.base;
+        unsigned cls = 0;
+        for (int q = 0; q < NSYS; q++) {
+            cost += (double)c.nst[q] * sc.flops[q];
+            if (c.nst[q]) cls |= 1u << q;
+        }
+        unsigned bucket = (unsigned)fmax(0.0, fmin(4095.0, 64.0 * log2(cost)));
+        keys[p] = ((unsigned long long)bucket << 52) | ((unsigned long long)cls << 44) |
+                  ((unsigned long long)p & ((1ull << 44) - 1));
+        vals[p] = ((unsigned long long)e << 48) | ((unsigned long long)li << 24) |
+                  (unsigned long long)(j - 1);
+    }
+}
+
+}  // namespace
+
+size_t pair_sort_tmp_bytes(long long npairs)
+{
+    size_t bytes = 0;
+    cub::DoubleBuffer<unsigned long long> k(nullptr, nullptr), v(nullptr, nullptr);
+    cub::DeviceRadixSort::SortPairsDescending(nullptr, bytes, k, v, (int)npairs);
+    return bytes;
+}
+
+cudaError_t launch_pair_schedule(const Knot* kn, const Seg* sg, const ModelHdr* mh,
+                                 const EventDev* evs, const long long* off, int nev, long long npairs,
+                                 const StepCost& sc, unsigned long long* keys[2],
+                                 unsigned long long* vals[2], void* tmp, size_t tmp_bytes,
+                                 unsigned long long** sorted, cudaStream_t st)
+{
+    if (npairs <= 0) return cudaSuccess;
+    if (npairs >= (1ll << 31)) return cudaErrorInvalidValue;
+    int dev = 0, nsm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    long long blocks = (npairs + 127) / 128;
+    if (blocks > (long long)nsm * 16) blocks = (long long)nsm * 16;
+    k_pair_cost<<<(unsigned)blocks, 128, 0, st>>>(kn, sg, mh, evs, off, nev, sc, keys[0], vals[0]);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    cub::DoubleBuffer<unsigned long long> k(keys[0], keys[1]), v(vals[0], vals[1]);
+    e = cub::DeviceRadixSort::SortPairsDescending(tmp, tmp_bytes, k, v, (int)npairs, 0, 64, st);
+    if (e != cudaSuccess) return e;
+    *sorted = v.Current();
+    return cudaSuccess;
+}
+
+}  // namespace ysg

@@ -12,10 +12,13 @@
 //     the instruction cache: measured slower.)  The plain form keeps all
 //     stage vectors in local memory, which spills through L1 into L2.
 //   * a persistent grid (resident blocks only) pulls work items from an
-//     atomic counter.  An item is (event, l, 32 consecutive frequencies):
-//     the lanes of a warp share l and step through nearly identical radial
-//     grids.  Items are ordered by predicted cost, most expensive first
-//     (longest-processing-time first), so the tail is short.
+//     atomic counter, one item per warp.  Schedule 0: an item is (event, l,
+//     32 consecutive frequencies); the lanes share l and step through
+//     nearly identical radial grids; items are ordered by a cost estimate,
+//     most expensive first (longest-processing-time first), so the tail is
+//     short.  Schedule 1: an item is 32 pairs of equal code path and
+//     near-equal exact cost from the sorted list of k_schedule.cu, so the
+//     lanes of a warp finish together.
 //   * items may come from several events (different frequency grids,
 //     degrees, sources, switches) sharing one model: one launch serves a
 //     whole batch.
@@ -27,16 +30,17 @@ namespace ysg {
 
 constexpr int SLAB = 5 * 14;     // complex entries per thread (five stage slots)
 
-// MINB = resident blocks per SM the registers are budgeted for (the shared
-// memory admits three): 3 keeps the full 255 registers per thread.
-template <int MINB>
-__global__ void __launch_bounds__(64, MINB) k_solve_batched(const Knot* __restrict__ kn,
+// Three 64-thread blocks per SM (the shared memory admits three), each
+// thread with the full 255 registers.
+template <int SCHED>
+__global__ void __launch_bounds__(64, 3) k_solve_batched(const Knot* __restrict__ kn,
                                                       const Seg* __restrict__ sg,
                                                       const ModelHdr* __restrict__ mh,
                                                       const EventDev* __restrict__ evs,
                                                       cd* const* __restrict__ coefs,
-                                                      const int4* __restrict__ items, int nitems,
-                                                      int* counter,
+                                                      const int4* __restrict__ items,
+                                                      const unsigned long long* __restrict__ pairs,
+                                                      long long npairs, int nitems, int* counter,
                                                       unsigned long long* __restrict__ work)
 {
     // the slab is all the shared memory a block has: four blocks fill the SM
@@ -53,11 +57,22 @@ __global__ void __launch_bounds__(64, MINB) k_solve_batched(const Knot* __restri
         if (lane == 0) it = atomicAdd(counter, 1);
         it = __shfl_sync(0xffffffffu, it, 0);
         if (it >= nitems) break;
-        const int4 w = items[it];
-        const EventDev& ev = evs[w.x];
-        const int li = w.y;
-        const int j = w.z + lane + 1;
-        if (j > ev.nw) continue;
+        int e, li, j;
+        if (SCHED == 0) {
+            const int4 w = items[it];
+            e = w.x;
+            li = w.y;
+            j = w.z + lane + 1;
+            if (j > evs[e].nw) continue;
+        } else {
+            const long long p = (long long)it * 32 + lane;
+            if (p >= npairs) continue;
+            const unsigned long long v = pairs[p];
+            e = (int)(v >> 48);
+            li = (int)((v >> 24) & 0xffffffu);
+            j = (int)(v & 0xffffffu) + 1;
+        }
+        const EventDev& ev = evs[e];
         const int l = ev.lmin + li;
         c.ats = (double)ev.ats;
         cd out[NCOEF];
@@ -69,7 +84,7 @@ __global__ void __launch_bounds__(64, MINB) k_solve_batched(const Knot* __restri
                 for (int q = 10; q < 15; q++) out[q] = mk(0.0);
             pair_spheroidal(c, ev, l, j, out, out + 5);
         }
-        cd* dst = coefs[w.x] + (size_t)li * NCOEF * ev.nw + (j - 1);
+        cd* dst = coefs[e] + (size_t)li * NCOEF * ev.nw + (j - 1);
         for (int q = 0; q < NCOEF; q++) dst[(size_t)q * ev.nw] = out[q];
     }
     for (int q = 0; q < NSYS; q++) {
@@ -84,15 +99,14 @@ namespace {
 constexpr int kBlock = 64;
 
 using SolveFn = void (*)(const Knot*, const Seg*, const ModelHdr*, const EventDev*, cd* const*,
-                         const int4*, int, int*, unsigned long long*);
+                         const int4*, const unsigned long long*, long long, int, int*,
+                         unsigned long long*);
 
-SolveFn solve_fn(int) { return k_solve_batched<3>; }
+SolveFn solve_fn(int sched) { return sched == 1 ? k_solve_batched<1> : k_solve_batched<0>; }
 
 size_t solve_smem() { return (size_t)kBlock * SLAB * sizeof(cd); }
 
 }  // namespace
-
-int solve_batched_variants() { return 1; }
 
 int solve_batched_blocks(int variant)
 {
@@ -111,8 +125,8 @@ int solve_batched_blocks(int variant)
 
 cudaError_t launch_solve_batched(int variant, const Knot* kn, const Seg* sg, const ModelHdr* mh,
                                  const EventDev* evs_dev, cd* const* coefs_dev, const int4* items,
-                                 int nitems, int* counter, unsigned long long* work, int nblocks,
-                                 cudaStream_t st)
+                                 const unsigned long long* pairs, long long npairs, int nitems,
+                                 int* counter, unsigned long long* work, int nblocks, cudaStream_t st)
 {
     if (nitems <= 0) return cudaSuccess;
     SolveFn f = solve_fn(variant);
@@ -120,8 +134,8 @@ cudaError_t launch_solve_batched(int variant, const Knot* kn, const Seg* sg, con
     if (e != cudaSuccess) return e;
     e = cudaMemsetAsync(counter, 0, sizeof(int), st);
     if (e != cudaSuccess) return e;
-    f<<<nblocks, kBlock, solve_smem(), st>>>(kn, sg, mh, evs_dev, coefs_dev, items, nitems, counter,
-                                             work);
+    f<<<nblocks, kBlock, solve_smem(), st>>>(kn, sg, mh, evs_dev, coefs_dev, items, pairs, npairs,
+                                             nitems, counter, work);
     return cudaGetLastError();
 }
 

@@ -16,14 +16,31 @@ cudaError_t launch_solve_plain(const Knot* kn, const Seg* sg, const ModelHdr& mh
 // K1 batched persistent: work items (event, l index, first frequency - 1)
 // of one or more events, one thread per (omega,l) pair, stage vectors in
 // shared memory.  counter must be device memory (reset by the launcher).
-// `variant` selects the register budget (0: four 64-thread blocks per SM,
-// 1: five); solve_batched_blocks gives the resident grid of a variant.
-int solve_batched_variants();
-int solve_batched_blocks(int variant);
-cudaError_t launch_solve_batched(int variant, const Knot* kn, const Seg* sg, const ModelHdr* mh,
+// Schedules (k_solve_batched.cu): 0 = tiles of (event, l, 32 consecutive
+// frequencies) from `items`; 1 = lists of 32 pairs from `pairs` (packed
+// event << 48 | l index << 24 | j - 1, sorted by launch_pair_schedule).
+// solve_batched_blocks gives the resident grid of a schedule.
+constexpr int NSCHED = 2;
+int solve_batched_blocks(int sched);
+cudaError_t launch_solve_batched(int sched, const Knot* kn, const Seg* sg, const ModelHdr* mh,
                                  const EventDev* evs_dev, cd* const* coefs_dev, const int4* items,
-                                 int nitems, int* counter, unsigned long long* work, int nblocks,
-                                 cudaStream_t st);
+                                 const unsigned long long* pairs, long long npairs, int nitems,
+                                 int* counter, unsigned long long* work, int nblocks, cudaStream_t st);
+
+// Pair cost model and ordering for schedule 1 (k_schedule.cu).  off[e] is
+// the flat index of event e's first pair (off[nev] = npairs); keys and vals
+// are two pairs of npairs-element buffers; *sorted receives the buffer
+// holding the packed pairs in schedule order.
+struct StepCost {
+    double flops[NSYS_COUNT];    // FP64 work per Cash-Karp step, per system class
+    double base;                 // per-pair work outside the stepping
+};
+size_t pair_sort_tmp_bytes(long long npairs);
+cudaError_t launch_pair_schedule(const Knot* kn, const Seg* sg, const ModelHdr* mh,
+                                 const EventDev* evs, const long long* off, int nev, long long npairs,
+                                 const StepCost& sc, unsigned long long* keys[2],
+                                 unsigned long long* vals[2], void* tmp, size_t tmp_bytes,
+                                 unsigned long long** sorted, cudaStream_t st);
 
 // K2: Legendre table, T[((l * nr) + k) * 8 + q].
 cudaError_t launch_legendre(int nr, int lmax, const double* delta, const double* ct,

@@ -15,16 +15,24 @@
 #pragma once
 #include "ysg_model.cuh"
 
-// Two builds of the solver code exist: the plain form keeps the Cash-Karp
+// Three builds of the solver code exist: the plain form keeps the Cash-Karp
 // stage vectors in per-thread arrays (the compiler places them in local
 // memory); with YSG_SMEM_STAGES the stage vectors live in a per-thread slab
-// of shared memory and only y and the stage input stay in registers.  Each
-// form gets its own inline namespace so the two translation units never
+// of shared memory and only y and the stage input stay in registers; with
+// YSG_COUNT_ONLY yint only counts the steps it would take (the cost model of
+// the pair scheduler: every integer decision of a solve -- start levels,
+// layers, step counts -- is made as in a real solve, no state is stepped).
+// Each form gets its own inline namespace so the translation units never
 // share a definition.
 #ifndef YSG_SMEM_STAGES
 #define YSG_SMEM_STAGES 0
 #endif
-#if YSG_SMEM_STAGES
+#ifndef YSG_COUNT_ONLY
+#define YSG_COUNT_ONLY 0
+#endif
+#if YSG_COUNT_ONLY
+#define YSG_VARIANT v_count
+#elif YSG_SMEM_STAGES
 #define YSG_VARIANT v_smem
 #else
 #define YSG_VARIANT v_local
@@ -609,6 +617,7 @@ __device__ YSG_YINT_ATTR void yint(Ctx& c, int i1, int i2, double r1, double r2,
         int n = 2 + (int)fmin(nf, 4194304.0);
         drr = (rr2 - rr1) / (double)(n - 1);
         c.nst[Sys::CLS] += (unsigned)(n - 1);
+        if (YSG_COUNT_ONLY) continue;
         for (int j = 1; j <= n - 1; j++) {
             double rr = __dadd_rn(rr1, __dmul_rn((double)(j - 1), drr));
 #if YSG_SMEM_STAGES

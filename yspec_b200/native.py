@@ -74,8 +74,8 @@ class YshNorms(C.Structure):
 EXPORTS = [
     "ysg_create", "ysg_model_upload", "ysg_event_spectra", "ysg_event_traces", "ysg_trace_rows",
     "ysg_event_run", "ysg_event_prepare", "ysg_event_execute", "ysg_event_fetch", "ysg_get_stream",
-    "ysg_batch_run", "ysg_event_coef", "ysg_legendre_table", "ysg_set_solver", "ysg_set_schedule",
-    "ysg_last_timings", "ysg_last_work", "ysg_last_bytes", "ysg_fp64_peak", "ysg_status_string",
+    "ysg_batch_run", "ysg_event_coef", "ysg_legendre_table", "ysg_set_solver", "ysg_set_schedule", "ysg_last_schedule",
+    "ysg_last_timings", "ysg_last_work", "ysg_last_bytes", "ysg_last_launches", "ysg_fp64_peak", "ysg_status_string",
     "ysg_last_cuda_error", "ysg_destroy", "ysg_traces_noalloc",
     "ysh_norms_get", "ysh_read_params", "ysh_free_params", "ysh_read_model", "ysh_model_view",
     "ysh_model_nknot", "ysh_model_array", "ysh_free_model", "ysh_event_setup", "ysh_free_event",
@@ -119,9 +119,11 @@ def lib() -> C.CDLL:
     L.ysg_legendre_table.argtypes = [vp, C.c_int, C.c_int, _dp, _dp, _dp, _dp]
     L.ysg_set_solver.argtypes = [vp, C.c_int]
     L.ysg_set_schedule.argtypes = [vp, C.c_int]
+    L.ysg_last_schedule.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_float)]
     L.ysg_last_timings.argtypes = [vp, C.POINTER(C.c_float)]
     L.ysg_last_work.argtypes = [vp, _dp, _dp]
     L.ysg_last_bytes.argtypes = [vp, _dp, _dp]
+    L.ysg_last_launches.argtypes = [vp, C.POINTER(C.c_longlong)]
     L.ysg_fp64_peak.argtypes = [C.c_int, _dp]
     L.ysg_status_string.argtypes = [C.c_int]
     L.ysg_status_string.restype = C.c_char_p

@@ -36,7 +36,8 @@ def main(argv=None) -> None:
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--event", type=int, default=0, help="event index within the configuration")
-    ap.add_argument("--schedule", type=int, default=0, help="batched-solver schedule variant")
+    ap.add_argument("--schedule", type=int, default=-1,
+                    help="batched-solver schedule: 0 tiles, 1 pair lists, -1 autotuned")
     ap.add_argument("--batch", action="store_true", help="run every event of the configuration as one batch")
     ap.add_argument("--set", action="append", default=[], metavar="KEY=VALUE",
                     help="override a parameter of the configuration")
@@ -59,7 +60,8 @@ def main(argv=None) -> None:
             wall = time.perf_counter() - t
             ms = eng.timings()
             pairs, fl = eng.work()
-            print(f"{a.config} {a.solver} rep{rep}: wall {wall:.3f} s  stages (ms) "
+            sched = eng.last_schedule()[0] if a.solver == "batched" else "-"
+            print(f"{a.config} {a.solver} sched {sched} rep{rep}: wall {wall:.3f} s  stages (ms) "
                   f"legendre {ms[0]:.3f} solve {ms[1]:.3f} lsum {ms[2]:.3f} ifft {ms[3]:.3f}  "
                   f"pairs {pairs:.0f}  solves/s {pairs / (ms[1] / 1e3):.4g}  "
                   f"solve FP64 {fl / (ms[1] / 1e3) / 1e12:.3f} TFLOP/s", flush=True)
