@@ -263,7 +263,7 @@ int upload_items(ysg_handle* h, std::vector<Item>& items, const std::vector<Even
     const long long np = off.back();
     CK(h->offs.ensure(off.size() * sizeof(long long)));
     CK(cudaMemcpyAsync(h->offs.p, off.data(), off.size() * sizeof(long long), cudaMemcpyHostToDevice, h->st));
-    const size_t pb = (size_t)std::max<long long>(np, 1) * sizeof(unsigned long long);
+    const size_t pb = (size_t)std::max<long long>(2 * np, 1) * sizeof(unsigned long long);
     CK(h->keys0.ensure(pb));
     CK(h->keys1.ensure(pb));
     CK(h->vals0.ensure(pb));
@@ -431,7 +431,7 @@ int enqueue_solve(ysg_handle* h, int nev)
                                     h->npairs, sc, keys, vals, h->sort_tmp.p, h->sort_tmp.cap, &sorted,
                                     h->st));
             pairs = sorted;
-            nitems = (int)((h->npairs + 31) / 32);
+            nitems = (int)((2 * h->npairs + 31) / 32);
         }
         h->launches += 1;
         CK(launch_solve_batched(s, h->kn.as<Knot>(), h->sg.as<Seg>(), h->hdr_dev.as<ModelHdr>(),

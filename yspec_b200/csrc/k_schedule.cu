@@ -7,12 +7,17 @@
 // count-only build of the solver code, where yint makes every integer
 // decision a real solve makes (start level, layers, steps per layer,
 // module_int.f90:1847-1968) but steps no state, so the counts are exact.
-// The cost is the counted FP64 work, sum over systems of steps x flops per
-// step; the path class is the set of systems a pair integrates.  Pairs are
-// then sorted (CUB radix sort, descending) by
-//   key = log-cost bucket (1.1% wide) | path class | flat pair index,
+// A pair with l >= 2 gives two list entries, its spheroidal part (with the
+// radial mode for l = 0) and its toroidal part (yspec.f90:301-316), which
+// are independent solves writing disjoint coefficients; so a warp runs one
+// kind of system.  The cost of an entry is its counted FP64 work, sum over
+// systems of steps x flops per step; the path class is the set of systems
+// it integrates.  Entries are then sorted (CUB radix sort, descending) by
+//   key = log-cost bucket (1.1% wide) | path class | entry index,
 // so a warp's 32 lanes take the same yint sequence with nearly the same
 // number of steps, and the persistent kernel takes the costliest first.
+// Entry value: event << 48 | part << 47 | l index << 24 | j - 1 (part 1 =
+// toroidal).
 #define YSG_COUNT_ONLY 1
 #include "ysg_kernels.h"
 #include "ysg_solvers.cuh"
@@ -42,8 +47,10 @@ __global__ void __launch_bounds__(128) k_pair_cost(const Knot* __restrict__ kn, 
                                                    unsigned long long* __restrict__ vals)
 {
     const long long np = off[nev];
-    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < np;
-         p += (long long)gridDim.x * blockDim.x) {
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < 2 * np;
+         q += (long long)gridDim.x * blockDim.x) {
+        const long long p = q >> 1;
+        const int part = (int)(q & 1);
         const int e = event_of(off, nev, p);
         const EventDev& ev = evs[e];
         const long long local = p - off[e];
@@ -53,28 +60,33 @@ __global__ void __launch_bounds__(128) k_pair_cost(const Knot* __restrict__ kn, 
         Ctx c;
         c.kn = kn;
         c.mh = mh;
+        c.pib = mh->pibigg;
         c.sg = sg;
         c.kb = nullptr;
         c.ats = (double)ev.ats;
         for (int q = 0; q < NSYS; q++) c.nst[q] = 0;
         cd out[NCOEF];
-        if (l == 0) {
+        if (part == 1) {
+            if (l > 1) pair_toroidal(c, ev, l, j, out + 10);
+        } else if (l == 0) {
             pair_radial(c, ev, j, out);
         } else {
-            if (l > 1) pair_toroidal(c, ev, l, j, out + 10);
             pair_spheroidal(c, ev, l, j, out, out + 5);
         }
         double cost = sc.base;
         unsigned cls = 0;
-        for (int q = 0; q < NSYS; q++) {
-            cost += (double)c.nst[q] * sc.flops[q];
-            if (c.nst[q]) cls |= 1u << q;
+        for (int s = 0; s < NSYS; s++) {
+            cost += (double)c.nst[s] * sc.flops[s];
+            if (c.nst[s]) cls |= 1u << s;
         }
-        unsigned bucket = (unsigned)fmax(0.0, fmin(4095.0, 64.0 * log2(cost)));
-        keys[p] = ((unsigned long long)bucket << 52) | ((unsigned long long)cls << 44) |
-                  ((unsigned long long)p & ((1ull << 44) - 1));
-        vals[p] = ((unsigned long long)e << 48) | ((unsigned long long)li << 24) |
-                  (unsigned long long)(j - 1);
+        // an l < 2 pair has no toroidal part: its entry sorts last and is skipped
+        const bool none = part == 1 && l < 2;
+        unsigned bucket = none ? 0u : (unsigned)fmax(1.0, fmin(4095.0, 64.0 * log2(cost)));
+        keys[q] = ((unsigned long long)bucket << 52) | ((unsigned long long)cls << 44) |
+                  ((unsigned long long)q & ((1ull << 44) - 1));
+        vals[q] = none ? ~0ull
+                       : ((unsigned long long)e << 48) | ((unsigned long long)part << 47) |
+                             ((unsigned long long)li << 24) | (unsigned long long)(j - 1);
     }
 }
 
@@ -84,7 +96,7 @@ size_t pair_sort_tmp_bytes(long long npairs)
 {
     size_t bytes = 0;
     cub::DoubleBuffer<unsigned long long> k(nullptr, nullptr), v(nullptr, nullptr);
-    cub::DeviceRadixSort::SortPairsDescending(nullptr, bytes, k, v, (int)npairs);
+    cub::DeviceRadixSort::SortPairsDescending(nullptr, bytes, k, v, (int)(2 * npairs));
     return bytes;
 }
 
@@ -95,17 +107,17 @@ cudaError_t launch_pair_schedule(const Knot* kn, const Seg* sg, const ModelHdr* 
                                  unsigned long long** sorted, cudaStream_t st)
 {
     if (npairs <= 0) return cudaSuccess;
-    if (npairs >= (1ll << 31)) return cudaErrorInvalidValue;
+    if (2 * npairs >= (1ll << 31)) return cudaErrorInvalidValue;
     int dev = 0, nsm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    long long blocks = (npairs + 127) / 128;
+    long long blocks = (2 * npairs + 127) / 128;
     if (blocks > (long long)nsm * 16) blocks = (long long)nsm * 16;
     k_pair_cost<<<(unsigned)blocks, 128, 0, st>>>(kn, sg, mh, evs, off, nev, sc, keys[0], vals[0]);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     cub::DoubleBuffer<unsigned long long> k(keys[0], keys[1]), v(vals[0], vals[1]);
-    e = cub::DeviceRadixSort::SortPairsDescending(tmp, tmp_bytes, k, v, (int)npairs, 0, 64, st);
+    e = cub::DeviceRadixSort::SortPairsDescending(tmp, tmp_bytes, k, v, (int)(2 * npairs), 0, 64, st);
     if (e != cudaSuccess) return e;
     *sorted = v.Current();
     return cudaSuccess;

@@ -49,6 +49,7 @@ __global__ void __launch_bounds__(64, 3) k_solve_batched(const Knot* __restrict_
     Ctx c;
     c.kn = kn;
     c.mh = mh;
+    c.pib = mh->pibigg;
     c.sg = sg;
     c.kb = slab + (threadIdx.x >> 5) * (SLAB * KS) + lane;
     for (int q = 0; q < NSYS; q++) c.nst[q] = 0;
@@ -57,7 +58,7 @@ __global__ void __launch_bounds__(64, 3) k_solve_batched(const Knot* __restrict_
         if (lane == 0) it = atomicAdd(counter, 1);
         it = __shfl_sync(0xffffffffu, it, 0);
         if (it >= nitems) break;
-        int e, li, j;
+        int e, li, j, part = 2;             // part: 0 spheroidal, 1 toroidal, 2 both
         if (SCHED == 0) {
             const int4 w = items[it];
             e = w.x;
@@ -66,26 +67,33 @@ __global__ void __launch_bounds__(64, 3) k_solve_batched(const Knot* __restrict_
             if (j > evs[e].nw) continue;
         } else {
             const long long p = (long long)it * 32 + lane;
-            if (p >= npairs) continue;
+            if (p >= 2 * npairs) continue;
             const unsigned long long v = pairs[p];
+            if (v == ~0ull) continue;           // l < 2 has no toroidal entry
             e = (int)(v >> 48);
-            li = (int)((v >> 24) & 0xffffffu);
+            part = (int)((v >> 47) & 1u);
+            li = (int)((v >> 24) & 0x7fffffu);
             j = (int)(v & 0xffffffu) + 1;
         }
         const EventDev& ev = evs[e];
         const int l = ev.lmin + li;
         c.ats = (double)ev.ats;
         cd out[NCOEF];
-        if (l == 0) {
+        int q0 = 0, q1 = NCOEF;             // coefficients this entry writes
+        if (part == 1) {
+            pair_toroidal(c, ev, l, j, out + 10);
+            q0 = 10;
+        } else if (l == 0) {
             pair_radial(c, ev, j, out);
         } else {
-            if (l > 1) pair_toroidal(c, ev, l, j, out + 10);
+            if (part == 2 && l > 1) pair_toroidal(c, ev, l, j, out + 10);
             else
                 for (int q = 10; q < 15; q++) out[q] = mk(0.0);
             pair_spheroidal(c, ev, l, j, out, out + 5);
+            if (part == 0 && l > 1) q1 = 10;
         }
         cd* dst = coefs[e] + (size_t)li * NCOEF * ev.nw + (j - 1);
-        for (int q = 0; q < NCOEF; q++) dst[(size_t)q * ev.nw] = out[q];
+        for (int q = q0; q < q1; q++) dst[(size_t)q * ev.nw] = out[q];
     }
     for (int q = 0; q < NSYS; q++) {
         unsigned long long v = c.nst[q];

@@ -28,6 +28,7 @@ __global__ void __launch_bounds__(128) k_solve_plain(const Knot* __restrict__ kn
     Ctx c;
     c.kn = kn;
     c.mh = mhs;
+    c.pib = mh.pibigg;
     c.ats = (double)ev.ats;
     c.sg = sg;
     c.kb = nullptr;

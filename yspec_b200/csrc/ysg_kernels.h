@@ -17,8 +17,9 @@ cudaError_t launch_solve_plain(const Knot* kn, const Seg* sg, const ModelHdr& mh
 // of one or more events, one thread per (omega,l) pair, stage vectors in
 // shared memory.  counter must be device memory (reset by the launcher).
 // Schedules (k_solve_batched.cu): 0 = tiles of (event, l, 32 consecutive
-// frequencies) from `items`; 1 = lists of 32 pairs from `pairs` (packed
-// event << 48 | l index << 24 | j - 1, sorted by launch_pair_schedule).
+// frequencies) from `items`; 1 = lists of 32 entries from `pairs` (2 npairs
+// entries, the spheroidal and toroidal part of each pair, packed event << 48
+// | part << 47 | l index << 24 | j - 1, sorted by launch_pair_schedule).
 // solve_batched_blocks gives the resident grid of a schedule.
 constexpr int NSCHED = 2;
 int solve_batched_blocks(int sched);

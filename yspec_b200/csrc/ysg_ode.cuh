@@ -63,6 +63,7 @@ struct Ctx {
     const Seg* sg;   // power-form spline segments (right-hand sides)
     cd* kb;          // shared-memory stage slab of this thread (smem form)
     double zeta, zeta2, zeta2m2, szeta2m2, nu, dr, ats;
+    double pib;      // pi * bigg of the model (module_model.f90:490), = mh->pibigg
     cd omega, omega2, omegai, omegai2, lno;
 };
 
@@ -208,7 +209,7 @@ __device__ __forceinline__ SolidCoef solid_amat(const Ctx& c, double rr)
         a.s12 = (c.zeta * (rgr - 2.0 * gamma)) * ri2;
     }
     if (KIND == 2) {
-        double pib = c.mh->pibigg;
+        double pib = c.pib;
         a.t31 = -(4.0 * pib * rrho);
         a.t33 = -((double)c.ll * ri);
         a.k33 = 4.0 * pib;
@@ -251,7 +252,7 @@ __device__ __forceinline__ FluidCoef fluid_amat(const Ctx& c, double rr)
     a.t11 = (gzw * ri - 1.0) * ri;
     a.s11 = -(c.omega2 * rrho) + (rrho * gg) * ((gzw * ri - 4.0) * ri);
     if (KIND == 2) {
-        double pib = c.mh->pibigg;
+        double pib = c.pib;
         a.t12 = (c.zeta2 * c.omegai2) * (ri * ri);
         a.t21 = -4.0 * pib * rrho;
         a.t22 = -((double)c.ll * ri);
@@ -587,14 +588,18 @@ __device__ __forceinline__ void rescale(cd* y, int* scale)
 #endif
 
 template <class Sys>
-__device__ YSG_YINT_ATTR void yint(Ctx& c, int i1, int i2, double r1, double r2, cd* yio, int* scale)
+__device__ YSG_YINT_ATTR void yint(Ctx& cio, int i1, int i2, double r1, double r2, cd* yio, int* scale)
 {
     if (r2 == r1) return;
 #if YSG_SMEM_STAGES
+    // a private copy of the context: the caller's lives in memory (its
+    // address is passed in), the copy's fields can stay in registers
+    Ctx c = cio;
     cd y[Sys::N];
 #pragma unroll
     for (int k = 0; k < Sys::N; k++) y[k] = yio[k];
 #else
+    Ctx& c = cio;
     cd* y = yio;
 #endif
     const bool up = r2 > r1;
@@ -631,6 +636,8 @@ __device__ YSG_YINT_ATTR void yint(Ctx& c, int i1, int i2, double r1, double r2,
 #if YSG_SMEM_STAGES
 #pragma unroll
     for (int k = 0; k < Sys::N; k++) yio[k] = y[k];
+    cio.il = c.il;
+    cio.nst[Sys::CLS] = c.nst[Sys::CLS];
 #endif
 }
 
