@@ -101,6 +101,13 @@ int ysg_model_upload(ysg_handle *h, const ysg_model *m);
  * for ysg_event_traces. */
 int ysg_event_spectra(ysg_handle *h, const ysg_event *ev, double *ur, double *ut, double *up);
 
+/* ysg_event_spectra into device buffers the caller owns (complex (nw, nr)
+ * column-major each, on the handle's device), for callers that pass the
+ * spectra on without a host round trip (the multi-GPU receiver exchange).
+ * Returns when the copies are done. */
+int ysg_event_spectra_device(ysg_handle *h, const ysg_event *ev, void *d_ur, void *d_ut,
+                             void *d_up);
+
 /* Time series of the last spectra: module_fourier.f90:55-145 and
  * yspec.f90:432-486.  out is (nout, 4, nr) column-major: time in seconds,
  * then Re of the Z, N, E components in SI units, exactly the four columns

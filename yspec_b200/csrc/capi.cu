@@ -968,6 +968,26 @@ int ysg_event_spectra(ysg_handle* h, const ysg_event* ev, double* ur, double* ut
     return finish(h, 1, true, false);
 }
 
+int ysg_event_spectra_device(ysg_handle* h, const ysg_event* ev, void* d_ur, void* d_ut, void* d_up)
+{
+    int rc = check_event(h, ev);
+    if (rc) return rc;
+    cudaSetDevice(h->device);
+    h->has_spectra = false;
+    rc = prepare_single(h, ev);
+    if (rc) return rc;
+    rc = enqueue_spectra(h, 1);
+    if (rc) return rc;
+    const int nr = ev->nr, nw = ev->nw;
+    const size_t nspec = (size_t)nw * std::max(nr, 1);
+    const cd* d_spec = slot0(h).spec.as<cd>();
+    const size_t nb = (size_t)nw * nr * sizeof(cd);
+    if (d_ur && nr > 0) CK(cudaMemcpyAsync(d_ur, d_spec, nb, cudaMemcpyDeviceToDevice, h->st));
+    if (d_ut && nr > 0) CK(cudaMemcpyAsync(d_ut, d_spec + nspec, nb, cudaMemcpyDeviceToDevice, h->st));
+    if (d_up && nr > 0) CK(cudaMemcpyAsync(d_up, d_spec + 2 * nspec, nb, cudaMemcpyDeviceToDevice, h->st));
+    return finish(h, 1, true, false);
+}
+
 int ysg_event_traces(ysg_handle* h, const ysg_time* tm, double* out, int* nout)
 {
     if (!h || !tm) return YSG_ERR_ARG;
