@@ -81,6 +81,9 @@ void ysh_free_model(ysh_model *m);
  * Allocates e->delta/azst/azep (free with ysh_free_event). */
 int ysh_event_setup(const ysh_model *m, const ysh_params *p, ysh_event *e);
 void ysh_free_event(ysh_event *e);
+/* The per-receiver files of yspec.f90:488-503 (pref_out.1 .. pref_out.nr,
+ * nout lines of four E15.6 fields), byte-identical to the reference; the
+ * receivers' files are formatted and written on several threads. */
 int ysh_write_traces(const char *pref_out, const double *out, int nout, int nr);
 /* The whole program: parameter file -> traces on `device`.  When out is
  * non-NULL it receives a malloc'd (nout, 4, nr) array (free with
@@ -88,6 +91,13 @@ int ysh_write_traces(const char *pref_out, const double *out, int nout, int nr);
  * as the reference writes them. */
 int ysh_run(const char *param_file, int device, int write_files, double **out, int *nout,
             int *nr);
+/* Several parameter files in one go: the events that name the same model
+ * deck run as one ysg_batch_run (one batched solve launch, one CUDA graph),
+ * and each event's files are written under its own output prefix exactly as
+ * a single run writes them.  On an error *failed (if non-NULL) is the index
+ * of the parameter file concerned. */
+int ysh_run_batch(int nfiles, const char *const *param_files, int device, int write_files,
+                  int *failed);
 void ysh_free(void *ptr);
 const char *ysh_status_string(int status);
 

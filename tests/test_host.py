@@ -125,9 +125,11 @@ def test_missing_files(workdir):
     assert ei.value.status == 103
 
 
-def test_writer_byte_identical_to_oracle(workdir):
+@pytest.mark.parametrize("nout,nr", [(7, 12), (3, 1037)])
+def test_writer_byte_identical_to_oracle(workdir, nout, nr):
+    """The threaded writer (receivers' files on several threads) against the
+    oracle's serial writer, byte for byte, including 4-digit file suffixes."""
     rng = np.random.default_rng(0)
-    nout, nr = 7, 12
     out = rng.normal(size=(nr, 4, nout)) * 10.0 ** rng.integers(-120, 120, size=(nr, 4, nout))
     out[0, 1, 0] = -0.0
     out[0, 2, 1] = 0.0

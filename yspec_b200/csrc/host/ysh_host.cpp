@@ -19,7 +19,10 @@
 #include <cstring>
 #include <fstream>
 #include <memory>
+#include <atomic>
+#include <map>
 #include <string>
+#include <thread>
 #include <vector>
 
 namespace {
@@ -569,31 +572,52 @@ void ysh_free_event(ysh_event* e)
     e->delta = e->azst = e->azep = nullptr;
 }
 
+// One receiver's file (yspec.f90:488-503): nout lines of four E15.6 fields.
+static bool write_one(const char* pref_out, const double* out, int nout, int k)
+{
+    // string_cat_int: digits counted with a single-precision log10
+    char num[16];
+    std::snprintf(num, sizeof num, "%10d", k);
+    int j = (int)std::floor(std::log10((float)k));
+    std::string path = std::string(pref_out) + "." + std::string(num + 9 - j);
+    std::string text;
+    text.reserve((size_t)nout * 61);
+    char f[16];
+    const double* base = out + (size_t)nout * 4 * (size_t)(k - 1);
+    for (int i = 0; i < nout; i++) {
+        for (int c = 0; c < 4; c++) {
+            e15_6(base[(size_t)i + (size_t)nout * c], f);
+            text.append(f, 15);
+        }
+        text += '\n';
+    }
+    std::FILE* fp = std::fopen(path.c_str(), "w");
+    if (!fp) return false;
+    const bool ok = std::fwrite(text.data(), 1, text.size(), fp) == text.size();
+    return std::fclose(fp) == 0 && ok;
+}
+
 int ysh_write_traces(const char* pref_out, const double* out, int nout, int nr)
 {
-    std::string line;
-    char f[16];
-    for (int k = 1; k <= nr; k++) {
-        // string_cat_int: digits counted with a single-precision log10
-        char num[16];
-        std::snprintf(num, sizeof num, "%10d", k);
-        int j = (int)std::floor(std::log10((float)k));
-        std::string path = std::string(pref_out) + "." + std::string(num + 9 - j);
-        std::FILE* fp = std::fopen(path.c_str(), "w");
-        if (!fp) return YSH_ERR_IO;
-        const double* base = out + (size_t)nout * 4 * (size_t)(k - 1);
-        for (int i = 0; i < nout; i++) {
-            line.clear();
-            for (int c = 0; c < 4; c++) {
-                e15_6(base[(size_t)i + (size_t)nout * c], f);
-                line += f;
-            }
-            line += '\n';
-            std::fputs(line.c_str(), fp);
-        }
-        std::fclose(fp);
+    // Receivers are independent files: format and write them on several
+    // threads (the text conversion dominates at thousands of receivers).
+    unsigned hw = std::thread::hardware_concurrency();
+    int nth = (int)std::min<unsigned>(hw ? hw : 1, 32u);
+    nth = std::max(1, std::min(nth, nr / 4));
+    std::atomic<int> next{1};
+    std::atomic<bool> ok{true};
+    auto work = [&]() {
+        for (int k = next++; k <= nr; k = next++)
+            if (!write_one(pref_out, out, nout, k)) ok = false;
+    };
+    if (nth == 1) {
+        work();
+    } else {
+        std::vector<std::thread> pool;
+        for (int t = 0; t < nth; t++) pool.emplace_back(work);
+        for (auto& t : pool) t.join();
     }
-    return YSH_OK;
+    return ok ? YSH_OK : YSH_ERR_IO;
 }
 
 int ysh_run(const char* param_file, int device, int write_files, double** out, int* nout, int* nr)
@@ -636,6 +660,75 @@ int ysh_run(const char* param_file, int device, int write_files, double** out, i
     ysh_free_event(&e);
     ysh_free_model(m);
     ysh_free_params(&p);
+    return rc;
+}
+
+int ysh_run_batch(int nfiles, const char* const* param_files, int device, int write_files,
+                  int* failed)
+{
+    if (failed) *failed = -1;
+    if (nfiles < 1 || !param_files) return YSG_ERR_ARG;
+    // read every parameter file first (the reference stops at the first bad one)
+    std::vector<ysh_params> ps((size_t)nfiles);
+    int rc = 0, nread = 0;
+    for (; nread < nfiles; nread++) {
+        rc = ysh_read_params(param_files[nread], &ps[(size_t)nread]);
+        if (rc) {
+            if (failed) *failed = nread;
+            break;
+        }
+    }
+    // events sharing a model deck run as one batch on the device
+    std::map<std::string, std::vector<int>> groups;
+    for (int i = 0; i < nread && !rc; i++) groups[ps[(size_t)i].model_file].push_back(i);
+    ysg_handle* h = nullptr;
+    if (!rc) rc = ysg_create(&h, device);
+    for (auto it = groups.begin(); it != groups.end() && !rc; ++it) {
+        const std::vector<int>& ids = it->second;
+        ysh_model* m = nullptr;
+        rc = ysh_read_model(it->first.c_str(), &m);
+        if (rc) {
+            if (failed) *failed = ids[0];
+            break;
+        }
+        std::vector<ysh_event> es(ids.size());
+        size_t nset = 0;
+        for (; nset < ids.size(); nset++) {
+            rc = ysh_event_setup(m, &ps[(size_t)ids[nset]], &es[nset]);
+            if (rc) {
+                if (failed) *failed = ids[nset];
+                break;
+            }
+        }
+        std::vector<ysg_event> evs;
+        std::vector<ysg_time> tms;
+        std::vector<std::vector<double>> bufs(ids.size());
+        std::vector<double*> outs;
+        std::vector<int> nouts(ids.size(), 0);
+        if (!rc) {
+            ysg_model view;
+            ysh_model_view(m, &view);
+            rc = ysg_model_upload(h, &view);
+        }
+        if (!rc) {
+            for (size_t e = 0; e < ids.size(); e++) {
+                evs.push_back(es[e].ev);
+                tms.push_back(es[e].tm);
+                bufs[e].resize((size_t)ysg_trace_rows(&es[e].tm) * 4 * (size_t)std::max(es[e].ev.nr, 1));
+                outs.push_back(bufs[e].data());
+            }
+            rc = ysg_batch_run(h, (int)ids.size(), evs.data(), tms.data(), outs.data(), nouts.data());
+        }
+        for (size_t e = 0; e < ids.size() && !rc && write_files; e++) {
+            const ysh_params& p = ps[(size_t)ids[e]];
+            rc = ysh_write_traces(p.pref_out, bufs[e].data(), nouts[e], p.nr);
+            if (rc && failed) *failed = ids[e];
+        }
+        for (size_t e = 0; e < nset; e++) ysh_free_event(&es[e]);
+        ysh_free_model(m);
+    }
+    if (h) ysg_destroy(h);
+    for (int i = 0; i < nread; i++) ysh_free_params(&ps[(size_t)i]);
     return rc;
 }
 

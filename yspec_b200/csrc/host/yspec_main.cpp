@@ -1,6 +1,8 @@
 // yspec_main.cpp -- the `yspec input.in` command (yspec.f90:1-511) on the
 // B200 engine: same argument, parameter file, model deck and per-receiver
 // ASCII output files as the reference.  Set YSPEC_DEVICE to pick the GPU.
+// `yspec a.in b.in ...` runs several events; those sharing a model deck
+// are solved as one batch (each still writes its own files).
 #include <cstdio>
 #include <cstdlib>
 
@@ -9,12 +11,23 @@
 int main(int argc, char** argv)
 {
     if (argc < 2) {
-        std::fprintf(stderr, "usage: yspec input.in\n");
+        std::fprintf(stderr, "usage: yspec input.in [more.in ...]\n");
         return 2;
     }
     const char* dev = std::getenv("YSPEC_DEVICE");
-    int rc = ysh_run(argv[1], dev ? std::atoi(dev) : 0, 1, nullptr, nullptr, nullptr);
+    const int device = dev ? std::atoi(dev) : 0;
+    if (argc == 2) {
+        int rc = ysh_run(argv[1], device, 1, nullptr, nullptr, nullptr);
+        if (rc) {
+            std::fprintf(stderr, "%s\n", ysh_status_string(rc));
+            return 1;
+        }
+        return 0;
+    }
+    int failed = -1;
+    int rc = ysh_run_batch(argc - 1, argv + 1, device, 1, &failed);
     if (rc) {
+        if (failed >= 0) std::fprintf(stderr, "%s: ", argv[1 + failed]);
         std::fprintf(stderr, "%s\n", ysh_status_string(rc));
         return 1;
     }
