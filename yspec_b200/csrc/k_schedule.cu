@@ -13,9 +13,11 @@
 // kind of system.  The cost of an entry is its counted FP64 work, sum over
 // systems of steps x flops per step; the path class is the set of systems
 // it integrates.  Entries are then sorted (CUB radix sort, descending) by
-//   key = log-cost bucket (1.1% wide) | path class | entry index,
+//   key = spheroidal first | log-cost bucket (1.1% wide) | path class | entry index,
 // so a warp's 32 lanes take the same yint sequence with nearly the same
-// number of steps, and the persistent kernel takes the costliest first.
+// number of steps, the persistent kernel takes the costliest first, and
+// the spheroidal and toroidal stepping code do not compete for an SM's
+// instruction cache except where the two parts meet.
 // Entry value: event << 48 | part << 47 | l index << 24 | j - 1 (part 1 =
 // toroidal).
 #define YSG_COUNT_ONLY 1
@@ -82,8 +84,8 @@ __global__ void __launch_bounds__(128) k_pair_cost(const Knot* __restrict__ kn, 
         // an l < 2 pair has no toroidal part: its entry sorts last and is skipped
         const bool none = part == 1 && l < 2;
         unsigned bucket = none ? 0u : (unsigned)fmax(1.0, fmin(4095.0, 64.0 * log2(cost)));
-        keys[q] = ((unsigned long long)bucket << 52) | ((unsigned long long)cls << 44) |
-                  ((unsigned long long)q & ((1ull << 44) - 1));
+        keys[q] = ((unsigned long long)(part == 0) << 63) | ((unsigned long long)bucket << 51) |
+                  ((unsigned long long)cls << 43) | ((unsigned long long)q & ((1ull << 43) - 1));
         vals[q] = none ? ~0ull
                        : ((unsigned long long)e << 48) | ((unsigned long long)part << 47) |
                              ((unsigned long long)li << 24) | (unsigned long long)(j - 1);
