@@ -124,3 +124,32 @@ def test_explosion_has_no_transverse_motion(engine, workdir):
     tr = engine.run(Event(model, Params(pf)))
     z = tr[:, 1]
     assert rel_l2(z[1], z[0]) < 1e-10
+
+
+@pytest.mark.parametrize("nrec", [45, 8])
+def test_spectra_many_receivers_match_oracle(engine, workdir, nrec):
+    """Receiver counts of 8 and more take the tensor-core l-sum (DMMA tiles of
+    16 frequencies x 32 receivers): 45 receivers span a full and a partial
+    receiver tile, and the band is not a multiple of the frequency tile."""
+    import numpy as _np
+
+    p = small(seed=9, ats=1, out=2, cor=1, lmax=37)
+    p.receivers = W.sphere_points(_np.random.default_rng(77), nrec)
+    pf = p.write(workdir / f"many{nrec}.in")
+    model = Model(p.model_file)
+    ev = Event(model, Params(pf))
+    ref = yo.Problem(pf)
+    assert ev.nw % 16 != 0 or nrec % 32 != 0
+    for solver in SOLVERS:
+        engine.set_solver(solver)
+        engine.upload(model)
+        gu, gt, gp = engine.spectra(ev)
+        ru, rt, rp = ref.spectra(nthreads=8)
+        for g, r in ((gu, ru), (gt, rt), (gp, rp)):
+            for k in range(g.shape[0]):
+                assert rel_l2(g[k], r[k]) <= TOL, (solver, k)
+        got = engine.run(ev)
+        want = ref.run(nthreads=8)
+        for k in range(got.shape[0]):
+            for c in range(1, 4):
+                assert rel_l2(got[k, c], want[k, c]) <= TOL
