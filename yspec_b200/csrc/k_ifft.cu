@@ -23,6 +23,10 @@ constexpr int TILE_A = 512;
 
 __device__ __forceinline__ unsigned bitrev(unsigned g, int p) { return __brev(g) >> (32 - p); }
 
+// All extents below are powers of two: index arithmetic uses shifts and
+// masks (log2 by count of trailing zeros), never integer division.
+__device__ __forceinline__ int lg2(int v) { return __ffs(v) - 1; }
+
 // Element i (0-based, natural order) of the filtered Hermitian row.
 __device__ __forceinline__ cd row_value(unsigned i, const TraceDev& td, const cd* __restrict__ spec,
                                         const double* __restrict__ filt)
@@ -56,12 +60,13 @@ __global__ void __launch_bounds__(TILE_A / 2) k_ifft_a(TraceDev td, const cd* __
         d[t] = row_value(bitrev(base + t, p), td, spec, filt);
     __syncthreads();
     const int half = tile / 2, hb = b1 / 2, n2 = n / 2;
+    const int lhb = lg2(hb), ln2 = lg2(n2);
     for (int s = 0, mh = 1; mh < b1; s++, mh <<= 1) {
         for (int t = threadIdx.x; t < half; t += blockDim.x) {
-            const int sb = t / hb, tt = t - sb * hb;
-            const int grp = tt / mh, pos = tt - grp * mh;
+            const int sb = t >> lhb, tt = t & (hb - 1);
+            const int grp = tt >> s, pos = tt & (mh - 1);
             const int i = sb * b1 + grp * 2 * mh + pos, j = i + mh;
-            const cd w = tw[(size_t)pos * (n2 / mh)];
+            const cd w = tw[(size_t)pos << (ln2 - s)];
             const cd tmp = w * d[j];
             const cd di = d[i];
             d[j] = di - tmp;
@@ -83,17 +88,18 @@ __global__ void __launch_bounds__(256) k_ifft_b(TraceDev td, int G, const cd* __
     const int k = row / 3, c = row - 3 * k;
     const int r0 = blockIdx.x * G;
     const cd* src = scr + (size_t)row * n;
+    const int lG = lg2(G), lB2 = lg2(B2);
     for (int e = threadIdx.x; e < G * B2; e += blockDim.x) {
-        const int g = e % G, u = e / G;
+        const int g = e & (G - 1), u = e >> lG;
         sb[e] = src[(size_t)r0 + g + (size_t)b1 * u];
     }
     __syncthreads();
     const int nbf = G * B2 / 2;
-    for (int mu = 1; mu < B2; mu <<= 1) {
-        const int stride = B2 / (2 * mu);
+    for (int mu = 1, lmu = 0; mu < B2; mu <<= 1, lmu++) {
+        const int stride = 1 << (lB2 - lmu - 1);
         for (int t = threadIdx.x; t < nbf; t += blockDim.x) {
-            const int g = t % G, tt = t / G;
-            const int grp = tt / mu, posu = tt - grp * mu;
+            const int g = t & (G - 1), tt = t >> lG;
+            const int grp = tt >> lmu, posu = tt & (mu - 1);
             const int u = grp * 2 * mu + posu, v = u + mu;
             const int r = r0 + g;
             const cd w = tw[(size_t)(r + b1 * posu) * stride];
@@ -107,7 +113,7 @@ __global__ void __launch_bounds__(256) k_ifft_b(TraceDev td, int G, const cd* __
     (void)n2;
     double* o = out + (size_t)td.nout * 4 * k;
     for (int e = threadIdx.x; e < G * B2; e += blockDim.x) {
-        const int g = e % G, u = e / G;
+        const int g = e & (G - 1), u = e >> lG;
         const int i = r0 + g + b1 * u;
         if (i >= td.nout) continue;
         // data/(dt*n), * e^{eps t}, * amplitude scale (yspec.f90:439-460)
