@@ -25,7 +25,7 @@ def _parse_set(items: list[str]) -> dict:
     out = {}
     for kv in items:
         k, v = kv.split("=", 1)
-        out[k] = type(getattr(W.Params(), k))(v)
+        out[k] = int(v) if k == "nrec" else type(getattr(W.Params(), k))(v)
     return out
 
 

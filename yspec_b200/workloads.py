@@ -106,8 +106,10 @@ def moment_tensor(rng: np.random.Generator) -> list[float]:
 
 
 def config(name: str, seed: int = 0, **over) -> list[Params]:
-    """Parameter sets of a configuration (one per event)."""
+    """Parameter sets of a configuration (one per event).  `over` sets
+    Params fields; nrec=n keeps each event's first n receivers."""
     rng = np.random.default_rng(seed)
+    nrec = over.pop("nrec", None)
     if name == "c1":
         (ls, lo), = sphere_points(rng, 1)
         p = Params(ats=0, grav=2, out=0, cor=0, lmax=150, fmin=0.1, fmax=10.0, tout=60.0, dt=10.0,
@@ -150,4 +152,6 @@ def config(name: str, seed: int = 0, **over) -> list[Params]:
     for p in ps:
         for k, v in over.items():
             setattr(p, k, v)
+        if nrec is not None:
+            p.receivers = p.receivers[: int(nrec)]
     return ps
