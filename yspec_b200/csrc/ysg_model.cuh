@@ -94,8 +94,11 @@ static_assert(sizeof(Seg) == 432, "segment record size");
 
 __device__ __forceinline__ double seg(const Seg& s, double t, int p)
 {
-    const double* c = s.c[p];
-    return fma(fma(fma(c[3], t, c[2]), t, c[1]), t, c[0]);
+    // two 128-bit loads through the read-only path (the table never changes
+    // during a launch)
+    const double2* c = reinterpret_cast<const double2*>(s.c[p]);
+    const double2 lo = __ldg(c), hi = __ldg(c + 1);
+    return fma(fma(fma(hi.y, t, hi.x), t, lo.y), t, lo.x);
 }
 
 }  // namespace ysg
