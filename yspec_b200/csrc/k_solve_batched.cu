@@ -2,15 +2,17 @@
 //
 // Same per-pair work as the plain form (yspec.f90:259-400 for one
 // (omega_j, l)), organised for the B200:
-//   * one thread per pair, but the five Cash-Karp stage vectors of the
+//   * one thread per pair, but the Cash-Karp stage vectors of the
 //     14-component minor / b-vector systems live in a per-thread slab of
-//     shared memory (70 complex values, 1120 bytes), interleaved across the
-//     lanes of a warp so accesses are bank-conflict free and every offset is
-//     a constant; y and the stage input stay in registers.  Three 64-thread
-//     blocks share an SM.  (Folding the stages into partial sums needs only
-//     four slots and fits a fourth block, but the extra stage code overflows
-//     the instruction cache: measured slower.)  The plain form keeps all
-//     stage vectors in local memory, which spills through L1 into L2.
+//     shared memory: four slots of 14 complex values (896 bytes), the stages
+//     folded into partial sums as they are produced (ysg_ode.cuh
+//     rkck_step_loop), interleaved across the lanes of a warp so accesses
+//     are bank-conflict free and every offset is a constant; y and the
+//     stage input stay in registers.  Four 64-thread blocks (57 KB each)
+//     fill an SM's 228 KB of shared memory -- two warps on every SMSP --
+//     once the kernel asks for the largest shared-memory carveout.  The
+//     plain form keeps all stage vectors in local memory, which spills
+//     through L1 into L2.
 //   * a persistent grid (resident blocks only) pulls work items from an
 //     atomic counter, one item per warp.  Schedule 0: an item is (event, l,
 //     32 consecutive frequencies); the lanes share l and step through
@@ -28,12 +30,12 @@
 
 namespace ysg {
 
-constexpr int SLAB = 5 * 14;     // complex entries per thread (five stage slots)
+constexpr int SLAB = 4 * 14;     // complex entries per thread (four stage slots)
 
-// Three 64-thread blocks per SM (the shared memory admits three), each
-// thread with the full 255 registers.
+// Four 64-thread blocks per SM (shared memory admits four), each thread
+// with the full 255 registers.
 template <int SCHED>
-__global__ void __launch_bounds__(64, 3) k_solve_batched(const Knot* __restrict__ kn,
+__global__ void __launch_bounds__(64, 4) k_solve_batched(const Knot* __restrict__ kn,
                                                       const Seg* __restrict__ sg,
                                                       const ModelHdr* __restrict__ mh,
                                                       const EventDev* __restrict__ evs,
@@ -123,8 +125,10 @@ int solve_batched_blocks(int variant)
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
         return 0;
     SolveFn f = solve_fn(variant);
+    // the largest carveout: four slabs need all 228 KB of the SM's shared memory
     if (cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)solve_smem()) !=
             cudaSuccess ||
+        cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, 100) != cudaSuccess ||
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, f, kBlock, solve_smem()) != cudaSuccess)
         return 0;
     if (per < 1) per = 1;

@@ -470,89 +470,97 @@ __device__ __forceinline__ void rkck_step(const Ctx& c, cd* y, double x, double 
 // values per entry (no bank conflicts) and every offset is a constant.
 constexpr int KS = 32;
 
-struct SlabOut {
+// Cash-Karp tableau (module_int.f90:2039-2049) for the looped step with
+// four slab slots A0..A3.  Stages 1-4 store k1..k4 in A0..A3.  Forming the
+// stage-5 input also folds A1 (k2, not needed again: c2 = 0) into the
+// partial stage-6 input P6 = b61 k1 + b62 k2 + b63 k3 + b64 k4, and k5 is
+// added into it (A1 += b65 k5) as the right-hand side produces it; forming
+// the stage-6 input from A1 then folds A1 into the partial increment
+// F = c1 k1 + c3 k3 + c4 k4 (c5 = 0), and k6 is added into it
+// (A1 += c6 k6); finally y += h A1.  The same sums as the textbook form,
+// associated differently.
+//   ck_in[s][t]   weight of slot t in the stage-s input (times h)
+//   ck_fold[s][t] weight of slot t in the new A1 (stages 5 and 6)
+//   ck_slot[s], ck_w[s]: where stage s's derivative goes and with what
+//   weight (store for stages 1-4, add for 5 and 6)
+__constant__ double ck_a[6] = {0.0, 0.2, 0.3, 0.6, 1.0, 0.875};
+__constant__ double ck_in[6][4] = {
+    {0.0, 0.0, 0.0, 0.0},
+    {0.2, 0.0, 0.0, 0.0},
+    {3.0 / 40.0, 9.0 / 40.0, 0.0, 0.0},
+    {0.3, -0.9, 1.2, 0.0},
+    {-11.0 / 54.0, 2.5, -70.0 / 27.0, 35.0 / 27.0},
+    {0.0, 1.0, 0.0, 0.0}};
+__constant__ double ck_fold[6][4] = {
+    {0.0, 0.0, 0.0, 0.0},
+    {0.0, 0.0, 0.0, 0.0},
+    {0.0, 0.0, 0.0, 0.0},
+    {0.0, 0.0, 0.0, 0.0},
+    {1631.0 / 55296.0, 175.0 / 512.0, 575.0 / 13824.0, 44275.0 / 110592.0},
+    {37.0 / 378.0, 0.0, 250.0 / 621.0, 125.0 / 594.0}};
+__constant__ int ck_slot[6] = {0, 1, 2, 3, 1, 1};
+__constant__ double ck_w[6] = {1.0, 1.0, 1.0, 1.0, 253.0 / 4096.0, 512.0 / 1771.0};
+
+// Derivative writer: stores (add = false) or adds w * value (add = true)
+// into one slab slot.  Held by value so it lives in registers.
+struct SlotOut {
     cd* p;
-    __device__ __forceinline__ cd& operator[](int i) const { return p[i * KS]; }
+    double w;
+    bool add;
+    struct Ref {
+        cd* a;
+        double w;
+        bool add;
+        __device__ __forceinline__ void operator=(cd v) const
+        {
+            if (add) *a += w * v;
+            else *a = v;
+        }
+    };
+    __device__ __forceinline__ Ref operator[](int i) const { return Ref{p + i * KS, w, add}; }
 };
 
-// Cash-Karp tableau (module_int.f90:2039-2049) for the looped step.
-__constant__ double ck_a[6] = {0.0, 0.2, 0.3, 0.6, 1.0, 0.875};
-__constant__ double ck_b[6][5] = {
-    {0.0, 0.0, 0.0, 0.0, 0.0},
-    {0.2, 0.0, 0.0, 0.0, 0.0},
-    {3.0 / 40.0, 9.0 / 40.0, 0.0, 0.0, 0.0},
-    {0.3, -0.9, 1.2, 0.0, 0.0},
-    {-11.0 / 54.0, 2.5, -70.0 / 27.0, 35.0 / 27.0, 0.0},
-    {1631.0 / 55296.0, 175.0 / 512.0, 575.0 / 13824.0, 44275.0 / 110592.0, 253.0 / 4096.0}};
-
 // The step as a runtime loop over the six stages with one copy of the
-// right-hand side: the unrolled form inlines six 14-component RHS bodies,
-// which overflows the instruction cache and leaves warps waiting on
-// instruction fetch.  Stage vectors live in the thread's shared-memory slab;
-// the sixth stage reuses the second stage's entries.
+// right-hand side (six inlined 14-component bodies overflow the
+// instruction cache); the stage inputs and the two folds are loops over
+// the slots with weights from the tables above, so the step body stays
+// small.  Four slots of 14 complex values let four 64-thread blocks share
+// an SM.
 template <class Sys>
 __device__ __forceinline__ void rkck_step_loop(const Ctx& c, cd* y, double x, double h)
 {
     constexpr int N = Sys::N;
-    constexpr double c1 = 37.0 / 378.0, c3 = 250.0 / 621.0, c4 = 125.0 / 594.0,
-                     c6 = 512.0 / 1771.0;
+    constexpr int S = N * KS;                // slot stride in the slab
     cd* const kb = c.kb;
     cd yt[N];
 #pragma unroll 1
     for (int s = 0; s < 6; s++) {
 #pragma unroll
         for (int i = 0; i < N; i++) yt[i] = y[i];
-        for (int j = 0; j < s; j++) {
-            const double hb = h * ck_b[s][j];
-            const cd* kj = kb + j * N * KS;
+#pragma unroll 1
+        for (int t = 0; t < 4; t++) {
+            const double wt = ck_in[s][t];
+            if (wt == 0.0) continue;
+            const double hb = h * wt;
+            const cd* kt = kb + t * S;
 #pragma unroll
-            for (int i = 0; i < N; i++) yt[i] += hb * kj[i * KS];
+            for (int i = 0; i < N; i++) yt[i] += hb * kt[i * KS];
         }
-        const int slot = (s == 5) ? 1 : s;
-        Sys::f(c, x + ck_a[s] * h, yt, SlabOut{kb + slot * N * KS});
+        if (s >= 4) {
+            const double f0 = ck_fold[s][0], f1 = ck_fold[s][1], f2 = ck_fold[s][2],
+                         f3 = ck_fold[s][3];
+            cd* const a1 = kb + S;
+#pragma unroll 1
+            for (int i = 0; i < N; i++) {
+                const int o = i * KS;
+                a1[o] = f0 * kb[o] + f1 * a1[o] + f2 * kb[2 * S + o] + f3 * kb[3 * S + o];
+            }
+        }
+        Sys::f(c, x + ck_a[s] * h, yt, SlotOut{kb + ck_slot[s] * S, ck_w[s], s >= 4});
     }
+    const cd* a1 = kb + S;
 #pragma unroll
-    for (int i = 0; i < N; i++)
-        y[i] = y[i] + h * (c1 * kb[i * KS] + c3 * kb[(2 * N + i) * KS] + c4 * kb[(3 * N + i) * KS] +
-                           c6 * kb[(N + i) * KS]);
-}
-
-template <class Sys>
-__device__ __forceinline__ void rkck_step_smem(const Ctx& c, cd* y, double x, double h)
-{
-    constexpr int N = Sys::N;
-    constexpr double a2 = 0.2, a3 = 0.3, a4 = 0.6, a5 = 1.0, a6 = 0.875;
-    constexpr double b21 = 0.2, b31 = 3.0 / 40.0, b32 = 9.0 / 40.0;
-    constexpr double b41 = 0.3, b42 = -0.9, b43 = 1.2;
-    constexpr double b51 = -11.0 / 54.0, b52 = 2.5, b53 = -70.0 / 27.0, b54 = 35.0 / 27.0;
-    constexpr double b61 = 1631.0 / 55296.0, b62 = 175.0 / 512.0, b63 = 575.0 / 13824.0,
-                     b64 = 44275.0 / 110592.0, b65 = 253.0 / 4096.0;
-    constexpr double c1 = 37.0 / 378.0, c3 = 250.0 / 621.0, c4 = 125.0 / 594.0,
-                     c6 = 512.0 / 1771.0;
-    cd* const kb = c.kb;
-    const SlabOut K0{kb}, K1{kb + N * KS}, K2{kb + 2 * N * KS};
-    const SlabOut K3{kb + 3 * N * KS}, K4{kb + 4 * N * KS};
-    cd yt[N];
-    Sys::f(c, x, y, K0);
-#pragma unroll
-    for (int i = 0; i < N; i++) yt[i] = y[i] + (b21 * h) * K0[i];
-    Sys::f(c, x + a2 * h, yt, K1);
-#pragma unroll
-    for (int i = 0; i < N; i++) yt[i] = y[i] + h * (b31 * K0[i] + b32 * K1[i]);
-    Sys::f(c, x + a3 * h, yt, K2);
-#pragma unroll
-    for (int i = 0; i < N; i++) yt[i] = y[i] + h * (b41 * K0[i] + b42 * K1[i] + b43 * K2[i]);
-    Sys::f(c, x + a4 * h, yt, K3);
-#pragma unroll
-    for (int i = 0; i < N; i++)
-        yt[i] = y[i] + h * (b51 * K0[i] + b52 * K1[i] + b53 * K2[i] + b54 * K3[i]);
-    Sys::f(c, x + a5 * h, yt, K4);
-#pragma unroll
-    for (int i = 0; i < N; i++)
-        yt[i] = y[i] + h * (b61 * K0[i] + b62 * K1[i] + b63 * K2[i] + b64 * K3[i] + b65 * K4[i]);
-    Sys::f(c, x + a6 * h, yt, K1);   // the sixth stage reuses k2's entries
-#pragma unroll
-    for (int i = 0; i < N; i++) y[i] = y[i] + h * (c1 * K0[i] + c3 * K2[i] + c4 * K3[i] + c6 * K1[i]);
+    for (int i = 0; i < N; i++) y[i] = y[i] + h * a1[i * KS];
 }
 
 // yint's rescaling (module_int.f90:1910-1919, 1952-1961).  |y| is compared through
