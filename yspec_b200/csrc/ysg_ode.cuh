@@ -86,6 +86,10 @@ __device__ __forceinline__ void set_omega(Ctx& c, cd w)
     c.omega2 = w * w;
     c.omegai = 1.0 / w;
     c.omegai2 = c.omegai * c.omegai;
+    if (YSG_COUNT_ONLY) {          // the attenuation term steers no integer decision
+        c.lno = mk(0.0);
+        return;
+    }
     cd z = imul(w) / c.mh->tref;
     c.lno = c.ats * ((2.0 * clog(z)) / PI_D);
 }
@@ -730,6 +734,7 @@ __device__ __forceinline__ cd sbessj2(int l, cd x) { return x / (double)(float)(
 // (r dj/dr)/j, or its power series when Re(x^2) <= 0.
 __device__ inline cd bfs(int l, cd xsq, double eps)
 {
+    if (YSG_COUNT_ONLY) return mk(1.0);     // start values steer no integer decision
     if (xsq.x > 0.0) {
         cd x = csqrt(xsq);
         int lp1 = l + 1;

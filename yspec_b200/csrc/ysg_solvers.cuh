@@ -13,6 +13,7 @@ inline namespace YSG_VARIANT {
 
 __device__ __forceinline__ double huge_pow(int k)
 {
+    if (YSG_COUNT_ONLY) return 1.0;
     // huge**k for the integer exponents produced by the rescaling counters
     return k == 0 ? 1.0 : pow(SC_HUGE, (double)k);
 }
@@ -296,7 +297,9 @@ __device__ inline void sph_solver_g(Ctx& c, double rr, double rs, int ir, int is
     }
     cd delta = delta_solid(ms3, ms2);
     const int jump[4] = {0, 1, 3, 4};
-    for (int i = 0; i < 4; i++) {
+    // the four jumps integrate the same span at the same omega: in the
+    // count-only build one pass counts for four
+    for (int i = 0; i < (YSG_COUNT_ONLY ? 1 : 4); i++) {
         cd s[6] = {mk(0.0), mk(0.0), mk(0.0), mk(0.0), mk(0.0), mk(0.0)};
         s[jump[i]] = mk(1.0);
         int scale4 = 0;
@@ -315,6 +318,7 @@ __device__ inline void sph_solver_g(Ctx& c, double rr, double rs, int ir, int is
         double f = huge_pow(scale3 - scale4);
         for (int k = 0; k < 6; k++) yout[k][i] = ys[k] * f;
     }
+    if (YSG_COUNT_ONLY) c.nst[BvecSolidG::CLS] *= 4u;
 }
 
 // No gravity (KIND 0) / Cowling (KIND 1): sph_solver_ng (:827-1010),
@@ -374,7 +378,7 @@ __device__ inline void sph_solver_nc(Ctx& c, double rr, double rs, int ir, int i
         yint<MinorSolidNC<KIND>>(c, mh->nknot, ibot, kn[mh->nknot].r, rbot, ms2, &scale2);
     }
     cd delta = delta_solid_ngcow(ms3, ms2);
-    for (int i = 0; i < 4; i++) {
+    for (int i = 0; i < (YSG_COUNT_ONLY ? 1 : 4); i++) {     // see sph_solver_g
         cd s[4] = {mk(0.0), mk(0.0), mk(0.0), mk(0.0)};
         s[i] = mk(1.0);
         int scale4 = 0;
@@ -393,6 +397,7 @@ __device__ inline void sph_solver_nc(Ctx& c, double rr, double rs, int ir, int i
         double f = huge_pow(scale3 - scale4);
         for (int k = 0; k < 4; k++) yout[k][i] = ys[k] * f;
     }
+    if (YSG_COUNT_ONLY) c.nst[BvecSolidNC<KIND>::CLS] *= 4u;
 }
 
 // ---------------------------------------------------------------------------
