@@ -339,9 +339,13 @@ def run_b200(args) -> None:
         if world == 1 and not args.no_cpu:
             threads = os.cpu_count() or 1
             n, dt, nw, L = cpu_sample(pf, 1, threads)
+            n1, dt1, _, _ = cpu_sample(pf, 41, 1)
             line["cpu_baseline"] = {"value": n / dt, "unit": UNIT, "cores": threads, "kind": "port",
                                     "sample": f"the whole event: {nw} frequencies x {L} degrees "
-                                              f"({n} pairs, {dt:.1f} s on {threads} threads)"}
+                                              f"({n} pairs, {dt:.1f} s on {threads} threads)",
+                                    "single_thread": {"value": n1 / dt1, "unit": UNIT, "cores": 1,
+                                                      "sample": f"every 41st of {nw} frequencies x "
+                                                                f"{L} degrees ({n1} pairs, {dt1:.1f} s)"}}
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
