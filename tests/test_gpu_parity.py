@@ -153,3 +153,25 @@ def test_spectra_many_receivers_match_oracle(engine, workdir, nrec):
         for k in range(got.shape[0]):
             for c in range(1, 4):
                 assert rel_l2(got[k, c], want[k, c]) <= TOL
+
+
+def test_receivers_beyond_one_launch(engine, workdir):
+    """More receivers than one launch of the time-series stage takes (21,845:
+    three rows per receiver in grid.y): the stage runs in receiver chunks,
+    and receivers on both sides of a chunk boundary must match the oracle
+    run of those receivers alone."""
+    import numpy as _np
+
+    p = small(seed=12, lmax=20, fmax=4.0, f21=3.0, f22=3.8, dt=40.0, tout=40.0)
+    p.receivers = W.sphere_points(_np.random.default_rng(5), 21900)
+    pf = p.write(workdir / "wide.in")
+    model = Model(p.model_file)
+    engine.set_solver("batched")
+    engine.upload(model)
+    got = engine.run(Event(model, Params(pf)))
+    pick = [0, 21844, 21845, 21899]
+    p.receivers = [p.receivers[k] for k in pick]
+    want = yo.Problem(p.write(workdir / "pick.in")).run(nthreads=8)
+    for i, k in enumerate(pick):
+        for c in range(1, 4):
+            assert rel_l2(got[k, c], want[i, c]) <= TOL, (k, c)

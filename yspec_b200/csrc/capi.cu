@@ -459,6 +459,16 @@ int enqueue_solve(ysg_handle* h, int nev)
 int resolve_schedule(ysg_handle* h, int nev)
 {
     if (h->solver != 1) return YSG_OK;
+    // schedule 1 packs an entry as event (16 bits) | part | l index (23) | j - 1 (24)
+    bool packable = nev <= 65535;
+    for (int e = 0; e < nev && packable; e++) {
+        const EventDev& d = h->slots[(size_t)e].pev;
+        packable = d.lmax - d.lmin + 1 < (1 << 23) && d.nw < (1 << 24);
+    }
+    if (!packable) {
+        h->cur_sched = 0;
+        return YSG_OK;
+    }
     if (h->sched >= 0) {
         h->cur_sched = h->sched;
         return YSG_OK;

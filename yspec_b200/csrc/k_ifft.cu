@@ -241,21 +241,33 @@ cudaError_t launch_ifft(const TraceDev& td, const cd* ur, const cd* ut, const cd
     if (td.nr <= 0) return cudaSuccess;
     const int n = td.nt;
     if (n < 8 || n > (1 << 20)) return cudaErrorInvalidValue;
-    const int tile = n < FT ? n : FT;
-    dim3 ga(n / tile, 3 * td.nr);
-    k_ifft_a2<<<ga, tile / 8, 0, s>>>(td, ur, ut, up, filt, tw, scratch);
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
-    const int B2 = n / td.b1;
-    int G = FT / B2;
-    if (G > td.b1) G = td.b1;
-    dim3 gb(td.b1 / G, 3 * td.nr);
-    k_ifft_b2<<<gb, G * B2 / 8, 0, s>>>(td, G, tw, expt, scratch, out);
-    e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
-    dim3 gr((td.nout + 255) / 256, td.nr);
-    k_rotate<<<gr, 256, 0, s>>>(td.nout, td.nr, cs_azep, out);
-    return cudaGetLastError();
+    // one row per receiver and component in grid.y (at most 65535): receivers
+    // go in chunks; each chunk's rows start at the top of the scratch buffer
+    const int chunk = 65535 / 3;
+    for (int k0 = 0; k0 < td.nr; k0 += chunk) {
+        TraceDev sub = td;
+        sub.nr = td.nr - k0 < chunk ? td.nr - k0 : chunk;
+        const size_t so = (size_t)k0 * td.nw;
+        const cd *sur = ur + so, *sut = ut + so, *sup = up + so;
+        double* sout = out + (size_t)k0 * td.nout * 4;
+        const int tile = n < FT ? n : FT;
+        dim3 ga(n / tile, 3 * sub.nr);
+        k_ifft_a2<<<ga, tile / 8, 0, s>>>(sub, sur, sut, sup, filt, tw, scratch);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        const int B2 = n / td.b1;
+        int G = FT / B2;
+        if (G > td.b1) G = td.b1;
+        dim3 gb(td.b1 / G, 3 * sub.nr);
+        k_ifft_b2<<<gb, G * B2 / 8, 0, s>>>(sub, G, tw, expt, scratch, sout);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        dim3 gr((td.nout + 255) / 256, sub.nr);
+        k_rotate<<<gr, 256, 0, s>>>(td.nout, sub.nr, cs_azep + 2 * (size_t)k0, sout);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
 }
 
 }  // namespace ysg
