@@ -155,3 +155,18 @@ def test_no_device_fails_loudly():
     with pytest.raises(N.YspecError) as ei:
         Engine(0)
     assert ei.value.status == 6               # YSG_ERR_NO_DEVICE: no CPU fallback
+
+
+def test_run_batch_reports_failing_file(workdir):
+    """Several parameter files: every file is read before any device work,
+    and a missing one is reported with its index (no GPU needed)."""
+    from yspec_b200 import workloads as W
+
+    p = W.config("c1", seed=1)[0]
+    p.write(workdir / "a.in")
+    files = (C.c_char_p * 3)(b"a.in", b"missing.in", b"a.in")
+    failed = C.c_int(-2)
+    rc = N.lib().ysh_run_batch(3, files, 0, 0, C.byref(failed))
+    assert rc == 101 and failed.value == 1
+    rc = N.lib().ysh_run_batch(0, files, 0, 0, C.byref(failed))
+    assert rc != 0
