@@ -243,6 +243,7 @@ def run_b200(args) -> None:
     p, pf = make_event(tmp)
     model = Model(p.model_file)
     eng = Engine(local, solver=args.solver)
+    eng.set_schedule(args.schedule)
     eng.upload(model)
     ev = Event(model, Params(pf))
     nr, nout = ev.nr, ev.nout()
@@ -358,6 +359,8 @@ def main() -> int:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--solver", default="batched", choices=["batched", "plain"])
+    ap.add_argument("--schedule", type=int, default=-1,
+                    help="batched-solver schedule: 0 tiles, 1 pair lists, 2 split pair lists, -1 autotuned")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-vs-plain comparison")
     args = ap.parse_args()

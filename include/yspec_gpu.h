@@ -177,16 +177,20 @@ int ysg_legendre_table(ysg_handle *h, int nr, int lmax, const double *delta, con
 int ysg_set_solver(ysg_handle *h, int which);
 
 /* Work schedule of the batched solver: 0 = tiles of (event, l, 32
- * consecutive frequencies) ordered by estimated cost; 1 = lists of 32 pairs
- * of equal code path and near-equal exact step-count cost (a count-only
- * pass and a sort before the solve); -1 (default) = autotuned: the first
- * time a workload signature is seen, the solve stage runs once with each
- * schedule and the faster is kept.  Results do not depend on the schedule. */
+ * consecutive frequencies) ordered by estimated cost; 1 = lists of 32
+ * entries (the spheroidal and the toroidal part of each pair) of equal code
+ * path and near-equal exact step-count cost (a count-only pass and a sort
+ * before the solve); 2 = the same lists in two concurrent launches, the
+ * spheroidal parts and the toroidal parts (a small-slab, higher-occupancy
+ * kernel on a second stream); -1
+ * (default) = autotuned: the first time a workload signature is seen, the
+ * solve stage runs once with each schedule and the fastest is kept.
+ * Results do not depend on the schedule beyond rounding. */
 int ysg_set_schedule(ysg_handle *h, int sched);
 
 /* Schedule of the last batched solve, and the solve-stage times in ms of
  * each schedule from the last autotuning run (tune_ms may be NULL). */
-int ysg_last_schedule(ysg_handle *h, int *sched, float tune_ms[2]);
+int ysg_last_schedule(ysg_handle *h, int *sched, float tune_ms[3]);
 
 /* Device times in ms of the last event's stages, measured with CUDA events
  * on the handle's stream: [0] Legendre table, [1] solves, [2] l-sum,

@@ -91,8 +91,9 @@ def test_batch_repeat_and_reshape(engine, workdir):
 
 
 def test_schedules_agree(engine, workdir):
-    """Both work schedules (tiles, cost-sorted pair lists) and the autotuned
-    choice give the same traces: each pair is computed by one thread with
+    """Every work schedule (tiles, cost-sorted pair lists, the lists split
+    into a spheroidal and a toroidal launch) and the autotuned choice give
+    the same traces: each pair is computed by one thread with
     the same arithmetic whatever lane or warp it lands in.  The two kernel
     instantiations inline the pair code separately, so the compiler may
     round a few operations differently: agreement is to 1e-12 relative L2
@@ -104,22 +105,23 @@ def test_schedules_agree(engine, workdir):
     engine.upload(model)
     evs = [Event(model, Params(pf)) for _, pf in cases]
     runs = {}
-    for sched in (0, 1, -1):
+    for sched in (0, 1, 2, -1):
         engine.set_schedule(sched)
         runs[sched] = engine.batch_run(evs)
         used, _ = engine.last_schedule()
-        assert used in (0, 1) and (sched < 0 or used == sched)
-    for s in (1, -1):
+        assert used in (0, 1, 2) and (sched < 0 or used == sched)
+    for s in (1, 2, -1):
         for a, b in zip(runs[0], runs[s]):
             np.testing.assert_array_equal(a[:, 0], b[:, 0])
             for k in range(a.shape[0]):
                 for c in range(1, 4):
                     assert rel_l2(b[k, c], a[k, c]) <= 1e-12
-    for (p, pf), g in zip(cases, runs[1]):
+    for (p, pf), g1, g2 in zip(cases, runs[1], runs[2]):
         want = yo.Problem(pf).run(nthreads=8)
-        for k in range(g.shape[0]):
-            for c in range(1, 4):
-                assert rel_l2(g[k, c], want[k, c]) <= TOL
+        for g in (g1, g2):
+            for k in range(g.shape[0]):
+                for c in range(1, 4):
+                    assert rel_l2(g[k, c], want[k, c]) <= TOL
     engine.set_schedule(1)
     single = engine.run(evs[1])
     np.testing.assert_array_equal(single, runs[1][1])

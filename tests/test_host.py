@@ -33,6 +33,19 @@ def test_library_exports_every_declared_symbol():
     assert not missing, missing
 
 
+def test_output_array_lengths_match_header():
+    """The buffers the Python API hands to the engine's fill-in entry points
+    are as long as the arrays include/yspec_gpu.h declares: a shorter one
+    would be written past its end."""
+    from yspec_b200 import api
+    txt = (ROOT / "include" / "yspec_gpu.h").read_text()
+    want = {"ysg_last_timings": api.N_STAGE_TIMES, "ysg_last_schedule": api.N_SCHEDULES}
+    for fn, n in want.items():
+        m = re.search(fn + r"\([^)]*\bfloat\s+\w+\[(\d+)\]\)", txt)
+        assert m, fn
+        assert int(m.group(1)) == n, fn
+
+
 @pytest.mark.parametrize("deck", DECKS)
 def test_model_bit_identical_to_oracle(workdir, deck):
     p = W.config("c1", seed=2, model_file=str(W.GOLDEN / deck), depth_r=3.0)[0]

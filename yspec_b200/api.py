@@ -22,6 +22,10 @@ import numpy as np
 
 from . import native as N
 
+# lengths of the arrays the engine fills (include/yspec_gpu.h)
+N_STAGE_TIMES = 4   # ysg_last_timings: legendre, solve, l-sum, time series
+N_SCHEDULES = 3     # ysg_last_schedule: tuning time of each batched-solver schedule
+
 
 def norms() -> dict:
     n = N.YshNorms()
@@ -134,13 +138,14 @@ class Engine:
         N.check(N.lib().ysg_set_solver(self.h, {"plain": 0, "batched": 1}[which]), "set_solver")
 
     def set_schedule(self, sched: int) -> None:
-        """Batched-solver schedule: 0 tiles, 1 cost-sorted pair lists, -1 autotuned."""
+        """Batched-solver schedule: 0 tiles, 1 cost-sorted pair lists, 2 the same lists
+        as a spheroidal and a toroidal launch, -1 autotuned."""
         N.check(N.lib().ysg_set_schedule(self.h, sched), "set_schedule")
 
     def last_schedule(self) -> tuple[int, list[float]]:
         """Schedule of the last batched solve and the last autotuning times (ms)."""
         s = C.c_int()
-        ms = (C.c_float * 2)()
+        ms = (C.c_float * N_SCHEDULES)()
         N.check(N.lib().ysg_last_schedule(self.h, C.byref(s), ms), "last_schedule")
         return s.value, list(ms)
 
@@ -215,7 +220,7 @@ class Engine:
         return tab
 
     def timings(self) -> list[float]:
-        ms = (C.c_float * 4)()
+        ms = (C.c_float * N_STAGE_TIMES)()
         N.check(N.lib().ysg_last_timings(self.h, ms), "timings")
         return list(ms)
 

@@ -119,10 +119,10 @@ struct ysg_handle {
     int sched = -1;                  // batched-solver schedule; -1 = autotuned
     int cur_sched = 0;               // schedule of the next solve launch
     std::map<Signature, int> tuned;  // autotuner choices
-    float tune_ms[NSCHED] = {};      // solve times of the last tuning run
+    float tune_ms[NSCHED] = {};      // solve times of the last tuning run (per schedule)
     bool tune_warm = false;          // every schedule's kernels have been launched once
     long long launches = 0;          // this library's kernels enqueued since the last prepare
-    int solve_blocks[NSCHED] = {};   // resident grid per schedule
+    int solve_blocks[NSOLVE_KERNELS] = {};   // resident grid per solve kernel
     bool has_spectra = false;
     // CUDA graph of the last batch (updated in place when the shape repeats)
     cudaGraphExec_t gexec = nullptr;
@@ -259,7 +259,7 @@ int upload_items(ysg_handle* h, std::vector<Item>& items, const std::vector<Even
     CK(h->items.ensure(std::max<size_t>(packed.size(), 1) * sizeof(int4)));
     CK(h->evdev.ensure(std::max<size_t>(evs.size(), 1) * sizeof(EventDev)));
     CK(h->coefptr.ensure(std::max<size_t>(coefs.size(), 1) * sizeof(cd*)));
-    CK(h->counter.ensure(sizeof(int)));
+    CK(h->counter.ensure(2 * sizeof(int)));
     if (!packed.empty())
         CK(cudaMemcpyAsync(h->items.p, packed.data(), packed.size() * sizeof(int4), cudaMemcpyHostToDevice, h->st));
     CK(cudaMemcpyAsync(h->evdev.p, evs.data(), evs.size() * sizeof(EventDev), cudaMemcpyHostToDevice, h->st));
@@ -283,8 +283,8 @@ int upload_items(ysg_handle* h, std::vector<Item>& items, const std::vector<Even
     h->nitems = (int)packed.size();
     h->npairs = np;
     h->nev_items = (int)evs.size();
-    for (int v = 0; v < NSCHED; v++) {
-        if (h->solve_blocks[v] == 0) h->solve_blocks[v] = solve_batched_blocks(v);
+    for (int v = 0; v < NSOLVE_KERNELS; v++) {
+        if (h->solve_blocks[v] == 0) h->solve_blocks[v] = solve_kernel_blocks(v);
         if (h->solve_blocks[v] == 0) return YSG_ERR_CUDA;
     }
     return YSG_OK;
@@ -411,6 +411,9 @@ int upload_time(ysg_handle* h, Slot& s, const ysg_time* tm, int nw)
 
 // K1 for slots 0..nev-1: one batched launch over all their items, or one
 // plain launch per event.
+int fork_side(ysg_handle* h, int nside);
+int join_side(ysg_handle* h, int nside);
+
 int enqueue_solve(ysg_handle* h, int nev)
 {
     CK(cudaMemsetAsync(h->work.p, 0, NSYS_COUNT * sizeof(unsigned long long), h->st));
@@ -425,8 +428,7 @@ int enqueue_solve(ysg_handle* h, int nev)
     } else {
         const int s = h->cur_sched;
         const unsigned long long* pairs = nullptr;
-        int nitems = h->nitems;
-        if (s == 1) {
+        if (s >= 1) {
             StepCost sc;
             for (int q = 0; q < NSYS_COUNT; q++) sc.flops[q] = kStepFlops[q];
             sc.base = kPairBaseFlops;
@@ -439,13 +441,35 @@ int enqueue_solve(ysg_handle* h, int nev)
                                     h->npairs, sc, keys, vals, h->sort_tmp.p, h->sort_tmp.cap, &sorted,
                                     h->st));
             pairs = sorted;
-            nitems = (int)((2 * h->npairs + 31) / 32);
         }
-        h->launches += 1;
-        CK(launch_solve_batched(s, h->kn.as<Knot>(), h->sg.as<Seg>(), h->hdr_dev.as<ModelHdr>(),
-                                h->evdev.as<EventDev>(), h->coefptr.as<cd*>(), h->items.as<int4>(),
-                                pairs, h->npairs, nitems, h->counter.as<int>(),
-                                h->work.as<unsigned long long>(), h->solve_blocks[s], h->st));
+        const long long np = h->npairs;
+        int* ctr = h->counter.as<int>();
+        auto launch = [&](int kid, long long plo, long long phi, int i0, int i1, int* cnt) {
+            h->launches += 1;
+            return launch_solve_kernel(kid, h->kn.as<Knot>(), h->sg.as<Seg>(), h->hdr_dev.as<ModelHdr>(),
+                                       h->evdev.as<EventDev>(), h->coefptr.as<cd*>(), h->items.as<int4>(),
+                                       pairs, plo, phi, i0, i1, cnt, h->work.as<unsigned long long>(),
+                                       h->solve_blocks[kid], h->st);
+        };
+        if (s == 0) {
+            CK(launch(0, 0, 0, 0, h->nitems, ctr));
+        } else if (s == 1) {
+            CK(launch(1, 0, 2 * np, 0, (int)((2 * np + 31) / 32), ctr));
+        } else {
+            // Spheroidal entries sort first (k_schedule.cu): [0, np), then the
+            // toroidal ones.  The two parts write disjoint coefficients: the
+            // toroidal launch runs on a side stream and takes SMs as the
+            // spheroidal kernel drains.
+            int rc = fork_side(h, 1);
+            if (rc) return rc;
+            CK(launch(2, 0, np, 0, (int)((np + 31) / 32), ctr));
+            cudaStream_t main = h->st;
+            h->st = h->side[0];
+            const cudaError_t e2 = launch(3, np, 2 * np, (int)(np / 32), (int)((2 * np + 31) / 32), ctr + 1);
+            h->st = main;
+            CK(e2);
+            if ((rc = join_side(h, 1))) return rc;
+        }
     }
     return YSG_OK;
 }
@@ -811,6 +835,8 @@ int ysg_set_schedule(ysg_handle* h, int sched)
     h->has_spectra = false;
     return YSG_OK;
 }
+
+static_assert(NSCHED == 3, "ysg_last_schedule's tune_ms[] holds 3 entries (yspec_gpu.h)");
 
 int ysg_last_schedule(ysg_handle* h, int* sched, float* tune_ms)
 {

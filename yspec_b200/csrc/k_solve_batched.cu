@@ -20,7 +20,10 @@
 //     most expensive first (longest-processing-time first), so the tail is
 //     short.  Schedule 1: an item is 32 pairs of equal code path and
 //     near-equal exact cost from the sorted list of k_schedule.cu, so the
-//     lanes of a warp finish together.
+//     lanes of a warp finish together.  Schedule 2: the same list run by two
+//     kernels, one for the spheroidal / radial entries and one for the
+//     toroidal entries, whose 2-component system needs an eighth of the slab
+//     and fewer registers, so more warps share an SM.
 //   * items may come from several events (different frequency grids,
 //     degrees, sources, switches) sharing one model: one launch serves a
 //     whole batch.
@@ -30,22 +33,31 @@
 
 namespace ysg {
 
-constexpr int SLAB = 4 * 14;     // complex entries per thread (four stage slots)
+// Launch shape per PART (which entries a kernel runs: 2 = every part of
+// every pair, 0 = spheroidal / radial entries only, 1 = toroidal entries
+// only).  The kernels that run 14-component systems need four slots of 14
+// complex values per thread: four 64-thread blocks fill the SM's shared
+// memory, each thread with the full 255 registers.  The toroidal-only
+// kernel steps a 2-component system: a small slab and a smaller register
+// budget (168 registers, no spills) let twelve warps share an SM.
+template <int PART>
+struct SolveCfg {
+    static constexpr int BLOCK = 64, MINB = 4, SLAB = 4 * 14;
+};
+template <>
+struct SolveCfg<1> {
+    static constexpr int BLOCK = 128, MINB = 3, SLAB = 4 * 2;
+};
 
-// Four 64-thread blocks per SM (shared memory admits four), each thread
-// with the full 255 registers.
-template <int SCHED>
-__global__ void __launch_bounds__(64, 4) k_solve_batched(const Knot* __restrict__ kn,
-                                                      const Seg* __restrict__ sg,
-                                                      const ModelHdr* __restrict__ mh,
-                                                      const EventDev* __restrict__ evs,
-                                                      cd* const* __restrict__ coefs,
-                                                      const int4* __restrict__ items,
-                                                      const unsigned long long* __restrict__ pairs,
-                                                      long long npairs, int nitems, int* counter,
-                                                      unsigned long long* __restrict__ work)
+template <int SCHED, int PART>
+__global__ void __launch_bounds__(SolveCfg<PART>::BLOCK, SolveCfg<PART>::MINB)
+    k_solve_batched(const Knot* __restrict__ kn, const Seg* __restrict__ sg,
+                    const ModelHdr* __restrict__ mh, const EventDev* __restrict__ evs,
+                    cd* const* __restrict__ coefs, const int4* __restrict__ items,
+                    const unsigned long long* __restrict__ pairs, long long plo, long long phi,
+                    int item0, int item_end, int* counter, unsigned long long* __restrict__ work)
 {
-    // the slab is all the shared memory a block has: four blocks fill the SM
+    constexpr int SLAB = SolveCfg<PART>::SLAB;
     extern __shared__ cd slab[];
     const int lane = threadIdx.x & 31;
     Ctx c;
@@ -57,9 +69,9 @@ __global__ void __launch_bounds__(64, 4) k_solve_batched(const Knot* __restrict_
     for (int q = 0; q < NSYS; q++) c.nst[q] = 0;
     for (;;) {
         int it = 0;
-        if (lane == 0) it = atomicAdd(counter, 1);
+        if (lane == 0) it = item0 + atomicAdd(counter, 1);
         it = __shfl_sync(0xffffffffu, it, 0);
-        if (it >= nitems) break;
+        if (it >= item_end) break;
         int e, li, j, part = 2;             // part: 0 spheroidal, 1 toroidal, 2 both
         if (SCHED == 0) {
             const int4 w = items[it];
@@ -69,30 +81,36 @@ __global__ void __launch_bounds__(64, 4) k_solve_batched(const Knot* __restrict_
             if (j > evs[e].nw) continue;
         } else {
             const long long p = (long long)it * 32 + lane;
-            if (p >= 2 * npairs) continue;
+            if (p < plo || p >= phi) continue;
             const unsigned long long v = pairs[p];
             if (v == ~0ull) continue;           // l < 2 has no toroidal entry
             e = (int)(v >> 48);
             part = (int)((v >> 47) & 1u);
             li = (int)((v >> 24) & 0x7fffffu);
             j = (int)(v & 0xffffffu) + 1;
+            if (PART != 2 && part != PART) continue;
         }
         const EventDev& ev = evs[e];
         const int l = ev.lmin + li;
         c.ats = (double)ev.ats;
         cd out[NCOEF];
         int q0 = 0, q1 = NCOEF;             // coefficients this entry writes
-        if (part == 1) {
+        if constexpr (PART == 1) {
             pair_toroidal(c, ev, l, j, out + 10);
             q0 = 10;
-        } else if (l == 0) {
-            pair_radial(c, ev, j, out);
         } else {
-            if (part == 2 && l > 1) pair_toroidal(c, ev, l, j, out + 10);
-            else
-                for (int q = 10; q < 15; q++) out[q] = mk(0.0);
-            pair_spheroidal(c, ev, l, j, out, out + 5);
-            if (part == 0 && l > 1) q1 = 10;
+            if (PART == 2 && part == 1) {
+                pair_toroidal(c, ev, l, j, out + 10);
+                q0 = 10;
+            } else if (l == 0) {
+                pair_radial(c, ev, j, out);
+            } else {
+                if (PART == 2 && part == 2 && l > 1) pair_toroidal(c, ev, l, j, out + 10);
+                else
+                    for (int q = 10; q < 15; q++) out[q] = mk(0.0);
+                pair_spheroidal(c, ev, l, j, out, out + 5);
+                if (part == 0 && l > 1) q1 = 10;
+            }
         }
         cd* dst = coefs[e] + (size_t)li * NCOEF * ev.nw + (j - 1);
         for (int q = q0; q < q1; q++) dst[(size_t)q * ev.nw] = out[q];
@@ -106,48 +124,66 @@ __global__ void __launch_bounds__(64, 4) k_solve_batched(const Knot* __restrict_
 
 namespace {
 
-constexpr int kBlock = 64;
-
 using SolveFn = void (*)(const Knot*, const Seg*, const ModelHdr*, const EventDev*, cd* const*,
-                         const int4*, const unsigned long long*, long long, int, int*,
-                         unsigned long long*);
+                         const int4*, const unsigned long long*, long long, long long, int, int,
+                         int*, unsigned long long*);
 
-SolveFn solve_fn(int sched) { return sched == 1 ? k_solve_batched<1> : k_solve_batched<0>; }
+struct KernelDesc {
+    SolveFn f;
+    int block;
+    size_t smem;
+};
 
-size_t solve_smem() { return (size_t)kBlock * SLAB * sizeof(cd); }
+template <int SCHED, int PART>
+KernelDesc desc()
+{
+    return {k_solve_batched<SCHED, PART>, SolveCfg<PART>::BLOCK,
+            (size_t)SolveCfg<PART>::BLOCK * SolveCfg<PART>::SLAB * sizeof(cd)};
+}
+
+KernelDesc kernel(int kid)
+{
+    switch (kid) {
+        case 1: return desc<1, 2>();
+        case 2: return desc<1, 0>();
+        case 3: return desc<1, 1>();
+        default: return desc<0, 2>();
+    }
+}
 
 }  // namespace
 
-int solve_batched_blocks(int variant)
+int solve_kernel_blocks(int kid)
 {
     int dev = 0, nsm = 0, per = 0;
     if (cudaGetDevice(&dev) != cudaSuccess ||
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
         return 0;
-    SolveFn f = solve_fn(variant);
-    // the largest carveout: four slabs need all 228 KB of the SM's shared memory
-    if (cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)solve_smem()) !=
+    const KernelDesc k = kernel(kid);
+    // the largest carveout: the 14-component kernels need all 228 KB of shared memory
+    if (cudaFuncSetAttribute(k.f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.smem) !=
             cudaSuccess ||
-        cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, 100) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, f, kBlock, solve_smem()) != cudaSuccess)
+        cudaFuncSetAttribute(k.f, cudaFuncAttributePreferredSharedMemoryCarveout, 100) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k.f, k.block, k.smem) != cudaSuccess)
         return 0;
     if (per < 1) per = 1;
     return nsm * per;
 }
 
-cudaError_t launch_solve_batched(int variant, const Knot* kn, const Seg* sg, const ModelHdr* mh,
-                                 const EventDev* evs_dev, cd* const* coefs_dev, const int4* items,
-                                 const unsigned long long* pairs, long long npairs, int nitems,
-                                 int* counter, unsigned long long* work, int nblocks, cudaStream_t st)
+cudaError_t launch_solve_kernel(int kid, const Knot* kn, const Seg* sg, const ModelHdr* mh,
+                                const EventDev* evs_dev, cd* const* coefs_dev, const int4* items,
+                                const unsigned long long* pairs, long long plo, long long phi,
+                                int item0, int item_end, int* counter, unsigned long long* work,
+                                int nblocks, cudaStream_t st)
 {
-    if (nitems <= 0) return cudaSuccess;
-    SolveFn f = solve_fn(variant);
-    cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)solve_smem());
+    if (item_end <= item0) return cudaSuccess;
+    const KernelDesc k = kernel(kid);
+    cudaError_t e = cudaFuncSetAttribute(k.f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.smem);
     if (e != cudaSuccess) return e;
     e = cudaMemsetAsync(counter, 0, sizeof(int), st);
     if (e != cudaSuccess) return e;
-    f<<<nblocks, kBlock, solve_smem(), st>>>(kn, sg, mh, evs_dev, coefs_dev, items, pairs, npairs,
-                                             nitems, counter, work);
+    k.f<<<nblocks, k.block, k.smem, st>>>(kn, sg, mh, evs_dev, coefs_dev, items, pairs, plo, phi, item0,
+                                          item_end, counter, work);
     return cudaGetLastError();
 }
 

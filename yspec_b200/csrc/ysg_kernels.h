@@ -16,17 +16,25 @@ cudaError_t launch_solve_plain(const Knot* kn, const Seg* sg, const ModelHdr& mh
 // K1 batched persistent: work items (event, l index, first frequency - 1)
 // of one or more events, one thread per (omega,l) pair, stage vectors in
 // shared memory.  counter must be device memory (reset by the launcher).
-// Schedules (k_solve_batched.cu): 0 = tiles of (event, l, 32 consecutive
+// Schedules of the batched solver: 0 = tiles of (event, l, 32 consecutive
 // frequencies) from `items`; 1 = lists of 32 entries from `pairs` (2 npairs
 // entries, the spheroidal and toroidal part of each pair, packed event << 48
-// | part << 47 | l index << 24 | j - 1, sorted by launch_pair_schedule).
-// solve_batched_blocks gives the resident grid of a schedule.
-constexpr int NSCHED = 2;
-int solve_batched_blocks(int sched);
-cudaError_t launch_solve_batched(int sched, const Knot* kn, const Seg* sg, const ModelHdr* mh,
-                                 const EventDev* evs_dev, cd* const* coefs_dev, const int4* items,
-                                 const unsigned long long* pairs, long long npairs, int nitems,
-                                 int* counter, unsigned long long* work, int nblocks, cudaStream_t st);
+// | part << 47 | l index << 24 | j - 1, sorted by launch_pair_schedule with
+// every spheroidal entry first); 2 = the same list as two concurrent
+// launches, the spheroidal entries [0, npairs) and the toroidal ones
+// [npairs, 2 npairs) with a small-slab kernel on a side stream.
+// Kernels (k_solve_batched.cu): kid 0 tiles, 1 pair lists (all parts),
+// 2 pair lists (spheroidal part), 3 pair lists (toroidal part).  A kernel
+// takes work items item0 .. item_end-1 (entries p = item 32 + lane in
+// [plo, phi) for the lists) from the device counter, which it resets.
+constexpr int NSCHED = 3;
+constexpr int NSOLVE_KERNELS = 4;
+int solve_kernel_blocks(int kid);
+cudaError_t launch_solve_kernel(int kid, const Knot* kn, const Seg* sg, const ModelHdr* mh,
+                                const EventDev* evs_dev, cd* const* coefs_dev, const int4* items,
+                                const unsigned long long* pairs, long long plo, long long phi,
+                                int item0, int item_end, int* counter, unsigned long long* work,
+                                int nblocks, cudaStream_t st);
 
 // Pair cost model and ordering for schedule 1 (k_schedule.cu).  off[e] is
 // the flat index of event e's first pair (off[nev] = npairs); keys and vals

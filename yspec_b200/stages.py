@@ -1,6 +1,6 @@
 """Time the device stages of a synthetic workload configuration.
 
-    python -m yspec_b200.stages c2 [--solver batched|plain] [--schedule 0|1] [--reps 3]
+    python -m yspec_b200.stages c2 [--solver batched|plain] [--schedule 0|1|2] [--reps 3]
                                    [--seed 0] [--set lmax=300 --set fmax=20.0] [--batch]
 
 Runs the configuration's first event through `Engine.run` (or, with
@@ -37,7 +37,7 @@ def main(argv=None) -> None:
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--event", type=int, default=0, help="event index within the configuration")
     ap.add_argument("--schedule", type=int, default=-1,
-                    help="batched-solver schedule: 0 tiles, 1 pair lists, -1 autotuned")
+                    help="batched-solver schedule: 0 tiles, 1 pair lists, 2 split pair lists, -1 autotuned")
     ap.add_argument("--batch", action="store_true", help="run every event of the configuration as one batch")
     ap.add_argument("--set", action="append", default=[], metavar="KEY=VALUE",
                     help="override a parameter of the configuration")
