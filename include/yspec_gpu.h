@@ -95,6 +95,15 @@ int ysg_create(ysg_handle **h, int device);
  * solver modules read).  Copies the arrays; the caller may free them. */
 int ysg_model_upload(ysg_handle *h, const ysg_model *m);
 
+/* Derivative of the uploaded model along one direction of model space, for
+ * the tangent-linear solver (ysg_set_solver 2): dm->val[p] and dm->cs[p]
+ * are the derivatives of the knot values and of their spline second
+ * derivatives.  Only those 26 arrays are read (nknot must match the
+ * uploaded model); radii, alpha, beta and the scalar fields are the
+ * uploaded model's.  No reference counterpart: the reference has no
+ * derivatives.  A new ysg_model_upload discards it. */
+int ysg_model_tangent_upload(ysg_handle *h, const ysg_model *dm);
+
 /* Spectra of one event: yspec.f90:250-426.  ur, ut, up are complex
  * (nw, nr) column-major host arrays (interleaved re/im), or NULL to keep
  * the spectra on the device only.  Also leaves the spectra on the device
@@ -173,7 +182,12 @@ int ysg_legendre_table(ysg_handle *h, int nr, int lmax, const double *delta, con
                        const double *st, double *table);
 
 /* Select the solve kernel: 0 = plain (one thread per (omega,l) pair, one
- * event per launch), 1 = batched persistent (default). */
+ * event per launch), 1 = batched persistent (default), 2 = tangent-linear:
+ * the solve stage returns the derivative of the uu / vv / ww coefficients
+ * along the direction given by ysg_model_tangent_upload, with the start
+ * levels and step counts of the uploaded model held fixed.  Every later
+ * stage is linear in the coefficients, so with solver 2 the spectra and
+ * traces of every entry point are the derivatives of the primal ones. */
 int ysg_set_solver(ysg_handle *h, int which);
 
 /* Work schedule of the batched solver: 0 = tiles of (event, l, 32

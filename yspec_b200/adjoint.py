@@ -15,8 +15,16 @@ batched solve launch, one CUDA graph).  `MomentTensorSynthetics` is a
 torch.autograd.Function over them.  Its backward is the exact adjoint of
 the linear map, dL/dmm_i = <dL/dtraces, G_i> / moment_norm.
 
-Gradients with respect to the model (per-knot rho, Vp, Vs) would need the
-adjoint of the radial integration itself.  They are not provided here.
+Gradients with respect to the earth model (per-knot rho, Vp, Vs) come from
+the tangent-linear solver (k_solve_tangent.cu): the per-pair solve compiled
+with dual numbers returns the derivative of every coefficient along one
+direction of the model, and the stages after it are linear, so a run with
+solver "tangent" returns the derivative of the traces along that direction
+(forward mode).  `ModelSynthetics` sweeps the 3 nknot knot parameters in
+its backward pass and contracts each derivative with the incoming gradient.
+The model arrays and their derivatives come from model_chain.KnotModel;
+start levels and step counts stay those of the deck's model (they are
+piecewise constant in the parameters).
 """
 from __future__ import annotations
 
@@ -108,3 +116,104 @@ def with_moment(event: Event, mm) -> _MomentCopy:
     or Engine.batch_run; it shares the event's receiver arrays."""
     mn = norms()["moment_norm"]
     return _MomentCopy(event, [m / mn for m in mm])
+
+
+def tangent_traces(engine: Engine, event, knot_model, direction, at=None) -> np.ndarray:
+    """Derivative of the event's Z, N, E traces (nr, 3, nout) along
+    direction = (drho, dvp, dvs) of the knot parameters at `at` (default: the
+    deck's), with the deck's start levels and step counts."""
+    km = knot_model
+    p = at if at is not None else km.params()
+    engine.set_solver("tangent")
+    try:
+        engine.upload(km.array_model(*p))
+        engine.upload_tangent(km.tangent(direction, at=p))
+        return engine.run(event)[:, 1:4, :]
+    finally:
+        engine.set_solver("batched")
+
+
+def _model_function():
+    import torch
+
+    class _ModelFn(torch.autograd.Function):
+        @staticmethod
+        def forward(ctx, rho, vp, vs, mm, syn):
+            G = syn._greens(rho, vp, vs)
+            ctx.save_for_backward(rho, vp, vs, mm, G)
+            ctx.syn = syn
+            return torch.einsum("i,iktn->ktn", mm, G) / syn.moment_norm
+
+        @staticmethod
+        def backward(ctx, grad):
+            rho, vp, vs, mm, G = ctx.saved_tensors
+            syn = ctx.syn
+            g_mm = torch.einsum("ktn,iktn->i", grad, G) / syn.moment_norm
+            g = syn._knot_gradient(rho, vp, vs, mm, grad)
+            n = syn.km.nknot
+            return g[:n], g[n:2 * n], g[2 * n:], g_mm, None
+
+    return _ModelFn
+
+
+class ModelSynthetics:
+    """Differentiable traces of one event with respect to the per-knot rho, Vp,
+    Vs of its earth model (SI units) and its moment tensor (N m).
+
+        km = model_chain.KnotModel(deck)
+        syn = ModelSynthetics(engine, event, km)
+        rho, vp, vs = (t.requires_grad_() for t in km.params())
+        traces = syn(rho, vp, vs, mm)        # (nr, 3, nout): Z, N, E
+        loss = 0.5 * ((traces - observed) ** 2).sum()
+        loss.backward()                      # rho.grad, vp.grad, vs.grad, mm.grad
+
+    Forward: the six unit-moment responses of the model at (rho, vp, vs), one
+    batched launch, combined with mm.  Backward: mm exactly as
+    MomentTensorSynthetics; each knot parameter by one tangent-linear run
+    along it (3 nknot runs, or those of `knots` only: the others get zero).
+    """
+
+    def __init__(self, engine: Engine, event: Event, knot_model, knots=None):
+        self.engine, self.event, self.km = engine, event, knot_model
+        self.moment_norm = norms()["moment_norm"]
+        n = knot_model.nknot
+        self.columns = (list(range(3 * n)) if knots is None else
+                        [q * n + k for q in range(3) for k in knots])
+        self._fn = _model_function()
+
+    def __call__(self, rho, vp, vs, mm):
+        return self._fn.apply(rho, vp, vs, mm, self)
+
+    def _greens(self, rho, vp, vs):
+        import torch
+
+        eng = self.engine
+        eng.set_solver("batched")
+        eng.upload(self.km.array_model(rho.detach(), vp.detach(), vs.detach()))
+        _, G = greens(eng, self.event)
+        return torch.from_numpy(G)
+
+    def _knot_gradient(self, rho, vp, vs, mm, grad):
+        """sum over traces of grad * d(traces)/d(parameter), per knot parameter."""
+        import torch
+
+        km, eng = self.km, self.engine
+        p = (rho.detach(), vp.detach(), vs.detach())
+        jac = km.jacobian(at=p)
+        n = km.nknot
+        z = np.zeros(n)
+        ev = with_moment(self.event, [float(x) for x in mm.detach()])
+        g = np.asarray(grad.detach().cpu().numpy(), dtype=np.float64)
+        out = np.zeros(3 * n)
+        eng.set_solver("tangent")
+        try:
+            eng.upload(km.array_model(*p))
+            from .model_chain import ArrayModel
+
+            for col in self.columns:
+                d = {k: v[:, col] for k, v in jac.items()}
+                eng.upload_tangent(ArrayModel(km.view0, km.r.numpy(), d, z, z))
+                out[col] = float(np.sum(g * eng.run(ev)[:, 1:4, :]))
+        finally:
+            eng.set_solver("batched")
+        return torch.from_numpy(out)

@@ -65,7 +65,10 @@ class Model:
 
     def __del__(self):
         if getattr(self, "ptr", None):
-            N.lib().ysh_free_model(self.ptr)
+            try:
+                N.lib().ysh_free_model(self.ptr)
+            except Exception:       # interpreter shutdown: the module may be gone
+                pass
             self.ptr = None
 
     def view(self) -> N.YsgModel:
@@ -131,11 +134,17 @@ class Engine:
 
     def __del__(self):
         if getattr(self, "h", None):
-            N.lib().ysg_destroy(self.h)
+            try:
+                N.lib().ysg_destroy(self.h)
+            except Exception:       # interpreter shutdown: the module may be gone
+                pass
             self.h = None
 
     def set_solver(self, which: str) -> None:
-        N.check(N.lib().ysg_set_solver(self.h, {"plain": 0, "batched": 1}[which]), "set_solver")
+        """"plain", "batched" or "tangent" (derivative of every output along the
+        model direction given to upload_tangent)."""
+        N.check(N.lib().ysg_set_solver(self.h, {"plain": 0, "batched": 1, "tangent": 2}[which]),
+                "set_solver")
 
     def set_schedule(self, sched: int) -> None:
         """Batched-solver schedule: 0 tiles, 1 cost-sorted pair lists, 2 the same lists
@@ -150,8 +159,16 @@ class Engine:
         return s.value, list(ms)
 
     def upload(self, model: Model) -> None:
+        """Upload a model: a Model read from a deck, or any object whose view()
+        returns a filled N.YsgModel (yspec_b200.model_chain.ArrayModel)."""
         v = model.view()
         N.check(N.lib().ysg_model_upload(self.h, C.byref(v)), "model_upload")
+
+    def upload_tangent(self, dmodel) -> None:
+        """Derivative of the uploaded model along one direction (an object with
+        view(), e.g. model_chain.ArrayModel holding derivative arrays)."""
+        v = dmodel.view()
+        N.check(N.lib().ysg_model_tangent_upload(self.h, C.byref(v)), "model_tangent_upload")
 
     def spectra(self, event: Event, copy: bool = True):
         nw, nr = event.nw, event.nr

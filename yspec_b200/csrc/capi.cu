@@ -99,7 +99,10 @@ struct ysg_handle {
     DevBuf kn, sg, hdr_dev;
     ModelHdr hdr{};
     std::vector<double> grav_host;   // knot gravity for the tilt correction
+    std::vector<double> r_host;      // knot radii of the uploaded model
     bool has_model = false;
+    DevBuf dkn, dsg;                 // model derivative for the tangent solver
+    bool has_tangent = false;
     // events
     std::vector<Slot> slots;
     int nactive = 0;                 // slots of the last prepare / batch
@@ -425,6 +428,15 @@ int enqueue_solve(ysg_handle* h, int nev)
             CK(launch_solve_plain(h->kn.as<Knot>(), h->sg.as<Seg>(), h->hdr, s.pev, s.coef.as<cd>(),
                                   h->work.as<unsigned long long>(), h->status.as<int>(), h->st));
         }
+    } else if (h->solver == 2) {
+        if (!h->has_tangent) return YSG_ERR_ARG;
+        for (int e = 0; e < nev; e++) {
+            const Slot& s = h->slots[(size_t)e];
+            h->launches += 1;
+            CK(launch_solve_tangent(h->kn.as<Knot>(), h->sg.as<Seg>(), h->dkn.as<Knot>(), h->dsg.as<Seg>(),
+                                    h->hdr_dev.as<ModelHdr>(), s.pev, s.coef.as<cd>(), nullptr,
+                                    h->work.as<unsigned long long>(), h->st));
+        }
     } else {
         const int s = h->cur_sched;
         const unsigned long long* pairs = nullptr;
@@ -743,6 +755,44 @@ int launch_batch_graph(ysg_handle* h, int nev)
     return YSG_OK;
 }
 
+// Knot records and power-form segments (ysg_model.cuh) of the 13 spline
+// parameters on radii r.  The segment coefficients are linear in the knot
+// values and second derivatives, so the same construction applied to their
+// derivatives gives the derivative tables of the tangent solver.
+void build_tables(int n, const double* r, const double* const* val, const double* const* cs,
+                  const double* alpha, const double* beta, std::vector<Knot>& rec, std::vector<Seg>& seg)
+{
+    rec.assign((size_t)n + 2, Knot{});
+    std::memset(rec.data(), 0, rec.size() * sizeof(Knot));
+    for (int i = 0; i < n; i++) {
+        Knot& k = rec[(size_t)i + 1];
+        k.r = r[i];
+        k.alpha = alpha ? alpha[i] : 0.0;
+        k.beta = beta ? beta[i] : 0.0;
+        for (int p = 0; p < NPARAM; p++) {
+            k.v[p][0] = val[p][i];
+            k.v[p][1] = cs[p][i];
+        }
+    }
+    seg.assign((size_t)n + 1, Seg{});
+    std::memset(seg.data(), 0, seg.size() * sizeof(Seg));
+    for (int i = 1; i < n; i++) {
+        Seg& s = seg[(size_t)i];
+        const Knot &a = rec[(size_t)i], &b = rec[(size_t)i + 1];
+        const double hh = b.r - a.r;
+        s.r0 = a.r;
+        for (int p = 0; p < NPARAM; p++) {
+            s.c[p][0] = a.v[p][0];
+            if (hh == 0.0) continue;
+            s.c[p][1] = (b.v[p][0] - a.v[p][0]) / hh - hh * (2.0 * a.v[p][1] + b.v[p][1]) / 6.0;
+            s.c[p][2] = 0.5 * a.v[p][1];
+            s.c[p][3] = (b.v[p][1] - a.v[p][1]) / (6.0 * hh);
+        }
+    }
+    seg[(size_t)n].r0 = rec[(size_t)n].r;
+    for (int p = 0; p < NPARAM; p++) seg[(size_t)n].c[p][0] = rec[(size_t)n].v[p][0];
+}
+
 }  // namespace
 
 extern "C" {
@@ -820,7 +870,7 @@ void ysg_destroy(ysg_handle* h)
 
 int ysg_set_solver(ysg_handle* h, int which)
 {
-    if (!h || which < 0 || which > 1) return YSG_ERR_ARG;
+    if (!h || which < 0 || which > 2) return YSG_ERR_ARG;
     h->solver = which;
     h->nactive = 0;          // work items depend on the solver: prepare again
     h->has_spectra = false;
@@ -862,18 +912,9 @@ int ysg_model_upload(ysg_handle* h, const ysg_model* m)
     const int n = m->nknot;
     if ((size_t)(n + 2) * sizeof(Knot) > 200 * 1024) return YSG_ERR_LIMIT;   // fits shared memory
     if (m->nic < 1 || m->noc <= m->nic || m->nsl <= m->noc || m->nsl > n) return YSG_ERR_ARG;
-    std::vector<Knot> rec((size_t)n + 2);
-    std::memset(rec.data(), 0, rec.size() * sizeof(Knot));
-    for (int i = 0; i < n; i++) {
-        Knot& k = rec[(size_t)i + 1];
-        k.r = m->r[i];
-        k.alpha = m->alpha[i];
-        k.beta = m->beta[i];
-        for (int p = 0; p < NPARAM; p++) {
-            k.v[p][0] = m->val[p][i];
-            k.v[p][1] = m->cs[p][i];
-        }
-    }
+    std::vector<Knot> rec;
+    std::vector<Seg> seg;
+    build_tables(n, m->r, m->val, m->cs, m->alpha, m->beta, rec, seg);
     ModelHdr hd{};
     hd.nknot = n;
     hd.nic = m->nic;
@@ -893,24 +934,6 @@ int ysg_model_upload(ysg_handle* h, const ysg_model* m)
     hd.tref = m->tref;
     hd.pibigg = m->pibigg;
     hd.fre_norm = m->fre_norm;
-    // power-form segments of the same splines (ysg_model.cuh, Seg)
-    std::vector<Seg> seg((size_t)n + 1);
-    std::memset(seg.data(), 0, seg.size() * sizeof(Seg));
-    for (int i = 1; i < n; i++) {
-        Seg& s = seg[(size_t)i];
-        const Knot &a = rec[(size_t)i], &b = rec[(size_t)i + 1];
-        const double hh = b.r - a.r;
-        s.r0 = a.r;
-        for (int p = 0; p < NPARAM; p++) {
-            s.c[p][0] = a.v[p][0];
-            if (hh == 0.0) continue;
-            s.c[p][1] = (b.v[p][0] - a.v[p][0]) / hh - hh * (2.0 * a.v[p][1] + b.v[p][1]) / 6.0;
-            s.c[p][2] = 0.5 * a.v[p][1];
-            s.c[p][3] = (b.v[p][1] - a.v[p][1]) / (6.0 * hh);
-        }
-    }
-    seg[(size_t)n].r0 = rec[(size_t)n].r;
-    for (int p = 0; p < NPARAM; p++) seg[(size_t)n].c[p][0] = rec[(size_t)n].v[p][0];
     cudaSetDevice(h->device);
     CK(h->kn.ensure(rec.size() * sizeof(Knot)));
     CK(cudaMemcpyAsync(h->kn.p, rec.data(), rec.size() * sizeof(Knot), cudaMemcpyHostToDevice, h->st));
@@ -921,9 +944,35 @@ int ysg_model_upload(ysg_handle* h, const ysg_model* m)
     CK(cudaStreamSynchronize(h->st));
     h->hdr = hd;
     h->grav_host.assign(m->val[P_GRAV], m->val[P_GRAV] + n);
+    h->r_host.assign(m->r, m->r + n);
     h->has_model = true;
+    h->has_tangent = false;
     h->has_spectra = false;
     for (Slot& s : h->slots) s.ev_ready = s.tm_ready = false;
+    return YSG_OK;
+}
+
+int ysg_model_tangent_upload(ysg_handle* h, const ysg_model* dm)
+{
+    if (!h || !dm) return YSG_ERR_ARG;
+    if (!h->has_model) return YSG_ERR_NO_MODEL;
+    const int n = dm->nknot;
+    if (n != h->hdr.nknot) return YSG_ERR_ARG;
+    for (int p = 0; p < NPARAM; p++)
+        if (!dm->val[p] || !dm->cs[p]) return YSG_ERR_ARG;
+    std::vector<Knot> rec;
+    std::vector<Seg> seg;
+    build_tables(n, h->r_host.data(), dm->val, dm->cs, nullptr, nullptr, rec, seg);
+    // the tables hold derivatives, except the radii the segments are based on
+    for (size_t i = 0; i < seg.size(); i++) seg[i].r0 = 0.0;
+    cudaSetDevice(h->device);
+    CK(h->dkn.ensure(rec.size() * sizeof(Knot)));
+    CK(cudaMemcpyAsync(h->dkn.p, rec.data(), rec.size() * sizeof(Knot), cudaMemcpyHostToDevice, h->st));
+    CK(h->dsg.ensure(seg.size() * sizeof(Seg)));
+    CK(cudaMemcpyAsync(h->dsg.p, seg.data(), seg.size() * sizeof(Seg), cudaMemcpyHostToDevice, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    h->has_tangent = true;
+    h->has_spectra = false;
     return YSG_OK;
 }
 

@@ -1,0 +1,83 @@
+// k_solve_tangent.cu -- tangent-linear solve stage.
+//
+// The per-pair solve of yspec.f90:259-400 compiled with dual numbers
+// (YSG_TANGENT, ysg_dual.cuh): every model value the solver reads comes with
+// its derivative along one direction of the earth model (the tangent knot
+// and segment tables), and each pair returns its uu / vv / ww coefficients
+// together with their derivatives.  The start levels, step counts and
+// rescaling decisions come from the value part, as in the primal solve.
+//
+// The l-sum, the filter, the inverse FFT and the post-processing that follow
+// are linear in the coefficients, so running them on the derivative
+// coefficients gives the derivative of the traces.  The kernel writes the
+// derivative coefficients in the layout of the primal ones (and, on request,
+// the values into a second buffer).
+//
+// One thread per (omega_j, l) pair, one event per launch, the stage vectors
+// in local memory: the dual solve needs twice the state of the primal one.
+#define YSG_TANGENT 1
+#include "ysg_kernels.h"
+#include "ysg_solvers.cuh"
+
+namespace ysg {
+
+__global__ void __launch_bounds__(128) k_solve_tangent(const Knot* __restrict__ kn,
+                                                       const Seg* __restrict__ sg,
+                                                       const Knot* __restrict__ dkn,
+                                                       const Seg* __restrict__ dsg,
+                                                       const ModelHdr* __restrict__ mh, EventDev ev,
+                                                       cd* __restrict__ dcoef, cd* __restrict__ vcoef,
+                                                       unsigned long long* __restrict__ work)
+{
+    const int L = ev.lmax - ev.lmin + 1;
+    const long long total = (long long)L * ev.nw;
+    const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    Ctx c;
+    c.kn = kn;
+    c.mh = mh;
+    c.pib = mh->pibigg;
+    c.ats = (double)ev.ats;
+    c.sg = sg;
+    c.kb = nullptr;
+    c.dkn = dkn;
+    c.dsg = dsg;
+    for (int q = 0; q < NSYS; q++) c.nst[q] = 0;
+    if (gid < total) {
+        const int li = (int)(gid / ev.nw);
+        const int j = (int)(gid - (long long)li * ev.nw) + 1;
+        const int l = ev.lmin + li;
+        mcplx out[NCOEF];
+        if (l == 0) {
+            pair_radial(c, ev, j, out);
+        } else {
+            if (l > 1) pair_toroidal(c, ev, l, j, out + 10);
+            else
+                for (int q = 10; q < 15; q++) out[q] = mk(0.0);
+            pair_spheroidal(c, ev, l, j, out, out + 5);
+        }
+        const size_t o = (size_t)li * NCOEF * ev.nw + (j - 1);
+        for (int q = 0; q < NCOEF; q++) dcoef[o + (size_t)q * ev.nw] = out[q].d;
+        if (vcoef)
+            for (int q = 0; q < NCOEF; q++) vcoef[o + (size_t)q * ev.nw] = out[q].v;
+    }
+    for (int q = 0; q < NSYS; q++) {
+        unsigned long long v = c.nst[q];
+        for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+        if ((threadIdx.x & 31) == 0 && v) atomicAdd(&work[q], v);
+    }
+}
+
+cudaError_t launch_solve_tangent(const Knot* kn, const Seg* sg, const Knot* dkn, const Seg* dsg,
+                                 const ModelHdr* mh, const EventDev& ev, cd* dcoef, cd* vcoef,
+                                 unsigned long long* work, cudaStream_t st)
+{
+    const long long total = (long long)(ev.lmax - ev.lmin + 1) * ev.nw;
+    if (total <= 0) return cudaSuccess;
+    const int bs = 128;
+    const long long nb = (total + bs - 1) / bs;
+    if (nb > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
+    k_solve_tangent<<<(unsigned)nb, bs, 0, st>>>(kn, sg, dkn, dsg, mh, ev, dcoef, vcoef, work);
+    return cudaGetLastError();
+}
+
+}  // namespace ysg

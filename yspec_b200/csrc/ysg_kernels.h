@@ -13,6 +13,12 @@ size_t solve_plain_smem(int nknot);
 cudaError_t launch_solve_plain(const Knot* kn, const Seg* sg, const ModelHdr& mh, const EventDev& ev,
                                cd* coef, unsigned long long* work, int* status, cudaStream_t st);
 
+// K1 tangent-linear: the plain layout with dual numbers; writes the
+// derivative coefficients to dcoef and, when vcoef is not null, the values.
+cudaError_t launch_solve_tangent(const Knot* kn, const Seg* sg, const Knot* dkn, const Seg* dsg,
+                                 const ModelHdr* mh, const EventDev& ev, cd* dcoef, cd* vcoef,
+                                 unsigned long long* work, cudaStream_t st);
+
 // K1 batched persistent: work items (event, l index, first frequency - 1)
 // of one or more events, one thread per (omega,l) pair, stage vectors in
 // shared memory.  counter must be device memory (reset by the launcher).

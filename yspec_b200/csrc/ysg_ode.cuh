@@ -13,15 +13,19 @@
 // points of the l = 0 gravity solve) are formed with explicitly rounded
 // operations so they agree bit for bit with the reference's unfused FP64.
 #pragma once
+#include "ysg_dual.cuh"
 #include "ysg_model.cuh"
 
-// Three builds of the solver code exist: the plain form keeps the Cash-Karp
+// Four builds of the solver code exist: the plain form keeps the Cash-Karp
 // stage vectors in per-thread arrays (the compiler places them in local
 // memory); with YSG_SMEM_STAGES the stage vectors live in a per-thread slab
 // of shared memory and only y and the stage input stay in registers; with
 // YSG_COUNT_ONLY yint only counts the steps it would take (the cost model of
 // the pair scheduler: every integer decision of a solve -- start levels,
-// layers, step counts -- is made as in a real solve, no state is stepped).
+// layers, step counts -- is made as in a real solve, no state is stepped);
+// with YSG_TANGENT every quantity that depends on the earth model is a dual
+// number (ysg_dual.cuh) and the solve returns, beside its value, the
+// derivative along one direction of the model (the tangent-linear solver).
 // Each form gets its own inline namespace so the translation units never
 // share a definition.
 #ifndef YSG_SMEM_STAGES
@@ -30,7 +34,12 @@
 #ifndef YSG_COUNT_ONLY
 #define YSG_COUNT_ONLY 0
 #endif
-#if YSG_COUNT_ONLY
+#ifndef YSG_TANGENT
+#define YSG_TANGENT 0
+#endif
+#if YSG_TANGENT
+#define YSG_VARIANT v_tangent
+#elif YSG_COUNT_ONLY
 #define YSG_VARIANT v_count
 #elif YSG_SMEM_STAGES
 #define YSG_VARIANT v_smem
@@ -40,6 +49,18 @@
 
 namespace ysg {
 inline namespace YSG_VARIANT {
+
+// Types of the quantities that depend on the earth model: model values and
+// everything formed from them (coefficient matrices, start vectors, the
+// solution).  Plain doubles and complex values except in the tangent build.
+// Quantities that depend only on omega, l and the radius stay double / cd.
+#if YSG_TANGENT
+using mreal = dreal;
+using mcplx = dcplx;
+#else
+using mreal = double;
+using mcplx = cd;
+#endif
 
 // nrtype.f90:18-27: pi_d and twopi_d are single-precision literals.
 constexpr double PI_D = (double)3.14159265358979323846f;
@@ -62,6 +83,10 @@ struct Ctx {
     unsigned nst[NSYS];
     const Seg* sg;   // power-form spline segments (right-hand sides)
     cd* kb;          // shared-memory stage slab of this thread (smem form)
+#if YSG_TANGENT
+    const Knot* dkn; // derivative of the knot values along the model direction
+    const Seg* dsg;  // derivative of the power-form segments
+#endif
     double zeta, zeta2, zeta2m2, szeta2m2, nu, dr, ats;
     double pib;      // pi * bigg of the model (module_model.f90:490), = mh->pibigg
     cd omega, omega2, omegai, omegai2, lno;
@@ -110,6 +135,27 @@ __device__ __forceinline__ void alpha_steps(Ctx& c)
     c.dr = (c.omega.x == 0.0) ? 1.0 / NW_STEP : 1.0 / (__dmul_rn((double)NW_STEP, c.omega.x) / a);
 }
 
+// Model value of parameter p on the current layer at offset u from its
+// base (power form), and at a knot-interval spline point (start values,
+// source vectors); duals in the tangent build.
+__device__ __forceinline__ mreal segr(const Ctx& c, const Seg& g, double u, int p)
+{
+#if YSG_TANGENT
+    return mreal(seg(g, u, p), seg(c.dsg[c.il], u, p));
+#else
+    return seg(g, u, p);
+#endif
+}
+
+__device__ __forceinline__ mreal splr(const Ctx& c, const SplPt& s, int p)
+{
+#if YSG_TANGENT
+    return mreal(spl(c.kn, s, p), spl(c.dkn, s, p));
+#else
+    return spl(c.kn, s, p);
+#endif
+}
+
 // ---------------------------------------------------------------------------
 // Coefficient matrices
 //
@@ -124,19 +170,19 @@ __device__ __forceinline__ void alpha_steps(Ctx& c)
 __device__ __forceinline__ double norm2(cd a) { return a.x * a.x + a.y * a.y; }
 
 // module_int.f90:134-164 tor_amat (t real, k and s complex)
-struct TorCoef { double t; cd k, s; };
+struct TorCoef { mreal t; mcplx k, s; };
 
 __device__ __forceinline__ TorCoef tor_amat(const Ctx& c, double rr)
 {
     const Seg& g = c.sg[c.il];
     const double u = rr - g.r0;
-    double rrho = seg(g, u, P_RHO), rlcon = seg(g, u, P_LCON);
-    double rncon = seg(g, u, P_NCON), rqmu = seg(g, u, P_QMU);
-    cd qll = 1.0 + rqmu * c.lno;
-    cd cncon = rncon * qll;
-    const double dl = rlcon * norm2(qll);
-    const double inv = 1.0 / (rr * dl);
-    double ri = dl * inv;
+    mreal rrho = segr(c, g, u, P_RHO), rlcon = segr(c, g, u, P_LCON);
+    mreal rncon = segr(c, g, u, P_NCON), rqmu = segr(c, g, u, P_QMU);
+    mcplx qll = 1.0 + rqmu * c.lno;
+    mcplx cncon = rncon * qll;
+    const mreal dl = rlcon * norm2(qll);
+    const mreal inv = 1.0 / (rr * dl);
+    mreal ri = dl * inv;
     TorCoef a;
     a.t = 2.0 * ri;
     a.k = conj(qll) * (rr * inv);     // 1 / (L (1 + qmu lno))
@@ -146,22 +192,22 @@ __device__ __forceinline__ TorCoef tor_amat(const Ctx& c, double rr)
 
 // module_int.f90:261-304 rad_amat.  rad_derivs_ng also calls this gravity
 // form (module_int.f90:388), so both radial systems share it.
-struct RadCoef { cd t, k, s; };
+struct RadCoef { mcplx t, k, s; };
 
 __device__ __forceinline__ RadCoef rad_amat(const Ctx& c, double rr)
 {
     const Seg& g = c.sg[c.il];
     const double u = rr - g.r0;
-    double rrho = seg(g, u, P_RHO), racon = seg(g, u, P_ACON), rccon = seg(g, u, P_CCON);
-    double rfcon = seg(g, u, P_FCON), rncon = seg(g, u, P_NCON), gg = seg(g, u, P_GRAV);
-    double rqmu = seg(g, u, P_QMU), rxlam = seg(g, u, P_XLAM), rxa2 = seg(g, u, P_XA2);
-    cd qaa = 1.0 + rxa2 * c.lno, qff = 1.0 + rxlam * c.lno, qll = 1.0 + rqmu * c.lno;
-    cd cacon = racon * qaa, cfcon = rfcon * qff, cncon = rncon * qll;
-    const double dc = rccon * norm2(qaa);
-    const double inv = 1.0 / (rr * dc);
-    cd cccon = conj(qaa) * (rr * inv);     // 1 / (C (1 + qa lno))
-    cd gamma = cacon - cncon - cfcon * cfcon * cccon;
-    double ri = dc * inv;
+    mreal rrho = segr(c, g, u, P_RHO), racon = segr(c, g, u, P_ACON), rccon = segr(c, g, u, P_CCON);
+    mreal rfcon = segr(c, g, u, P_FCON), rncon = segr(c, g, u, P_NCON), gg = segr(c, g, u, P_GRAV);
+    mreal rqmu = segr(c, g, u, P_QMU), rxlam = segr(c, g, u, P_XLAM), rxa2 = segr(c, g, u, P_XA2);
+    mcplx qaa = 1.0 + rxa2 * c.lno, qff = 1.0 + rxlam * c.lno, qll = 1.0 + rqmu * c.lno;
+    mcplx cacon = racon * qaa, cfcon = rfcon * qff, cncon = rncon * qll;
+    const mreal dc = rccon * norm2(qaa);
+    const mreal inv = 1.0 / (rr * dc);
+    mcplx cccon = conj(qaa) * (rr * inv);     // 1 / (C (1 + qa lno))
+    mcplx gamma = cacon - cncon - cfcon * cfcon * cccon;
+    mreal ri = dc * inv;
     RadCoef a;
     a.t = (1.0 - 2.0 * cfcon * cccon) * ri;
     a.k = cccon;
@@ -174,8 +220,8 @@ __device__ __forceinline__ RadCoef rad_amat(const Ctx& c, double rr)
 // 0 = no gravity (:564-616 / :720-747).  Entries that are real in value
 // are kept real.
 struct SolidCoef {
-    cd t11, t12, k11, k22, s11, s12, s22;
-    double t21, t22, t31, t33, k33, s13, s23;
+    mcplx t11, t12, k11, k22, s11, s12, s22;
+    mreal t21, t22, t31, t33, k33, s13, s23;
 };
 
 template <int KIND>
@@ -183,17 +229,17 @@ __device__ __forceinline__ SolidCoef solid_amat(const Ctx& c, double rr)
 {
     const Seg& g = c.sg[c.il];
     const double u = rr - g.r0;
-    double rrho = seg(g, u, P_RHO), racon = seg(g, u, P_ACON), rccon = seg(g, u, P_CCON);
-    double rfcon = seg(g, u, P_FCON), rncon = seg(g, u, P_NCON), rlcon = seg(g, u, P_LCON);
-    double rqmu = seg(g, u, P_QMU), rxlam = seg(g, u, P_XLAM), rxa2 = seg(g, u, P_XA2);
-    cd qaa = 1.0 + rxa2 * c.lno, qff = 1.0 + rxlam * c.lno, qll = 1.0 + rqmu * c.lno;
-    cd cacon = racon * qaa, cfcon = rfcon * qff, cncon = rncon * qll;
-    const double dc = rccon * norm2(qaa), dl = rlcon * norm2(qll);
-    const double inv = 1.0 / (rr * (dc * dl));
-    cd cccon = conj(qaa) * ((rr * dl) * inv);     // 1 / (C (1 + qa lno))
-    cd fc = cfcon * cccon;
-    cd gamma = cacon - cncon - cfcon * fc;
-    double ri = (dc * dl) * inv, ri2 = ri * ri;
+    mreal rrho = segr(c, g, u, P_RHO), racon = segr(c, g, u, P_ACON), rccon = segr(c, g, u, P_CCON);
+    mreal rfcon = segr(c, g, u, P_FCON), rncon = segr(c, g, u, P_NCON), rlcon = segr(c, g, u, P_LCON);
+    mreal rqmu = segr(c, g, u, P_QMU), rxlam = segr(c, g, u, P_XLAM), rxa2 = segr(c, g, u, P_XA2);
+    mcplx qaa = 1.0 + rxa2 * c.lno, qff = 1.0 + rxlam * c.lno, qll = 1.0 + rqmu * c.lno;
+    mcplx cacon = racon * qaa, cfcon = rfcon * qff, cncon = rncon * qll;
+    const mreal dc = rccon * norm2(qaa), dl = rlcon * norm2(qll);
+    const mreal inv = 1.0 / (rr * (dc * dl));
+    mcplx cccon = conj(qaa) * ((rr * dl) * inv);     // 1 / (C (1 + qa lno))
+    mcplx fc = cfcon * cccon;
+    mcplx gamma = cacon - cncon - cfcon * fc;
+    mreal ri = (dc * dl) * inv, ri2 = ri * ri;
     SolidCoef a;
     a.t11 = (1.0 - 2.0 * fc) * ri;
     a.t12 = (c.zeta * ri) * fc;
@@ -201,14 +247,14 @@ __device__ __forceinline__ SolidCoef solid_amat(const Ctx& c, double rr)
     a.t22 = 2.0 * ri;
     a.k11 = cccon;
     a.k22 = conj(qll) * ((rr * dc) * inv);       // 1 / (L (1 + qmu lno))
-    cd mw2r = -(c.omega2 * rrho);
+    mcplx mw2r = -(c.omega2 * rrho);
     a.s22 = mw2r + (c.zeta2 * (gamma + cncon) - 2.0 * cncon) * ri2;
     if (KIND == 0) {
         a.s11 = mw2r + (4.0 * gamma) * ri2;
         a.s12 = (-2.0 * c.zeta) * gamma * ri2;
     } else {
-        double gg = seg(g, u, P_GRAV);
-        double rgr = rrho * gg * rr;
+        mreal gg = segr(c, g, u, P_GRAV);
+        mreal rgr = rrho * gg * rr;
         a.s11 = mw2r + (4.0 * (gamma - rgr)) * ri2;
         a.s12 = (c.zeta * (rgr - 2.0 * gamma)) * ri2;
     }
@@ -226,8 +272,8 @@ __device__ __forceinline__ SolidCoef solid_amat(const Ctx& c, double rr)
 }
 
 struct FluidCoef {
-    cd t11, t12, k11, s11, s12, s22;
-    double t21, t22, k22;
+    mcplx t11, t12, k11, s11, s12, s22;
+    mreal t21, t22, k22;
 };
 
 template <int KIND>
@@ -235,13 +281,13 @@ __device__ __forceinline__ FluidCoef fluid_amat(const Ctx& c, double rr)
 {
     const Seg& g = c.sg[c.il];
     const double u = rr - g.r0;
-    double rrho = seg(g, u, P_RHO), rccon = seg(g, u, P_CCON), rxa2 = seg(g, u, P_XA2);
-    cd qaa = 1.0 + rxa2 * c.lno;
-    const double dc = rccon * norm2(qaa);
-    const double inv = 1.0 / (rr * rrho * dc);
-    cd cccon = conj(qaa) * ((rr * rrho) * inv);  // 1 / (C (1 + qa lno))
-    double ri = (rrho * dc) * inv;
-    const double irho = (rr * dc) * inv;          // 1 / rho
+    mreal rrho = segr(c, g, u, P_RHO), rccon = segr(c, g, u, P_CCON), rxa2 = segr(c, g, u, P_XA2);
+    mcplx qaa = 1.0 + rxa2 * c.lno;
+    const mreal dc = rccon * norm2(qaa);
+    const mreal inv = 1.0 / (rr * rrho * dc);
+    mcplx cccon = conj(qaa) * ((rr * rrho) * inv);  // 1 / (C (1 + qa lno))
+    mreal ri = (rrho * dc) * inv;
+    const mreal irho = (rr * dc) * inv;          // 1 / rho
     FluidCoef a;
     a.k11 = cccon - (c.zeta2 * c.omegai2) * ((ri * ri) * irho);
     if (KIND == 0) {
@@ -251,8 +297,8 @@ __device__ __forceinline__ FluidCoef fluid_amat(const Ctx& c, double rr)
         a.t21 = a.t22 = a.k22 = 0.0;
         return a;
     }
-    double gg = seg(g, u, P_GRAV);
-    cd gzw = (gg * c.zeta2) * c.omegai2;
+    mreal gg = segr(c, g, u, P_GRAV);
+    mcplx gzw = (gg * c.zeta2) * c.omegai2;
     a.t11 = (gzw * ri - 1.0) * ri;
     a.s11 = -(c.omega2 * rrho) + (rrho * gg) * ((gzw * ri - 4.0) * ri);
     if (KIND == 2) {
@@ -276,7 +322,7 @@ __device__ __forceinline__ FluidCoef fluid_amat(const Ctx& c, double rr)
 struct TorSys {
     static constexpr int N = 2, CLS = 0;
     template <class Out>
-    __device__ static __forceinline__ void f(const Ctx& c, double r, const cd* y, Out d)
+    __device__ static __forceinline__ void f(const Ctx& c, double r, const mcplx* y, Out d)
     {
         TorCoef a = tor_amat(c, r);       // module_int.f90:168-184
         d[0] = a.t * y[0] + a.k * y[1];
@@ -287,7 +333,7 @@ struct TorSys {
 struct RadSys {
     static constexpr int N = 2, CLS = 1;
     template <class Out>
-    __device__ static __forceinline__ void f(const Ctx& c, double r, const cd* y, Out d)
+    __device__ static __forceinline__ void f(const Ctx& c, double r, const mcplx* y, Out d)
     {
         RadCoef a = rad_amat(c, r);       // module_int.f90:357-392
         d[0] = a.t * y[0] + a.k * y[1];
@@ -299,11 +345,11 @@ struct RadSys {
 struct MinorSolidG {
     static constexpr int N = 14, CLS = 6;
     template <class Out>
-    __device__ static __forceinline__ void f(const Ctx& c, double r, const cd* m, Out d)
+    __device__ static __forceinline__ void f(const Ctx& c, double r, const mcplx* m, Out d)
     {
         SolidCoef a = solid_amat<2>(c, r);
-        cd a123 = a.t11 + (a.t22 + a.t33), a126 = a.t11 + (a.t22 - a.t33);
-        cd a135 = a.t11 - (a.t22 - a.t33), a234 = (a.t22 + a.t33) - a.t11;
+        mcplx a123 = a.t11 + (a.t22 + a.t33), a126 = a.t11 + (a.t22 - a.t33);
+        mcplx a135 = a.t11 - (a.t22 - a.t33), a234 = (a.t22 + a.t33) - a.t11;
         d[0] = a.k33 * m[3] - a.k22 * m[5] + a.k11 * m[9] + m[0] * a123;
         d[1] = -(a.k22 * m[6]) + m[0] * a.s13 - m[2] * a.t21 + m[1] * a.t22 - m[3] * a.t31;
         d[2] = -(a.k11 * m[10]) + m[0] * a.s23 + m[2] * a.t11 - m[1] * a.t12;
@@ -336,10 +382,10 @@ template <int KIND>
 struct MinorSolidNC {
     static constexpr int N = 5, CLS = 4;
     template <class Out>
-    __device__ static __forceinline__ void f(const Ctx& c, double r, const cd* m, Out d)
+    __device__ static __forceinline__ void f(const Ctx& c, double r, const mcplx* m, Out d)
     {
         SolidCoef a = solid_amat<KIND>(c, r);
-        cd a11 = a.t11 + a.t22, a22 = a.t11 - a.t22;
+        mcplx a11 = a.t11 + a.t22, a22 = a.t11 - a.t22;
         d[0] = a11 * m[0] + a.k22 * m[2] - a.k11 * m[3];
         d[1] = a.s12 * m[0] - a.t21 * m[2] + a.t12 * m[3];
         d[2] = a.s22 * m[0] - 2.0 * (a.t12 * m[1]) + a22 * m[2] + a.k11 * m[4];
@@ -352,10 +398,10 @@ struct MinorSolidNC {
 struct MinorFluidG {
     static constexpr int N = 5, CLS = 5;
     template <class Out>
-    __device__ static __forceinline__ void f(const Ctx& c, double r, const cd* m, Out d)
+    __device__ static __forceinline__ void f(const Ctx& c, double r, const mcplx* m, Out d)
     {
         FluidCoef a = fluid_amat<2>(c, r);
-        cd tp = a.t11 + a.t22, tm = a.t11 - a.t22;
+        mcplx tp = a.t11 + a.t22, tm = a.t11 - a.t22;
         d[0] = a.k22 * m[2] - a.k11 * m[3] + m[0] * tp;
         d[1] = m[0] * a.s12 + m[3] * a.t12 - m[2] * a.t21;
         d[2] = a.k11 * m[4] + m[0] * a.s22 - 2.0 * (m[1] * a.t12) + m[2] * tm;
@@ -369,7 +415,7 @@ template <int KIND>
 struct MinorFluidNC {
     static constexpr int N = 2, CLS = 2;
     template <class Out>
-    __device__ static __forceinline__ void f(const Ctx& c, double r, const cd* m, Out d)
+    __device__ static __forceinline__ void f(const Ctx& c, double r, const mcplx* m, Out d)
     {
         FluidCoef a = fluid_amat<KIND>(c, r);
         d[0] = a.t11 * m[0] + a.k11 * m[1];
@@ -381,13 +427,13 @@ struct MinorFluidNC {
 struct BvecSolidG {
     static constexpr int N = 14, CLS = 7;
     template <class Out>
-    __device__ static __forceinline__ void f(const Ctx& c, double r, const cd* b, Out d)
+    __device__ static __forceinline__ void f(const Ctx& c, double r, const mcplx* b, Out d)
     {
         SolidCoef a = solid_amat<2>(c, r);
-        const cd t11 = a.t11, t12 = a.t12, k11 = a.k11, k22 = a.k22;
-        const cd s11 = a.s11, s12 = a.s12, s22 = a.s22;
-        const double t21 = a.t21, t22 = a.t22, t31 = a.t31, t33 = a.t33, k33 = a.k33;
-        const double s13 = a.s13, s23 = a.s23;
+        const mcplx t11 = a.t11, t12 = a.t12, k11 = a.k11, k22 = a.k22;
+        const mcplx s11 = a.s11, s12 = a.s12, s22 = a.s22;
+        const mreal t21 = a.t21, t22 = a.t22, t31 = a.t31, t33 = a.t33, k33 = a.k33;
+        const mreal s13 = a.s13, s23 = a.s23;
         d[0] = s11 * b[6] + s12 * (b[7] - b[2]) + s13 * b[8] - s22 * b[3] - s23 * b[4] -
                (t11 + t22) * b[0] + t31 * b[5];
         d[1] = s11 * b[9] + s12 * b[10] - s13 * (2.0 * b[2] + b[7]) - s23 * b[3] -
@@ -416,7 +462,7 @@ template <int KIND>
 struct BvecSolidNC {
     static constexpr int N = 4, CLS = 3;
     template <class Out>
-    __device__ static __forceinline__ void f(const Ctx& c, double r, const cd* b, Out d)
+    __device__ static __forceinline__ void f(const Ctx& c, double r, const mcplx* b, Out d)
     {
         SolidCoef a = solid_amat<KIND>(c, r);
         d[0] = -(a.s11 * b[2]) - a.s12 * b[3] - a.t11 * b[0] - a.t21 * b[1];
@@ -431,7 +477,7 @@ struct BvecSolidNC {
 // the 1e+-20 rescaling of yint (module_int.f90:1910-1919).
 // ---------------------------------------------------------------------------
 template <class Sys>
-__device__ __forceinline__ void rkck_step(const Ctx& c, cd* y, double x, double h)
+__device__ __forceinline__ void rkck_step(const Ctx& c, mcplx* y, double x, double h)
 {
     constexpr int N = Sys::N;
     constexpr double a2 = 0.2, a3 = 0.3, a4 = 0.6, a5 = 1.0, a6 = 0.875;
@@ -442,7 +488,7 @@ __device__ __forceinline__ void rkck_step(const Ctx& c, cd* y, double x, double 
                      b64 = 44275.0 / 110592.0, b65 = 253.0 / 4096.0;
     constexpr double c1 = 37.0 / 378.0, c3 = 250.0 / 621.0, c4 = 125.0 / 594.0,
                      c6 = 512.0 / 1771.0;
-    cd k1[N], k2[N], k3[N], k4[N], k5[N], yt[N];
+    mcplx k1[N], k2[N], k3[N], k4[N], k5[N], yt[N];
     Sys::f(c, x, y, k1);
     const double hb21 = b21 * h;
 #pragma unroll
@@ -572,19 +618,19 @@ __device__ __forceinline__ void rkck_step_loop(const Ctx& c, cd* y, double x, do
 // decision can differ from the reference only within rounding of a bound,
 // where either choice scales y exactly as the scale count records.
 template <int N>
-__device__ __forceinline__ void rescale(cd* y, int* scale)
+__device__ __forceinline__ void rescale(mcplx* y, int* scale)
 {
     constexpr double TINY2 = SC_TINY * SC_TINY, HUGE2 = SC_HUGE * SC_HUGE;
     bool all_small = true, any_big = false;
 #pragma unroll
-    for (int k = 0; k < N; k++) all_small = all_small && (norm2(y[k]) < TINY2);
+    for (int k = 0; k < N; k++) all_small = all_small && (val(norm2(y[k])) < TINY2);
     if (all_small) {
         (*scale)++;
 #pragma unroll
         for (int k = 0; k < N; k++) y[k] = y[k] * SC_HUGE;
     }
 #pragma unroll
-    for (int k = 0; k < N; k++) any_big = any_big || (norm2(y[k]) > HUGE2);
+    for (int k = 0; k < N; k++) any_big = any_big || (val(norm2(y[k])) > HUGE2);
     if (any_big) {
         (*scale)--;
 #pragma unroll
@@ -600,7 +646,7 @@ __device__ __forceinline__ void rescale(cd* y, int* scale)
 #endif
 
 template <class Sys>
-__device__ YSG_YINT_ATTR void yint(Ctx& cio, int i1, int i2, double r1, double r2, cd* yio, int* scale)
+__device__ YSG_YINT_ATTR void yint(Ctx& cio, int i1, int i2, double r1, double r2, mcplx* yio, int* scale)
 {
     if (r2 == r1) return;
 #if YSG_SMEM_STAGES
@@ -612,7 +658,7 @@ __device__ YSG_YINT_ATTR void yint(Ctx& cio, int i1, int i2, double r1, double r
     for (int k = 0; k < Sys::N; k++) y[k] = yio[k];
 #else
     Ctx& c = cio;
-    cd* y = yio;
+    mcplx* y = yio;
 #endif
     const bool up = r2 > r1;
     const Knot* kn = c.kn;
@@ -728,43 +774,43 @@ __device__ inline int sph_start_level(const Ctx& c, int l, double w, int it)
 // Start values
 // ---------------------------------------------------------------------------
 // module_function.f90:447-490: the ratio j_{l+1}/j_l is the stub x/(2l+3).
-__device__ __forceinline__ cd sbessj2(int l, cd x) { return x / (double)(float)(2 * l + 3); }
+__device__ __forceinline__ mcplx sbessj2(int l, mcplx x) { return x / (double)(float)(2 * l + 3); }
 
 // module_function.f90:520-581 bfs: Lentz continued fraction for
 // (r dj/dr)/j, or its power series when Re(x^2) <= 0.
-__device__ inline cd bfs(int l, cd xsq, double eps)
+__device__ inline mcplx bfs(int l, mcplx xsq, double eps)
 {
     if (YSG_COUNT_ONLY) return mk(1.0);     // start values steer no integer decision
-    if (xsq.x > 0.0) {
-        cd x = csqrt(xsq);
+    if (val(xsq).x > 0.0) {
+        mcplx x = csqrt(xsq);
         int lp1 = l + 1;
-        cd rx = 2.0 / x;
+        mcplx rx = 2.0 / x;
         double nu = (double)lp1 - 0.5;
-        cd rj = nu * rx;
+        mcplx rj = nu * rx;
         rx = -rx;
-        cd denom = (nu + 1.0) * rx;
-        cd numer = denom + 1.0 / rj;
+        mcplx denom = (nu + 1.0) * rx;
+        mcplx numer = denom + 1.0 / rj;
         rj = (rj * numer) / denom;
         int nm1 = 1;
         for (int it = 0; it < 100000; it++) {
             nm1 = nm1 + 1;
             rx = -rx;
-            cd a3 = (nu + (double)nm1) * rx;
+            mcplx a3 = (nu + (double)nm1) * rx;
             denom = a3 + 1.0 / denom;
             numer = a3 + 1.0 / numer;
-            cd ratio = numer / denom;
+            mcplx ratio = numer / denom;
             rj = rj * ratio;
-            if (fabs(cabs(ratio) - 1.0) <= eps) break;
+            if (fabs(val(cabs(ratio)) - 1.0) <= eps) break;
         }
         return rj * x - (double)lp1;
     }
-    cd f = mk(1.0), fp = mk((double)(float)l), a = mk(1.0);
+    mcplx f = mk(1.0), fp = mk((double)(float)l), a = mk(1.0);
     double b = (double)(float)(l + l) + 1.0, cc = 2.0, d = (double)(float)l + 2.0;
     for (int it = 0; it < 100000; it++) {
         a = -(a * xsq) / (cc * (b + cc));
         f = f + a;
         fp = fp + a * d;
-        if (cabs(a * d) < eps) break;
+        if (val(cabs(a * d)) < eps) break;
         cc = cc + 2.0;
         d = d + 2.0;
     }
@@ -772,85 +818,85 @@ __device__ inline cd bfs(int l, cd xsq, double eps)
 }
 
 // module_function.f90:497-516 bfs_dum: the argument is sqrt(|x^2|).
-__device__ __forceinline__ cd bfs_dum(int l, cd xsq)
+__device__ __forceinline__ mcplx bfs_dum(int l, mcplx xsq)
 {
-    cd fp = bfs(l, xsq, 1.e-9);
-    double x = sqrt(cabs(xsq));
+    mcplx fp = bfs(l, xsq, 1.e-9);
+    mreal x = sqrt(cabs(xsq));
     return ((double)l - fp) / x;
 }
 
 // module_int.f90:213-250 tor_ystart
-__device__ inline void tor_ystart(const Ctx& c, int is, double rr, cd* y)
+__device__ inline void tor_ystart(const Ctx& c, int is, double rr, mcplx* y)
 {
     SplPt s = spl_at(c.kn, is, rr);
-    double rrho = spl(c.kn, s, P_RHO), rmu = spl(c.kn, s, P_MU), rqmu = spl(c.kn, s, P_QMU);
-    cd cmu = rmu * (1.0 + rqmu * c.lno);
-    cd cbeta = csqrt(cmu / rrho);
-    cd arg = (c.omega / cbeta) * rr;
-    cd ratio = sbessj2(c.llp1, arg);
+    mreal rrho = splr(c, s, P_RHO), rmu = splr(c, s, P_MU), rqmu = splr(c, s, P_QMU);
+    mcplx cmu = rmu * (1.0 + rqmu * c.lno);
+    mcplx cbeta = csqrt(cmu / rrho);
+    mcplx arg = (c.omega / cbeta) * rr;
+    mcplx ratio = sbessj2(c.llp1, arg);
     y[0] = mk(c.zeta * rr);
     y[1] = c.zeta * (cmu * ((double)(c.ll - 1) - arg * ratio));
 }
 
 // module_int.f90:417-489 rad_ystart (GRAV) / rad_ystart_ng
 template <bool GRAV>
-__device__ inline void rad_ystart(const Ctx& c, int is, double rr, cd* y)
+__device__ inline void rad_ystart(const Ctx& c, int is, double rr, mcplx* y)
 {
     SplPt s = spl_at(c.kn, is, rr);
     const Knot* kn = c.kn;
-    double rrho = spl(kn, s, P_RHO), rmu = spl(kn, s, P_MU), rqmu = spl(kn, s, P_QMU);
-    double rkappa = spl(kn, s, P_KAPPA), rqkappa = spl(kn, s, P_QKAPPA);
-    cd cmu = rmu * (1.0 + rqmu * c.lno);
-    cd ckappa = rkappa * (1.0 + rqkappa * c.lno);
-    cd calpha = ckappa + (4.0 * cmu) / 3.0;
-    cd gamma = GRAV ? c.omega2 + (16.0 * c.mh->pibigg * rrho) / 3.0 : c.omega2;
+    mreal rrho = splr(c, s, P_RHO), rmu = splr(c, s, P_MU), rqmu = splr(c, s, P_QMU);
+    mreal rkappa = splr(c, s, P_KAPPA), rqkappa = splr(c, s, P_QKAPPA);
+    mcplx cmu = rmu * (1.0 + rqmu * c.lno);
+    mcplx ckappa = rkappa * (1.0 + rqkappa * c.lno);
+    mcplx calpha = ckappa + (4.0 * cmu) / 3.0;
+    mcplx gamma = GRAV ? c.omega2 + (16.0 * c.mh->pibigg * rrho) / 3.0 : c.omega2;
     gamma = (rrho * gamma) / calpha;
-    cd arg = gamma * rr;
-    cd ratio = sbessj2(1, arg);
+    mcplx arg = gamma * rr;
+    mcplx ratio = sbessj2(1, arg);
     y[0] = rr * ratio;
     y[1] = (rr * calpha) * gamma - (4.0 * cmu) * ratio;
 }
 
-__device__ __forceinline__ cd det2(cd a1, cd a2, cd b1, cd b2) { return a1 * b2 - a2 * b1; }
+__device__ __forceinline__ mcplx det2(mcplx a1, mcplx a2, mcplx b1, mcplx b2) { return a1 * b2 - a2 * b1; }
 
 // module_int.f90:1192-1270 sph_solid_start followed by the 14 minors of
 // module_int.f90:1451-1485 (sph_minor_solid_start).
-__device__ inline void sph_minor_solid_start(const Ctx& c, int is, double rr, cd* m)
+__device__ inline void sph_minor_solid_start(const Ctx& c, int is, double rr, mcplx* m)
 {
     SplPt s = spl_at(c.kn, is, rr);
     const Knot* kn = c.kn;
     double pib = c.mh->pibigg;
-    double rrho = spl(kn, s, P_RHO), rmu = spl(kn, s, P_MU), rqmu = spl(kn, s, P_QMU);
-    double rkappa = spl(kn, s, P_KAPPA), rqkappa = spl(kn, s, P_QKAPPA);
-    cd cmu = rmu * (1.0 + rqmu * c.lno);
-    cd ckappa = rkappa * (1.0 + rqkappa * c.lno);
-    cd calpha = (ckappa + 1.3333333333 * cmu) / rrho;
-    cd cbeta = cmu / rrho;
-    cd tmp1 = c.omega2 / cbeta;
-    cd tmp2 = (c.omega2 + (5.3333333 * pib) * rrho) / calpha;
-    double t3 = 2.666666666 * pib * c.zeta * rrho;
-    cd tmp3 = (t3 * t3) / (calpha * cbeta);
+    mreal rrho = splr(c, s, P_RHO), rmu = splr(c, s, P_MU), rqmu = splr(c, s, P_QMU);
+    mreal rkappa = splr(c, s, P_KAPPA), rqkappa = splr(c, s, P_QKAPPA);
+    mcplx cmu = rmu * (1.0 + rqmu * c.lno);
+    mcplx ckappa = rkappa * (1.0 + rqkappa * c.lno);
+    mcplx calpha = (ckappa + 1.3333333333 * cmu) / rrho;
+    mcplx cbeta = cmu / rrho;
+    mcplx tmp1 = c.omega2 / cbeta;
+    mcplx tmp2 = (c.omega2 + (5.3333333 * pib) * rrho) / calpha;
+    mreal t3 = 2.666666666 * pib * c.zeta * rrho;
+    mcplx tmp3 = (t3 * t3) / (calpha * cbeta);
     double ll = (double)c.ll, llp1 = (double)c.llp1;
-    cd y[6][3];
+    mcplx y[6][3];
     double sign = 1.0;
     for (int i = 0; i < 2; i++) {
-        cd dd = tmp1 - tmp2;
-        cd gamma = dd * dd + tmp3;
+        mcplx dd = tmp1 - tmp2;
+        mcplx gamma = dd * dd + tmp3;
         gamma = 0.5 * (tmp1 + tmp2) + (0.5 * sign) * csqrt(gamma);
-        cd gamma2 = gamma;
+        mcplx gamma2 = gamma;
         gamma = csqrt(gamma);
-        cd zt = ((0.75 * cbeta) * (gamma2 - tmp1)) / (pib * rrho);
-        cd xi = zt - llp1;
-        cd args = (gamma2 * rr) * rr;
-        cd ratio = bfs_dum(c.ll, args);
-        cd grr = (gamma * rr) * ratio;
+        mcplx zt = ((0.75 * cbeta) * (gamma2 - tmp1)) / (pib * rrho);
+        mcplx xi = zt - llp1;
+        mcplx args = (gamma2 * rr) * rr;
+        mcplx ratio = bfs_dum(c.ll, args);
+        mcplx grr = (gamma * rr) * ratio;
         y[0][i] = ll * xi - zt * grr;
         y[1][i] = c.zeta * (xi + grr);
         y[2][i] = -(((4.0 * pib * rrho) * rr) * zt);
         y[3][i] = -((((rrho * calpha) * zt) * rr) * gamma2) +
                   (((2.0 * cmu) * ll) * (ll - 1.0)) * xi / rr +
                   ((2.0 * cmu) * (2.0 * zt + c.zeta2)) * gamma * ratio;
-        cd y5 = rr * gamma2 + ((2.0 * (ll - 1.0)) * xi) / rr - ((2.0 * (zt + 1.0)) * gamma) * ratio;
+        mcplx y5 = rr * gamma2 + ((2.0 * (ll - 1.0)) * xi) / rr - ((2.0 * (zt + 1.0)) * gamma) * ratio;
         y[4][i] = (cmu * c.zeta) * y5;
         y[5][i] = -(rrho * (c.zeta2 + llp1 * zt));
         sign = -sign;
@@ -875,7 +921,7 @@ __device__ inline void sph_minor_solid_start(const Ctx& c, int is, double rr, cd
     }
 }
 
-__device__ __forceinline__ void minors_of_2col(const cd y[4][2], cd* m)
+__device__ __forceinline__ void minors_of_2col(const mcplx y[4][2], mcplx* m)
 {
     m[0] = det2(y[0][0], y[1][0], y[0][1], y[1][1]);
     m[1] = det2(y[0][0], y[2][0], y[0][1], y[2][1]);
@@ -888,21 +934,21 @@ __device__ __forceinline__ void minors_of_2col(const cd y[4][2], cd* m)
 __device__ __forceinline__ int imul32(int a, int b) { return (int)((unsigned)a * (unsigned)b); }
 
 // module_int.f90:1275-1341 sph_solid_start_ng + :1489-1506 minors
-__device__ inline void sph_minor_solid_start_ng(const Ctx& c, int is, double rr, cd* m)
+__device__ inline void sph_minor_solid_start_ng(const Ctx& c, int is, double rr, mcplx* m)
 {
     SplPt s = spl_at(c.kn, is, rr);
     const Knot* kn = c.kn;
-    double rrho = spl(kn, s, P_RHO), rmu = spl(kn, s, P_MU), rqmu = spl(kn, s, P_QMU);
-    double rkappa = spl(kn, s, P_KAPPA), rqkappa = spl(kn, s, P_QKAPPA);
-    cd cmu = rmu * (1.0 + rqmu * c.lno);
-    cd ckappa = rkappa * (1.0 + rqkappa * c.lno);
-    cd calpha = (ckappa + 1.3333333333 * cmu) / rrho;
-    cd cbeta = cmu / rrho;
+    mreal rrho = splr(c, s, P_RHO), rmu = splr(c, s, P_MU), rqmu = splr(c, s, P_QMU);
+    mreal rkappa = splr(c, s, P_KAPPA), rqkappa = splr(c, s, P_QKAPPA);
+    mcplx cmu = rmu * (1.0 + rqmu * c.lno);
+    mcplx ckappa = rkappa * (1.0 + rqkappa * c.lno);
+    mcplx calpha = (ckappa + 1.3333333333 * cmu) / rrho;
+    mcplx cbeta = cmu / rrho;
     int l = c.ll, lp1 = c.llp1;
     double ll = (double)l;
-    cd y[4][2];
-    cd arg = (c.omega * rr) / csqrt(calpha);
-    cd jl2 = sbessj2(lp1, arg);
+    mcplx y[4][2];
+    mcplx arg = (c.omega * rr) / csqrt(calpha);
+    mcplx jl2 = sbessj2(lp1, arg);
     y[0][0] = ll - arg * jl2;
     y[1][0] = mk(c.zeta);
     y[2][0] = (-((((rrho * calpha) * arg) * arg)) +
@@ -919,24 +965,24 @@ __device__ inline void sph_minor_solid_start_ng(const Ctx& c, int is, double rr,
 }
 
 // module_int.f90:1346-1405 sph_fluid_start + :1509-1534 minors
-__device__ inline void sph_minor_fluid_start(const Ctx& c, int is, double rr, cd* m)
+__device__ inline void sph_minor_fluid_start(const Ctx& c, int is, double rr, mcplx* m)
 {
     SplPt s = spl_at(c.kn, is, rr);
     const Knot* kn = c.kn;
     double pib = c.mh->pibigg;
-    double rrho = spl(kn, s, P_RHO), rkappa = spl(kn, s, P_KAPPA), rqkappa = spl(kn, s, P_QKAPPA);
-    cd ckappa = rkappa * (1.0 + rqkappa * c.lno);
-    cd calpha = ckappa / rrho;
-    double gamg = (4.0 * pib * rrho) / 3.0;
-    cd gamma = ((c.omega2 + 4.0 * gamg) - ((c.zeta2 * gamg) * gamg) * c.omegai2) / calpha;
-    cd gamma2 = gamma;
+    mreal rrho = splr(c, s, P_RHO), rkappa = splr(c, s, P_KAPPA), rqkappa = splr(c, s, P_QKAPPA);
+    mcplx ckappa = rkappa * (1.0 + rqkappa * c.lno);
+    mcplx calpha = ckappa / rrho;
+    mreal gamg = (4.0 * pib * rrho) / 3.0;
+    mcplx gamma = ((c.omega2 + 4.0 * gamg) - ((c.zeta2 * gamg) * gamg) * c.omegai2) / calpha;
+    mcplx gamma2 = gamma;
     gamma = csqrt(gamma);
-    cd zt = -c.omega2 / gamg;
-    cd xi = zt - (double)c.llp1;
-    cd args = (gamma2 * rr) * rr;
-    cd ratio = bfs_dum(c.ll, args);
+    mcplx zt = -c.omega2 / gamg;
+    mcplx xi = zt - (double)c.llp1;
+    mcplx args = (gamma2 * rr) * rr;
+    mcplx ratio = bfs_dum(c.ll, args);
     double ll = (double)c.ll;
-    cd y[4][2];
+    mcplx y[4][2];
     y[0][0] = ll * xi - ((zt * gamma) * rr) * ratio;
     y[1][0] = -(((4.0 * pib * rrho) * rr) * zt);
     y[2][0] = -((((rrho * calpha) * zt) * rr) * gamma2);
@@ -950,15 +996,15 @@ __device__ inline void sph_minor_fluid_start(const Ctx& c, int is, double rr, cd
 }
 
 // module_int.f90:1407-1447 sph_fluid_start_ng (2 components)
-__device__ inline void sph_fluid_start_ng(const Ctx& c, int is, double rr, cd* y)
+__device__ inline void sph_fluid_start_ng(const Ctx& c, int is, double rr, mcplx* y)
 {
     SplPt s = spl_at(c.kn, is, rr);
     const Knot* kn = c.kn;
-    double rrho = spl(kn, s, P_RHO), rkappa = spl(kn, s, P_KAPPA), rqkappa = spl(kn, s, P_QKAPPA);
-    cd ckappa = rkappa * (1.0 + rqkappa * c.lno);
-    cd calpha = ckappa / rrho;
-    cd arg = (c.omega * rr) / csqrt(calpha);
-    cd ratio = sbessj2(c.llp1, arg);
+    mreal rrho = splr(c, s, P_RHO), rkappa = splr(c, s, P_KAPPA), rqkappa = splr(c, s, P_QKAPPA);
+    mcplx ckappa = rkappa * (1.0 + rqkappa * c.lno);
+    mcplx calpha = ckappa / rrho;
+    mcplx arg = (c.omega * rr) / csqrt(calpha);
+    mcplx ratio = sbessj2(c.llp1, arg);
     y[0] = (double)c.ll - arg * ratio;
     y[1] = (-((rrho * calpha) * arg * arg)) / rr;
 }
@@ -970,7 +1016,7 @@ __device__ inline void sph_fluid_start_ng(const Ctx& c, int is, double rr, cd* y
 #define YS(k) s[(k) - 1]
 #define YB(k) b[(k) - 1]
 
-__device__ __forceinline__ void b_solid_start(const cd* m, const cd* s, cd* b)
+__device__ __forceinline__ void b_solid_start(const mcplx* m, const mcplx* s, mcplx* b)
 {
     b[0] = YM(14) * YS(3) - YM(7) * YS(4) - YM(11) * YS(5) - YM(13) * YS(6);
     b[1] = -(YM(14) * YS(2)) - YM(8) * YS(4) - YM(12) * YS(5) + YM(11) * YS(6);
@@ -988,7 +1034,7 @@ __device__ __forceinline__ void b_solid_start(const cd* m, const cd* s, cd* b)
     b[13] = YM(10) * YS(1) - YM(5) * YS(2) + YM(2) * YS(3) - YM(1) * YS(4);
 }
 
-__device__ __forceinline__ void b_solid_start_ngcow(const cd* m, const cd* s, cd* b)
+__device__ __forceinline__ void b_solid_start_ngcow(const mcplx* m, const mcplx* s, mcplx* b)
 {
     b[0] = -(YM(5) * YS(2)) - YM(2) * YS(3) - YM(4) * YS(4);
     b[1] = YM(5) * YS(1) - YM(3) * YS(3) + YM(2) * YS(4);
@@ -996,18 +1042,18 @@ __device__ __forceinline__ void b_solid_start_ngcow(const cd* m, const cd* s, cd
     b[3] = YM(4) * YS(1) - YM(2) * YS(2) + YM(1) * YS(3);
 }
 
-__device__ __forceinline__ void s2f(const cd* m1, cd* m2)
+__device__ __forceinline__ void s2f(const mcplx* m1, mcplx* m2)
 {
     m2[0] = -m1[5]; m2[1] = -m1[6]; m2[2] = m1[8]; m2[3] = -m1[12]; m2[4] = m1[13];
 }
-__device__ __forceinline__ void s2f_ngcow(const cd* m1, cd* m2) { m2[0] = -m1[2]; m2[1] = -m1[4]; }
-__device__ __forceinline__ void f2s(const cd* m1, cd* m2)
+__device__ __forceinline__ void s2f_ngcow(const mcplx* m1, mcplx* m2) { m2[0] = -m1[2]; m2[1] = -m1[4]; }
+__device__ __forceinline__ void f2s(const mcplx* m1, mcplx* m2)
 {
 #pragma unroll
     for (int k = 0; k < 14; k++) m2[k] = mk(0.0);
     m2[0] = m1[0]; m2[1] = m1[1]; m2[3] = m1[2]; m2[9] = -m1[3]; m2[11] = -m1[4];
 }
-__device__ __forceinline__ void f2s_ngcow(const cd* m1, cd* m2)
+__device__ __forceinline__ void f2s_ngcow(const mcplx* m1, mcplx* m2)
 {
 #pragma unroll
     for (int k = 0; k < 5; k++) m2[k] = mk(0.0);
@@ -1015,7 +1061,7 @@ __device__ __forceinline__ void f2s_ngcow(const cd* m1, cd* m2)
     m2[3] = -m1[1];
 }
 
-__device__ __forceinline__ cd delta_solid(const cd* a, const cd* b)
+__device__ __forceinline__ mcplx delta_solid(const mcplx* a, const mcplx* b)
 {
 #define DA(k) a[(k) - 1]
 #define DB(k) b[(k) - 1]
@@ -1024,14 +1070,14 @@ __device__ __forceinline__ cd delta_solid(const cd* a, const cd* b)
            DA(10) * DB(9) + DA(9) * DB(10) - 2.0 * (DA(3) * DB(11)) - DA(6) * DB(12) -
            DA(4) * DB(13) + DA(1) * DB(14);
 }
-__device__ __forceinline__ cd delta_solid_ngcow(const cd* a, const cd* b)
+__device__ __forceinline__ mcplx delta_solid_ngcow(const mcplx* a, const mcplx* b)
 {
     return DA(5) * DB(1) + 2.0 * (DA(2) * DB(2)) + DA(4) * DB(3) + DA(3) * DB(4) + DA(1) * DB(5);
 #undef DA
 #undef DB
 }
 
-__device__ __forceinline__ void sph_ysol(const cd* m, const cd* b, cd* y)
+__device__ __forceinline__ void sph_ysol(const mcplx* m, const mcplx* b, mcplx* y)
 {
     y[0] = YM(3) * YB(3) + YM(1) * YB(6) + YM(2) * YB(7) + 2.0 * (YM(3) * YB(8)) + YM(4) * YB(9) +
            YM(5) * YB(10) + YM(6) * YB(11) + YM(7) * YB(12) + YM(8) * YB(13) + YM(9) * YB(14);
@@ -1048,7 +1094,7 @@ __device__ __forceinline__ void sph_ysol(const cd* m, const cd* b, cd* y)
            YM(14) * YB(12);
 }
 
-__device__ __forceinline__ void sph_ysol_ngcow(const cd* m, const cd* b, cd* y)
+__device__ __forceinline__ void sph_ysol_ngcow(const mcplx* m, const mcplx* b, mcplx* y)
 {
     y[0] = YM(1) * YB(2) + YM(2) * YB(3) + YM(3) * YB(4);
     y[1] = -(YM(1) * YB(1)) + YM(4) * YB(3) - YM(2) * YB(4);

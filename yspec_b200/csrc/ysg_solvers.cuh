@@ -19,12 +19,12 @@ __device__ __forceinline__ double huge_pow(int k)
 }
 
 // module_solver.f90:25-142.  Unit source jumps ss = I (yspec.f90:230-232).
-__device__ inline void tor_solver(Ctx& c, double rr, double rs, int ir, int is, cd yout[2][2])
+__device__ inline void tor_solver(Ctx& c, double rr, double rs, int ir, int is, mcplx yout[2][2])
 {
     const ModelHdr* mh = c.mh;
     const Knot* kn = c.kn;
     int scale1 = 0, scale2 = 0, scale3 = 0;
-    cd y1[2], y2[2], y3[2];
+    mcplx y1[2], y2[2], y3[2];
     const bool up = rr >= rs;
     int it = up ? is : ir;
     int i1 = tor_start_level(c, c.ll, c.omega.x, it);
@@ -32,7 +32,7 @@ __device__ inline void tor_solver(Ctx& c, double rr, double rs, int ir, int is, 
     double rt = kn[i1].r;
     if (i1 == mh->noc + 1) { y1[0] = mk(1.0); y1[1] = mk(0.0); }
     else tor_ystart(c, i1, rt, y1);
-    cd delta;
+    mcplx delta;
     if (up) {
         yint<TorSys>(c, i1, is, rt, rs, y1, &scale1);
         y3[0] = y1[0]; y3[1] = y1[1];
@@ -41,8 +41,8 @@ __device__ inline void tor_solver(Ctx& c, double rr, double rs, int ir, int is, 
         if (rr != kn[mh->nsl].r) yint<TorSys>(c, mh->nsl - 1, ir, kn[mh->nsl].r, rr, y2, &scale2);
         delta = 1.0 / (y2[1] * y3[0] - y2[0] * y3[1]);
         // b = y1(2)*ss(1,i) - y1(1)*ss(2,i); yout(:,i) = -delta*y2*b
-        cd b0 = y1[1], b1 = -y1[0];
-        cd dy0 = delta * y2[0], dy1 = delta * y2[1];
+        mcplx b0 = y1[1], b1 = -y1[0];
+        mcplx dy0 = delta * y2[0], dy1 = delta * y2[1];
         yout[0][0] = -(dy0 * b0); yout[1][0] = -(dy1 * b0);
         yout[0][1] = -(dy0 * b1); yout[1][1] = -(dy1 * b1);
     } else {
@@ -52,8 +52,8 @@ __device__ inline void tor_solver(Ctx& c, double rr, double rs, int ir, int is, 
         y3[0] = y2[0]; y3[1] = y2[1];
         if (rr != rs) yint<TorSys>(c, is, ir, rs, rr, y3, &scale3);
         delta = 1.0 / (y3[1] * y1[0] - y3[0] * y1[1]);
-        cd b0 = y2[1], b1 = -y2[0];
-        cd dy0 = delta * y1[0], dy1 = delta * y1[1];
+        mcplx b0 = y2[1], b1 = -y2[0];
+        mcplx dy0 = delta * y1[0], dy1 = delta * y1[1];
         yout[0][0] = -(dy0 * b0); yout[1][0] = -(dy1 * b0);
         yout[0][1] = -(dy0 * b1); yout[1][1] = -(dy1 * b1);
     }
@@ -65,12 +65,12 @@ __device__ inline void tor_solver(Ctx& c, double rr, double rs, int ir, int is, 
 }
 
 // module_solver.f90:335-441 rad_solver_ng (rad_derivs_ng == gravity matrix)
-__device__ inline void rad_solver_ng(Ctx& c, double rr, double rs, int ir, int is, cd yout[2][2])
+__device__ inline void rad_solver_ng(Ctx& c, double rr, double rs, int ir, int is, mcplx yout[2][2])
 {
     const ModelHdr* mh = c.mh;
     const Knot* kn = c.kn;
     int scale1 = 0, scale2 = 0, scale3 = 0;
-    cd y1[2], y2[2], y3[2], delta;
+    mcplx y1[2], y2[2], y3[2], delta;
     double rt = fmin(0.1 * c.dr, 0.1 * kn[2].r);
     rad_ystart<false>(c, 1, rt, y1);
     const bool up = rr >= rs;
@@ -88,11 +88,11 @@ __device__ inline void rad_solver_ng(Ctx& c, double rr, double rs, int ir, int i
         if (rr != rs) yint<RadSys>(c, is, ir, rs, rr, y3, &scale3);
     }
     delta = y3[1] * y1[0] - y3[0] * y1[1];
-    delta = cabs(delta) < 1.0e-100 ? mk(0.0) : 1.0 / delta;
-    const cd* ya = up ? y1 : y2;   // source-side solution forming b
-    const cd* yb = up ? y2 : y1;   // solution evaluated at the receiver
-    cd b0 = ya[1], b1 = -ya[0];
-    cd dy0 = delta * yb[0], dy1 = delta * yb[1];
+    delta = val(cabs(delta)) < 1.0e-100 ? mcplx(mk(0.0)) : 1.0 / delta;
+    const mcplx* ya = up ? y1 : y2;   // source-side solution forming b
+    const mcplx* yb = up ? y2 : y1;   // solution evaluated at the receiver
+    mcplx b0 = ya[1], b1 = -ya[0];
+    mcplx dy0 = delta * yb[0], dy1 = delta * yb[1];
     yout[0][0] = -(dy0 * b0); yout[1][0] = -(dy1 * b0);
     yout[0][1] = -(dy0 * b1); yout[1][1] = -(dy1 * b1);
     if (up) {
@@ -150,7 +150,7 @@ __device__ __forceinline__ int seg_npts(const GridSeg& s, double drr)
 
 // module_solver.f90:446-561 rad_solver_wg.  The potential pout is not used
 // by the driver (yspec.f90:277-281) and is not formed.
-__device__ inline void rad_solver_wg(Ctx& c, double rr, double rs, cd yout[2][2])
+__device__ inline void rad_solver_wg(Ctx& c, double rr, double rs, mcplx yout[2][2])
 {
     const ModelHdr* mh = c.mh;
     const Knot* kn = c.kn;
@@ -170,7 +170,7 @@ __device__ inline void rad_solver_wg(Ctx& c, double rr, double rs, cd yout[2][2]
         }
     }
     // pass 2: upward from rt through grid points 2..iss
-    cd y1[2], yrec[2] = {mk(0.0), mk(0.0)};
+    mcplx y1[2], yrec[2] = {mk(0.0), mk(0.0)};
     bool have_rec = false;
     {
         int k = 0, iprev = 0;
@@ -204,7 +204,7 @@ __device__ inline void rad_solver_wg(Ctx& c, double rr, double rs, cd yout[2][2]
         }
     }
     // pass 3: downward from grid point ngrid to iss
-    cd y2[2] = {mk(1.0), mk(0.0)};
+    mcplx y2[2] = {mk(1.0), mk(0.0)};
     {
         int k = ngrid + 1, iprev = 0;
         double rprev = 0.0;
@@ -229,11 +229,11 @@ __device__ inline void rad_solver_wg(Ctx& c, double rr, double rs, cd yout[2][2]
         }
     }
     (void)have_rec;
-    cd delta = 1.0 / (y2[1] * y1[0] - y2[0] * y1[1]);
-    cd b0, b1;
+    mcplx delta = 1.0 / (y2[1] * y1[0] - y2[0] * y1[1]);
+    mcplx b0, b1;
     if (irr <= iss) { b0 = y2[1]; b1 = -y2[0]; }
     else { b0 = y1[1]; b1 = -y1[0]; }
-    cd dy0 = delta * yrec[0], dy1 = delta * yrec[1];
+    mcplx dy0 = delta * yrec[0], dy1 = delta * yrec[1];
     yout[0][0] = -(dy0 * b0); yout[1][0] = -(dy1 * b0);
     yout[0][1] = -(dy0 * b1); yout[1][1] = -(dy1 * b1);
 }
@@ -241,13 +241,13 @@ __device__ inline void rad_solver_wg(Ctx& c, double rr, double rs, cd yout[2][2]
 // Spheroidal solve with self-gravitation: sph_solver (:640-823) and
 // sph_solver_fic (:1203-1382).  yout[6][4] holds the responses to unit
 // jumps in components 1, 2, 4, 5 (yspec.f90:234-238).
-__device__ inline void sph_solver_g(Ctx& c, double rr, double rs, int ir, int is, cd yout[6][4])
+__device__ inline void sph_solver_g(Ctx& c, double rr, double rs, int ir, int is, mcplx yout[6][4])
 {
     const ModelHdr* mh = c.mh;
     const Knot* kn = c.kn;
     const bool fic = mh->fic != 0;
     int scale1 = 0, scale2 = 0, scale3 = 0;
-    cd ms1[14], ms2[14], ms3[14], mf[5];
+    mcplx ms1[14], ms2[14], ms3[14], mf[5];
     const bool up = rr >= rs;
     const int it = up ? is : ir;
     const double rtop = up ? rs : rr;
@@ -285,7 +285,7 @@ __device__ inline void sph_solver_g(Ctx& c, double rr, double rs, int ir, int is
     const int ibot = up ? ir : is;
     const double rbot = up ? rr : rs;
     if (mh->ocean) {
-        cd mf2[5] = {mk(1.0), mk(0.0), mk(0.0), mk(0.0), mk(0.0)};
+        mcplx mf2[5] = {mk(1.0), mk(0.0), mk(0.0), mk(0.0), mk(0.0)};
         yint<MinorFluidG>(c, mh->nknot - 1, mh->nsl + 1, kn[mh->nknot].r, kn[mh->nsl + 1].r, mf2, &scale2);
         f2s(mf2, ms2);
         yint<MinorSolidG>(c, mh->nsl, ibot, kn[mh->nsl].r, rbot, ms2, &scale2);
@@ -295,15 +295,15 @@ __device__ inline void sph_solver_g(Ctx& c, double rr, double rs, int ir, int is
         ms2[0] = mk(1.0);
         yint<MinorSolidG>(c, up ? mh->nknot - 1 : mh->nknot, ibot, kn[mh->nknot].r, rbot, ms2, &scale2);
     }
-    cd delta = delta_solid(ms3, ms2);
+    mcplx delta = delta_solid(ms3, ms2);
     const int jump[4] = {0, 1, 3, 4};
     // the four jumps integrate the same span at the same omega: in the
     // count-only build one pass counts for four
     for (int i = 0; i < (YSG_COUNT_ONLY ? 1 : 4); i++) {
-        cd s[6] = {mk(0.0), mk(0.0), mk(0.0), mk(0.0), mk(0.0), mk(0.0)};
+        mcplx s[6] = {mk(0.0), mk(0.0), mk(0.0), mk(0.0), mk(0.0), mk(0.0)};
         s[jump[i]] = mk(1.0);
         int scale4 = 0;
-        cd b[14], ys[6];
+        mcplx b[14], ys[6];
         if (up) {
             b_solid_start(ms1, s, b);
             yint<BvecSolidG>(c, is, ir, rs, rr, b, &scale4);
@@ -325,13 +325,13 @@ __device__ inline void sph_solver_g(Ctx& c, double rr, double rs, int ir, int is
 // sph_solver_cow (:1014-1195), sph_solver_ng_fic (:1386-1562),
 // sph_solver_cow_fic (:1568-1740).  yout[4][4], ss = I (yspec.f90:240-243).
 template <int KIND>
-__device__ inline void sph_solver_nc(Ctx& c, double rr, double rs, int ir, int is, cd yout[4][4])
+__device__ inline void sph_solver_nc(Ctx& c, double rr, double rs, int ir, int is, mcplx yout[4][4])
 {
     const ModelHdr* mh = c.mh;
     const Knot* kn = c.kn;
     const bool fic = mh->fic != 0;
     int scale1 = 0, scale2 = 0, scale3 = 0;
-    cd ms1[5], ms2[5], ms3[5], mf[2];
+    mcplx ms1[5], ms2[5], ms3[5], mf[2];
     const bool up = rr >= rs;
     const int it = up ? is : ir;
     const double rtop = up ? rs : rr;
@@ -367,7 +367,7 @@ __device__ inline void sph_solver_nc(Ctx& c, double rr, double rs, int ir, int i
     const int ibot = up ? ir : is;
     const double rbot = up ? rr : rs;
     if (mh->ocean) {
-        cd mf2[2] = {mk(1.0), mk(0.0)};
+        mcplx mf2[2] = {mk(1.0), mk(0.0)};
         yint<MinorFluidNC<KIND>>(c, mh->nknot - 1, mh->nsl + 1, kn[mh->nknot].r, kn[mh->nsl + 1].r, mf2, &scale2);
         f2s_ngcow(mf2, ms2);
         yint<MinorSolidNC<KIND>>(c, mh->nsl, ibot, kn[mh->nsl].r, rbot, ms2, &scale2);
@@ -377,12 +377,12 @@ __device__ inline void sph_solver_nc(Ctx& c, double rr, double rs, int ir, int i
         ms2[0] = mk(1.0);
         yint<MinorSolidNC<KIND>>(c, mh->nknot, ibot, kn[mh->nknot].r, rbot, ms2, &scale2);
     }
-    cd delta = delta_solid_ngcow(ms3, ms2);
+    mcplx delta = delta_solid_ngcow(ms3, ms2);
     for (int i = 0; i < (YSG_COUNT_ONLY ? 1 : 4); i++) {     // see sph_solver_g
-        cd s[4] = {mk(0.0), mk(0.0), mk(0.0), mk(0.0)};
+        mcplx s[4] = {mk(0.0), mk(0.0), mk(0.0), mk(0.0)};
         s[i] = mk(1.0);
         int scale4 = 0;
-        cd b[4], ys[4];
+        mcplx b[4], ys[4];
         if (up) {
             b_solid_start_ngcow(ms1, s, b);
             yint<BvecSolidNC<KIND>>(c, is, ir, rs, rr, b, &scale4);
@@ -405,11 +405,11 @@ __device__ inline void sph_solver_nc(Ctx& c, double rr, double rs, int ir, int i
 // ---------------------------------------------------------------------------
 // module_solver.f90:145-215 (svt(:,1) and svt(:,2))
 __device__ inline void source_vector_tor(const Ctx& c, int is, double rs, const double* mm,
-                                         cd svt[5][2])
+                                         mcplx svt[5][2])
 {
     SplPt s = spl_at(c.kn, is, rs);
-    double rlcon = spl(c.kn, s, P_LCON), rqmu = spl(c.kn, s, P_QMU);
-    cd clcon = rlcon * (1.0 + rqmu * c.lno);
+    mreal rlcon = splr(c, s, P_LCON), rqmu = splr(c, s, P_QMU);
+    mcplx clcon = rlcon * (1.0 + rqmu * c.lno);
     for (int i = 0; i < 5; i++) svt[i][0] = svt[i][1] = mk(0.0);
     if (c.ll >= 1) {
         svt[1][0] = ((0.5 * rs) * mk(-mm[2], mm[1])) / clcon;
@@ -427,13 +427,13 @@ __device__ inline void source_vector_tor(const Ctx& c, int is, double rs, const 
 }
 
 // module_solver.f90:566-627
-__device__ inline void source_vector_rad(const Ctx& c, int is, double rs, const double* mm, cd s0[2])
+__device__ inline void source_vector_rad(const Ctx& c, int is, double rs, const double* mm, mcplx s0[2])
 {
     SplPt s = spl_at(c.kn, is, rs);
-    double rccon = spl(c.kn, s, P_CCON), rfcon = spl(c.kn, s, P_FCON);
-    double rxa2 = spl(c.kn, s, P_XA2), rxlam = spl(c.kn, s, P_XLAM);
-    cd cccon = 1.0 / (rccon * (1.0 + rxa2 * c.lno));
-    cd cfcon = rfcon * (1.0 + rxlam * c.lno);
+    mreal rccon = splr(c, s, P_CCON), rfcon = splr(c, s, P_FCON);
+    mreal rxa2 = splr(c, s, P_XA2), rxlam = splr(c, s, P_XLAM);
+    mcplx cccon = 1.0 / (rccon * (1.0 + rxa2 * c.lno));
+    mcplx cfcon = rfcon * (1.0 + rxlam * c.lno);
     s0[0] = (rs * mm[0]) * cccon;
     s0[1] = (-mm[3] - mm[5]) + ((2.0 * mm[0]) * cfcon) * cccon;
     cd den = (imul(c.omega) * rs) * rs;
@@ -444,17 +444,17 @@ __device__ inline void source_vector_rad(const Ctx& c, int is, double rs, const 
 // module_solver.f90:1747-1847.  qaa, qff and qll are declared real(dp)
 // there (:1771-1772), so only Re(1 + q*lno) enters the spheroidal source.
 __device__ inline void source_vector_sph(const Ctx& c, int is, double rs, const double* mm,
-                                         cd svs[5][6])
+                                         mcplx svs[5][6])
 {
     SplPt s = spl_at(c.kn, is, rs);
     const Knot* kn = c.kn;
-    double rlcon = spl(kn, s, P_LCON), rccon = spl(kn, s, P_CCON), rfcon = spl(kn, s, P_FCON);
-    double rqmu = spl(kn, s, P_QMU), rxlam = spl(kn, s, P_XLAM), rxa2 = spl(kn, s, P_XA2);
-    double qaa = 1.0 + rxa2 * c.lno.x;
-    double qff = 1.0 + rxlam * c.lno.x;
-    double qll = 1.0 + rqmu * c.lno.x;
-    double cccon = 1.0 / (rccon * qaa);
-    double cfcon = rfcon * qff, clcon = rlcon * qll;
+    mreal rlcon = splr(c, s, P_LCON), rccon = splr(c, s, P_CCON), rfcon = splr(c, s, P_FCON);
+    mreal rqmu = splr(c, s, P_QMU), rxlam = splr(c, s, P_XLAM), rxa2 = splr(c, s, P_XA2);
+    mreal qaa = 1.0 + rxa2 * c.lno.x;
+    mreal qff = 1.0 + rxlam * c.lno.x;
+    mreal qll = 1.0 + rqmu * c.lno.x;
+    mreal cccon = 1.0 / (rccon * qaa);
+    mreal cfcon = rfcon * qff, clcon = rlcon * qll;
     for (int i = 0; i < 5; i++)
         for (int j = 0; j < 6; j++) svs[i][j] = mk(0.0);
     double z = c.zeta;
@@ -473,6 +473,18 @@ __device__ inline void source_vector_sph(const Ctx& c, int is, double rs, const 
 // ---------------------------------------------------------------------------
 // One (omega_j, l) pair: yspec.f90:259-400.  coef = uu(1:5), vv(1:5), ww(1:5).
 // ---------------------------------------------------------------------------
+// grav(ir), the knot value the potential / tilt correction uses
+// (yspec.f90:388-391)
+__device__ __forceinline__ mreal grav_at_receiver(const Ctx& c, const EventDev& ev)
+{
+#if YSG_TANGENT
+    return mreal(ev.grav_ir, c.dkn[ev.ir].v[P_GRAV][0]);
+#else
+    (void)c;
+    return ev.grav_ir;
+#endif
+}
+
 __device__ __forceinline__ cd omega_of(const EventDev& ev, int j)
 {
     // w = wmin + (j-1)*dw - i*ep, formed without contraction (yspec.f90:261)
@@ -487,29 +499,29 @@ __device__ __forceinline__ cd out_factor(int out, cd w)
 }
 
 // l == 0: radial mode, yspec.f90:263-293
-__device__ inline void pair_radial(Ctx& c, const EventDev& ev, int j, cd* coef)
+__device__ inline void pair_radial(Ctx& c, const EventDev& ev, int j, mcplx* coef)
 {
     cd w = omega_of(ev, j);
     set_l(c, 0);
     set_omega(c, w);
-    cd sr0[2], yrad[2][2];
+    mcplx sr0[2], yrad[2][2];
     source_vector_rad(c, ev.is, ev.rs, ev.mm, sr0);
     alpha_steps(c);
     if (ev.grav == 0) rad_solver_ng(c, ev.rr, ev.rs, ev.ir, ev.is, yrad);
     else rad_solver_wg(c, ev.rr, ev.rs, yrad);
-    cd u3 = (sr0[0] * yrad[0][0] + sr0[1] * yrad[0][1]) / ev.rr;
+    mcplx u3 = (sr0[0] * yrad[0][0] + sr0[1] * yrad[0][1]) / ev.rr;
     if (ev.out != 0) u3 = out_factor(ev.out, w) * u3;
     for (int q = 0; q < NCOEF; q++) coef[q] = mk(0.0);
     coef[2] = u3;
 }
 
 // l >= 2: toroidal part, yspec.f90:301-316 -> ww(1:5)
-__device__ inline void pair_toroidal(Ctx& c, const EventDev& ev, int l, int j, cd* ww)
+__device__ inline void pair_toroidal(Ctx& c, const EventDev& ev, int l, int j, mcplx* ww)
 {
     cd w = omega_of(ev, j);
     set_l(c, l);
     set_omega(c, w);
-    cd svt[5][2], ytor[2][2];
+    mcplx svt[5][2], ytor[2][2];
     source_vector_tor(c, ev.is, ev.rs, ev.mm, svt);
     tor_solver(c, ev.rr, ev.rs, ev.ir, ev.is, ytor);
     if (ev.out != 0) {
@@ -523,18 +535,18 @@ __device__ inline void pair_toroidal(Ctx& c, const EventDev& ev, int l, int j, c
 }
 
 // l >= 1: spheroidal part, yspec.f90:344-400 -> uu(1:5), vv(1:5)
-__device__ inline void pair_spheroidal(Ctx& c, const EventDev& ev, int l, int j, cd* uu, cd* vv)
+__device__ inline void pair_spheroidal(Ctx& c, const EventDev& ev, int l, int j, mcplx* uu, mcplx* vv)
 {
     cd w = omega_of(ev, j);
     set_l(c, l);
     set_omega(c, w);
     alpha_steps(c);
-    cd svs[5][6], ysph[6][4];
+    mcplx svs[5][6], ysph[6][4];
     source_vector_sph(c, ev.is, ev.rs, ev.mm, svs);
     if (ev.grav == 2) {
         sph_solver_g(c, ev.rr, ev.rs, ev.ir, ev.is, ysph);
     } else {
-        cd yng[4][4];
+        mcplx yng[4][4];
         if (ev.grav == 1) sph_solver_nc<1>(c, ev.rr, ev.rs, ev.ir, ev.is, yng);
         else sph_solver_nc<0>(c, ev.rr, ev.rs, ev.ir, ev.is, yng);
         for (int b = 0; b < 4; b++) {                  // yspec.f90:367-374
@@ -554,10 +566,10 @@ __device__ inline void pair_spheroidal(Ctx& c, const EventDev& ev, int l, int j,
             for (int b = 0; b < 4; b++)
                 for (int a = 0; a < 3; a++) ysph[a][b] = mw2 * ysph[a][b];
         } else {                                       // yspec.f90:388-391
-            double gr = ev.grav_ir;
+            mreal gr = grav_at_receiver(c, ev);
             for (int b = 0; b < 4; b++) {
-                cd c1 = (-((double)(l + 1) * ysph[2][b] + (2.0 * gr) * ysph[0][b])) / ev.rr;
-                cd c2 = (zeta * (ysph[2][b] + gr * ysph[0][b])) / ev.rr;
+                mcplx c1 = (-((double)(l + 1) * ysph[2][b] + (2.0 * gr) * ysph[0][b])) / ev.rr;
+                mcplx c2 = (zeta * (ysph[2][b] + gr * ysph[0][b])) / ev.rr;
                 ysph[0][b] = mw2 * ysph[0][b] + c1;
                 ysph[1][b] = mw2 * ysph[1][b] + c2;
             }
