@@ -104,6 +104,12 @@ int ysg_model_upload(ysg_handle *h, const ysg_model *m);
  * derivatives.  A new ysg_model_upload discards it. */
 int ysg_model_tangent_upload(ysg_handle *h, const ysg_model *dm);
 
+/* ndir directions at once (dms[0..ndir-1], each as above).  With solver 2,
+ * slot s of ysg_batch_run takes direction s, so a batch of ndir copies of
+ * one event returns the derivatives of its traces along every direction
+ * in one solve launch; a single direction serves every slot. */
+int ysg_model_tangents_upload(ysg_handle *h, int ndir, const ysg_model *dms);
+
 /* Spectra of one event: yspec.f90:250-426.  ur, ut, up are complex
  * (nw, nr) column-major host arrays (interleaved re/im), or NULL to keep
  * the spectra on the device only.  Also leaves the spectra on the device

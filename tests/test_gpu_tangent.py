@@ -95,6 +95,20 @@ def test_tangent_is_linear_in_the_direction(engine, workdir):
     assert not zero.any()
 
 
+def test_directions_in_one_batch_equal_single_runs(engine, workdir):
+    """Slot s of a tangent batch takes direction s: the batched derivatives
+    equal one-direction runs."""
+    p = small(ats=1, out=2, cor=1)
+    pf = p.write(workdir / "many.in")
+    km = KnotModel(p.model_file)
+    ev = Event(km.host, Params(pf))
+    dirs = [_direction(km, 20 + k) for k in range(5)]
+    many = adjoint.tangent_traces_many(engine, ev, km, dirs)
+    for k, d in enumerate(dirs):
+        one = adjoint.tangent_traces(engine, ev, km, d)
+        assert np.linalg.norm(many[k] - one) <= 1e-12 * np.linalg.norm(one), k
+
+
 def test_tangent_needs_a_direction(engine, workdir):
     p = small()
     pf = p.write(workdir / "nodir.in")

@@ -133,6 +133,22 @@ def tangent_traces(engine: Engine, event, knot_model, direction, at=None) -> np.
         engine.set_solver("batched")
 
 
+def tangent_traces_many(engine: Engine, event, knot_model, directions, at=None) -> np.ndarray:
+    """Derivatives of the event's Z, N, E traces along several directions,
+    (len(directions), nr, 3, nout): one batch of copies of the event, slot s
+    on direction s, one tangent solve launch for all of them."""
+    km = knot_model
+    p = at if at is not None else km.params()
+    engine.set_solver("tangent")
+    try:
+        engine.upload(km.array_model(*p))
+        engine.upload_tangents([km.tangent(d, at=p) for d in directions])
+        outs = engine.batch_run([event] * len(directions))
+        return np.stack([o[:, 1:4, :] for o in outs])
+    finally:
+        engine.set_solver("batched")
+
+
 def _model_function():
     import torch
 
@@ -169,12 +185,14 @@ class ModelSynthetics:
 
     Forward: the six unit-moment responses of the model at (rho, vp, vs), one
     batched launch, combined with mm.  Backward: mm exactly as
-    MomentTensorSynthetics; each knot parameter by one tangent-linear run
-    along it (3 nknot runs, or those of `knots` only: the others get zero).
+    MomentTensorSynthetics; each knot parameter by a tangent-linear solve
+    along it (3 nknot directions, or those of `knots` only: the others get
+    zero), `chunk` directions per batched launch.
     """
 
-    def __init__(self, engine: Engine, event: Event, knot_model, knots=None):
+    def __init__(self, engine: Engine, event: Event, knot_model, knots=None, chunk: int = 64):
         self.engine, self.event, self.km = engine, event, knot_model
+        self.chunk = chunk
         self.moment_norm = norms()["moment_norm"]
         n = knot_model.nknot
         self.columns = (list(range(3 * n)) if knots is None else
@@ -210,10 +228,14 @@ class ModelSynthetics:
             eng.upload(km.array_model(*p))
             from .model_chain import ArrayModel
 
-            for col in self.columns:
-                d = {k: v[:, col] for k, v in jac.items()}
-                eng.upload_tangent(ArrayModel(km.view0, km.r.numpy(), d, z, z))
-                out[col] = float(np.sum(g * eng.run(ev)[:, 1:4, :]))
+            # `chunk` directions per batch: slot s of the batch on direction s
+            for c0 in range(0, len(self.columns), self.chunk):
+                cols = self.columns[c0:c0 + self.chunk]
+                dms = [ArrayModel(km.view0, km.r.numpy(), {k: v[:, col] for k, v in jac.items()}, z, z)
+                       for col in cols]
+                eng.upload_tangents(dms)
+                for col, o in zip(cols, eng.batch_run([ev] * len(cols))):
+                    out[col] = float(np.sum(g * o[:, 1:4, :]))
         finally:
             eng.set_solver("batched")
         return torch.from_numpy(out)

@@ -170,6 +170,12 @@ class Engine:
         v = dmodel.view()
         N.check(N.lib().ysg_model_tangent_upload(self.h, C.byref(v)), "model_tangent_upload")
 
+    def upload_tangents(self, dmodels) -> None:
+        """Several directions: with solver "tangent", slot s of batch_run takes
+        direction s."""
+        views = (N.YsgModel * len(dmodels))(*[d.view() for d in dmodels])
+        N.check(N.lib().ysg_model_tangents_upload(self.h, len(dmodels), views), "model_tangents_upload")
+
     def spectra(self, event: Event, copy: bool = True):
         nw, nr = event.nw, event.nr
         if not copy:

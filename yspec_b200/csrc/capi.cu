@@ -101,8 +101,8 @@ struct ysg_handle {
     std::vector<double> grav_host;   // knot gravity for the tilt correction
     std::vector<double> r_host;      // knot radii of the uploaded model
     bool has_model = false;
-    DevBuf dkn, dsg;                 // model derivative for the tangent solver
-    bool has_tangent = false;
+    DevBuf dkn, dsg;                 // model derivatives (directions) for the tangent solver
+    int ndir = 0;                    // directions loaded; 0 = none
     // events
     std::vector<Slot> slots;
     int nactive = 0;                 // slots of the last prepare / batch
@@ -293,6 +293,25 @@ int upload_items(ysg_handle* h, std::vector<Item>& items, const std::vector<Even
     return YSG_OK;
 }
 
+// Event records and coefficient pointers of slots 0..nev-1 on the device,
+// for the tangent solver's one launch over all slots.
+int upload_slot_tables(ysg_handle* h, int nev)
+{
+    std::vector<EventDev> evs((size_t)nev);
+    std::vector<cd*> coefs((size_t)nev);
+    for (int e = 0; e < nev; e++) {
+        evs[(size_t)e] = h->slots[(size_t)e].pev;
+        coefs[(size_t)e] = h->slots[(size_t)e].coef.as<cd>();
+    }
+    CK(h->evdev.ensure(evs.size() * sizeof(EventDev)));
+    CK(h->coefptr.ensure(coefs.size() * sizeof(cd*)));
+    CK(cudaMemcpyAsync(h->evdev.p, evs.data(), evs.size() * sizeof(EventDev), cudaMemcpyHostToDevice, h->st));
+    CK(cudaMemcpyAsync(h->coefptr.p, coefs.data(), coefs.size() * sizeof(cd*), cudaMemcpyHostToDevice, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    h->h2d += (double)(evs.size() * sizeof(EventDev) + coefs.size() * sizeof(cd*));
+    return YSG_OK;
+}
+
 // Work items of the batched solver for slots 0..nev-1, longest first.
 int upload_batch_items(ysg_handle* h, int nev)
 {
@@ -429,14 +448,17 @@ int enqueue_solve(ysg_handle* h, int nev)
                                   h->work.as<unsigned long long>(), h->status.as<int>(), h->st));
         }
     } else if (h->solver == 2) {
-        if (!h->has_tangent) return YSG_ERR_ARG;
+        // slot s takes direction s, or the one direction loaded
+        if (h->ndir == 0 || (h->ndir != 1 && h->ndir != nev)) return YSG_ERR_ARG;
+        long long maxp = 0;
         for (int e = 0; e < nev; e++) {
-            const Slot& s = h->slots[(size_t)e];
-            h->launches += 1;
-            CK(launch_solve_tangent(h->kn.as<Knot>(), h->sg.as<Seg>(), h->dkn.as<Knot>(), h->dsg.as<Seg>(),
-                                    h->hdr_dev.as<ModelHdr>(), s.pev, s.coef.as<cd>(), nullptr,
-                                    h->work.as<unsigned long long>(), h->st));
+            const EventDev& d = h->slots[(size_t)e].pev;
+            maxp = std::max<long long>(maxp, (long long)(d.lmax - d.lmin + 1) * d.nw);
         }
+        h->launches += 1;
+        CK(launch_solve_tangent(h->kn.as<Knot>(), h->sg.as<Seg>(), h->dkn.as<Knot>(), h->dsg.as<Seg>(),
+                                h->ndir, h->hdr_dev.as<ModelHdr>(), h->evdev.as<EventDev>(),
+                                h->coefptr.as<cd*>(), nev, maxp, h->work.as<unsigned long long>(), h->st));
     } else {
         const int s = h->cur_sched;
         const unsigned long long* pairs = nullptr;
@@ -710,6 +732,7 @@ int prepare_single(ysg_handle* h, const ysg_event* ev)
         if (!rc) rc = resolve_schedule(h, 1);
         return rc;
     }
+    if (h->solver == 2) return upload_slot_tables(h, 1);
     return YSG_OK;
 }
 
@@ -946,34 +969,49 @@ int ysg_model_upload(ysg_handle* h, const ysg_model* m)
     h->grav_host.assign(m->val[P_GRAV], m->val[P_GRAV] + n);
     h->r_host.assign(m->r, m->r + n);
     h->has_model = true;
-    h->has_tangent = false;
+    h->ndir = 0;
     h->has_spectra = false;
     for (Slot& s : h->slots) s.ev_ready = s.tm_ready = false;
     return YSG_OK;
 }
 
-int ysg_model_tangent_upload(ysg_handle* h, const ysg_model* dm)
+int ysg_model_tangents_upload(ysg_handle* h, int ndir, const ysg_model* dms)
 {
-    if (!h || !dm) return YSG_ERR_ARG;
+    if (!h || !dms || ndir < 1 || ndir > 65535) return YSG_ERR_ARG;
     if (!h->has_model) return YSG_ERR_NO_MODEL;
-    const int n = dm->nknot;
-    if (n != h->hdr.nknot) return YSG_ERR_ARG;
-    for (int p = 0; p < NPARAM; p++)
-        if (!dm->val[p] || !dm->cs[p]) return YSG_ERR_ARG;
-    std::vector<Knot> rec;
-    std::vector<Seg> seg;
-    build_tables(n, h->r_host.data(), dm->val, dm->cs, nullptr, nullptr, rec, seg);
-    // the tables hold derivatives, except the radii the segments are based on
-    for (size_t i = 0; i < seg.size(); i++) seg[i].r0 = 0.0;
+    const int n = h->hdr.nknot;
+    for (int d = 0; d < ndir; d++) {
+        if (dms[d].nknot != n) return YSG_ERR_ARG;
+        for (int p = 0; p < NPARAM; p++)
+            if (!dms[d].val[p] || !dms[d].cs[p]) return YSG_ERR_ARG;
+    }
+    const size_t nk = (size_t)n + 2, ns = (size_t)n + 1;
+    std::vector<Knot> rec_all(nk * ndir);
+    std::vector<Seg> seg_all(ns * ndir);
+    for (int d = 0; d < ndir; d++) {
+        std::vector<Knot> rec;
+        std::vector<Seg> seg;
+        build_tables(n, h->r_host.data(), dms[d].val, dms[d].cs, nullptr, nullptr, rec, seg);
+        // the tables hold derivatives, except the radii the segments are based on
+        for (size_t i = 0; i < seg.size(); i++) seg[i].r0 = 0.0;
+        std::copy(rec.begin(), rec.end(), rec_all.begin() + (ptrdiff_t)(nk * d));
+        std::copy(seg.begin(), seg.end(), seg_all.begin() + (ptrdiff_t)(ns * d));
+    }
     cudaSetDevice(h->device);
-    CK(h->dkn.ensure(rec.size() * sizeof(Knot)));
-    CK(cudaMemcpyAsync(h->dkn.p, rec.data(), rec.size() * sizeof(Knot), cudaMemcpyHostToDevice, h->st));
-    CK(h->dsg.ensure(seg.size() * sizeof(Seg)));
-    CK(cudaMemcpyAsync(h->dsg.p, seg.data(), seg.size() * sizeof(Seg), cudaMemcpyHostToDevice, h->st));
+    h->ndir = 0;
+    CK(h->dkn.ensure(rec_all.size() * sizeof(Knot)));
+    CK(cudaMemcpyAsync(h->dkn.p, rec_all.data(), rec_all.size() * sizeof(Knot), cudaMemcpyHostToDevice, h->st));
+    CK(h->dsg.ensure(seg_all.size() * sizeof(Seg)));
+    CK(cudaMemcpyAsync(h->dsg.p, seg_all.data(), seg_all.size() * sizeof(Seg), cudaMemcpyHostToDevice, h->st));
     CK(cudaStreamSynchronize(h->st));
-    h->has_tangent = true;
+    h->ndir = ndir;
     h->has_spectra = false;
     return YSG_OK;
+}
+
+int ysg_model_tangent_upload(ysg_handle* h, const ysg_model* dm)
+{
+    return ysg_model_tangents_upload(h, 1, dm);
 }
 
 int ysg_trace_rows(const ysg_time* tm)
@@ -1158,6 +1196,9 @@ int ysg_batch_run(ysg_handle* h, int nev, const ysg_event* evs, const ysg_time* 
     if (h->solver == 1) {
         int rc = upload_batch_items(h, nev);
         if (!rc) rc = resolve_schedule(h, nev);
+        if (rc) return rc;
+    } else if (h->solver == 2) {
+        int rc = upload_slot_tables(h, nev);
         if (rc) return rc;
     }
     h->nactive = nev;

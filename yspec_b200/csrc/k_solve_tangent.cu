@@ -10,11 +10,13 @@
 // The l-sum, the filter, the inverse FFT and the post-processing that follow
 // are linear in the coefficients, so running them on the derivative
 // coefficients gives the derivative of the traces.  The kernel writes the
-// derivative coefficients in the layout of the primal ones (and, on request,
-// the values into a second buffer).
+// derivative coefficients in the layout of the primal ones.
 //
-// One thread per (omega_j, l) pair, one event per launch, the stage vectors
-// in local memory: the dual solve needs twice the state of the primal one.
+// One thread per (omega_j, l) pair, the stage vectors in local memory (the
+// dual solve needs twice the state of the primal one).  One launch serves
+// every slot of a batch: blockIdx.y is the slot, and slot s takes model
+// direction s (or direction 0 when a single direction is loaded), so many
+// directions of one event run as one batch of copies of it.
 #define YSG_TANGENT 1
 #include "ysg_kernels.h"
 #include "ysg_solvers.cuh"
@@ -24,11 +26,17 @@ namespace ysg {
 __global__ void __launch_bounds__(128) k_solve_tangent(const Knot* __restrict__ kn,
                                                        const Seg* __restrict__ sg,
                                                        const Knot* __restrict__ dkn,
-                                                       const Seg* __restrict__ dsg,
-                                                       const ModelHdr* __restrict__ mh, EventDev ev,
-                                                       cd* __restrict__ dcoef, cd* __restrict__ vcoef,
+                                                       const Seg* __restrict__ dsg, int ndir,
+                                                       const ModelHdr* __restrict__ mh,
+                                                       const EventDev* __restrict__ evs,
+                                                       cd* const* __restrict__ coefs,
                                                        unsigned long long* __restrict__ work)
 {
+    const int slot = blockIdx.y;
+    const int dir = ndir == 1 ? 0 : slot;
+    const EventDev& ev = evs[slot];
+    cd* const dcoef = coefs[slot];
+    const int nknot = mh->nknot;
     const int L = ev.lmax - ev.lmin + 1;
     const long long total = (long long)L * ev.nw;
     const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -39,8 +47,8 @@ __global__ void __launch_bounds__(128) k_solve_tangent(const Knot* __restrict__ 
     c.ats = (double)ev.ats;
     c.sg = sg;
     c.kb = nullptr;
-    c.dkn = dkn;
-    c.dsg = dsg;
+    c.dkn = dkn + (size_t)dir * (nknot + 2);     // knot records 0..nknot+1
+    c.dsg = dsg + (size_t)dir * (nknot + 1);     // segment records 0..nknot
     for (int q = 0; q < NSYS; q++) c.nst[q] = 0;
     if (gid < total) {
         const int li = (int)(gid / ev.nw);
@@ -57,8 +65,6 @@ __global__ void __launch_bounds__(128) k_solve_tangent(const Knot* __restrict__ 
         }
         const size_t o = (size_t)li * NCOEF * ev.nw + (j - 1);
         for (int q = 0; q < NCOEF; q++) dcoef[o + (size_t)q * ev.nw] = out[q].d;
-        if (vcoef)
-            for (int q = 0; q < NCOEF; q++) vcoef[o + (size_t)q * ev.nw] = out[q].v;
     }
     for (int q = 0; q < NSYS; q++) {
         unsigned long long v = c.nst[q];
@@ -68,15 +74,17 @@ __global__ void __launch_bounds__(128) k_solve_tangent(const Knot* __restrict__ 
 }
 
 cudaError_t launch_solve_tangent(const Knot* kn, const Seg* sg, const Knot* dkn, const Seg* dsg,
-                                 const ModelHdr* mh, const EventDev& ev, cd* dcoef, cd* vcoef,
+                                 int ndir, const ModelHdr* mh, const EventDev* evs_dev,
+                                 cd* const* coefs_dev, int nslot, long long max_pairs,
                                  unsigned long long* work, cudaStream_t st)
 {
-    const long long total = (long long)(ev.lmax - ev.lmin + 1) * ev.nw;
-    if (total <= 0) return cudaSuccess;
+    if (max_pairs <= 0 || nslot <= 0) return cudaSuccess;
+    if (nslot > 65535) return cudaErrorInvalidConfiguration;
     const int bs = 128;
-    const long long nb = (total + bs - 1) / bs;
+    const long long nb = (max_pairs + bs - 1) / bs;
     if (nb > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
-    k_solve_tangent<<<(unsigned)nb, bs, 0, st>>>(kn, sg, dkn, dsg, mh, ev, dcoef, vcoef, work);
+    k_solve_tangent<<<dim3((unsigned)nb, (unsigned)nslot), bs, 0, st>>>(kn, sg, dkn, dsg, ndir, mh, evs_dev,
+                                                                       coefs_dev, work);
     return cudaGetLastError();
 }
 

@@ -13,10 +13,14 @@ size_t solve_plain_smem(int nknot);
 cudaError_t launch_solve_plain(const Knot* kn, const Seg* sg, const ModelHdr& mh, const EventDev& ev,
                                cd* coef, unsigned long long* work, int* status, cudaStream_t st);
 
-// K1 tangent-linear: the plain layout with dual numbers; writes the
-// derivative coefficients to dcoef and, when vcoef is not null, the values.
+// K1 tangent-linear: one thread per pair with dual numbers, one launch over
+// slots 0..nslot-1 (their EventDev records and coefficient buffers in
+// device arrays); slot s takes direction s of the ndir derivative tables
+// (nknot + 2 knot records and nknot + 1 segments each), or direction 0 when
+// ndir is 1, and receives the derivative coefficients.
 cudaError_t launch_solve_tangent(const Knot* kn, const Seg* sg, const Knot* dkn, const Seg* dsg,
-                                 const ModelHdr* mh, const EventDev& ev, cd* dcoef, cd* vcoef,
+                                 int ndir, const ModelHdr* mh, const EventDev* evs_dev,
+                                 cd* const* coefs_dev, int nslot, long long max_pairs,
                                  unsigned long long* work, cudaStream_t st);
 
 // K1 batched persistent: work items (event, l index, first frequency - 1)

@@ -72,7 +72,7 @@ class YshNorms(C.Structure):
 
 # Symbols declared in include/*.h, checked by the CPU test suite.
 EXPORTS = [
-    "ysg_create", "ysg_model_upload", "ysg_model_tangent_upload", "ysg_event_spectra", "ysg_event_spectra_device",
+    "ysg_create", "ysg_model_upload", "ysg_model_tangent_upload", "ysg_model_tangents_upload", "ysg_event_spectra", "ysg_event_spectra_device",
     "ysg_event_traces", "ysg_trace_rows",
     "ysg_event_run", "ysg_event_prepare", "ysg_event_execute", "ysg_event_fetch", "ysg_get_stream",
     "ysg_batch_run", "ysg_event_coef", "ysg_legendre_table", "ysg_set_solver", "ysg_set_schedule", "ysg_last_schedule",
@@ -107,6 +107,7 @@ def lib() -> C.CDLL:
     L.ysg_create.argtypes = [C.POINTER(vp), C.c_int]
     L.ysg_model_upload.argtypes = [vp, C.POINTER(YsgModel)]
     L.ysg_model_tangent_upload.argtypes = [vp, C.POINTER(YsgModel)]
+    L.ysg_model_tangents_upload.argtypes = [vp, C.c_int, C.POINTER(YsgModel)]
     L.ysg_event_spectra.argtypes = [vp, C.POINTER(YsgEvent), _dp, _dp, _dp]
     L.ysg_event_spectra_device.argtypes = [vp, C.POINTER(YsgEvent), vp, vp, vp]
     L.ysg_event_traces.argtypes = [vp, C.POINTER(YsgTime), _dp, C.POINTER(C.c_int)]
