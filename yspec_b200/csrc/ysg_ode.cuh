@@ -613,6 +613,62 @@ __device__ __forceinline__ void rkck_step_loop(const Ctx& c, cd* y, double x, do
     for (int i = 0; i < N; i++) y[i] = y[i] + h * a1[i * KS];
 }
 
+// The looped step with the four slots in a per-thread array (local
+// memory) instead of the shared slab, for the tangent build: its dual stage
+// vectors are twice the size, and six inlined dual right-hand sides would
+// overflow the instruction cache just as the unrolled primal step does.
+template <class T>
+struct LocalOut {
+    T* p;
+    double w;
+    bool add;
+    struct Ref {
+        T* a;
+        double w;
+        bool add;
+        __device__ __forceinline__ void operator=(T v) const
+        {
+            if (add) *a += w * v;
+            else *a = v;
+        }
+    };
+    __device__ __forceinline__ Ref operator[](int i) const { return Ref{p + i, w, add}; }
+};
+
+template <class Sys>
+__device__ __forceinline__ void rkck_step_loop_local(const Ctx& c, mcplx* y, double x, double h)
+{
+    constexpr int N = Sys::N;
+    mcplx kb[4 * N];
+    mcplx yt[N];
+#pragma unroll 1
+    for (int s = 0; s < 6; s++) {
+#pragma unroll
+        for (int i = 0; i < N; i++) yt[i] = y[i];
+#pragma unroll 1
+        for (int t = 0; t < 4; t++) {
+            const double wt = ck_in[s][t];
+            if (wt == 0.0) continue;
+            const double hb = h * wt;
+            const mcplx* kt = kb + t * N;
+#pragma unroll
+            for (int i = 0; i < N; i++) yt[i] += hb * kt[i];
+        }
+        if (s >= 4) {
+            const double f0 = ck_fold[s][0], f1 = ck_fold[s][1], f2 = ck_fold[s][2],
+                         f3 = ck_fold[s][3];
+            mcplx* const a1 = kb + N;
+#pragma unroll 1
+            for (int i = 0; i < N; i++)
+                a1[i] = f0 * kb[i] + f1 * a1[i] + f2 * kb[2 * N + i] + f3 * kb[3 * N + i];
+        }
+        Sys::f(c, x + ck_a[s] * h, yt, LocalOut<mcplx>{kb + ck_slot[s] * N, ck_w[s], s >= 4});
+    }
+    const mcplx* a1 = kb + N;
+#pragma unroll
+    for (int i = 0; i < N; i++) y[i] = y[i] + h * a1[i];
+}
+
 // yint's rescaling (module_int.f90:1910-1919, 1952-1961).  |y| is compared through
 // |y|^2 against the squared bounds (1e-40, 1e40, both normal doubles): the
 // decision can differ from the reference only within rounding of a bound,
@@ -639,7 +695,7 @@ __device__ __forceinline__ void rescale(mcplx* y, int* scale)
 }
 
 // module_int.f90:1847-1968 yint
-#if YSG_SMEM_STAGES
+#if YSG_SMEM_STAGES || YSG_TANGENT
 #define YSG_YINT_ATTR __noinline__
 #else
 #define YSG_YINT_ATTR
@@ -685,6 +741,8 @@ __device__ YSG_YINT_ATTR void yint(Ctx& cio, int i1, int i2, double r1, double r
             double rr = __dadd_rn(rr1, __dmul_rn((double)(j - 1), drr));
 #if YSG_SMEM_STAGES
             rkck_step_loop<Sys>(c, y, rr, drr);
+#elif YSG_TANGENT
+            rkck_step_loop_local<Sys>(c, y, rr, drr);
 #else
             rkck_step<Sys>(c, y, rr, drr);
 #endif
