@@ -124,13 +124,14 @@ def tangent_traces(engine: Engine, event, knot_model, direction, at=None) -> np.
     deck's), with the deck's start levels and step counts."""
     km = knot_model
     p = at if at is not None else km.params()
+    prev = engine.solver
     engine.set_solver("tangent")
     try:
         engine.upload(km.array_model(*p))
         engine.upload_tangent(km.tangent(direction, at=p))
         return engine.run(event)[:, 1:4, :]
     finally:
-        engine.set_solver("batched")
+        engine.set_solver(prev)
 
 
 def tangent_traces_many(engine: Engine, event, knot_model, directions, at=None) -> np.ndarray:
@@ -139,6 +140,7 @@ def tangent_traces_many(engine: Engine, event, knot_model, directions, at=None) 
     on direction s, one tangent solve launch for all of them."""
     km = knot_model
     p = at if at is not None else km.params()
+    prev = engine.solver
     engine.set_solver("tangent")
     try:
         engine.upload(km.array_model(*p))
@@ -146,7 +148,7 @@ def tangent_traces_many(engine: Engine, event, knot_model, directions, at=None) 
         outs = engine.batch_run([event] * len(directions))
         return np.stack([o[:, 1:4, :] for o in outs])
     finally:
-        engine.set_solver("batched")
+        engine.set_solver(prev)
 
 
 def _model_function():
@@ -206,9 +208,13 @@ class ModelSynthetics:
         import torch
 
         eng = self.engine
+        prev = eng.solver
         eng.set_solver("batched")
-        eng.upload(self.km.array_model(rho.detach(), vp.detach(), vs.detach()))
-        _, G = greens(eng, self.event)
+        try:
+            eng.upload(self.km.array_model(rho.detach(), vp.detach(), vs.detach()))
+            _, G = greens(eng, self.event)
+        finally:
+            eng.set_solver(prev)
         return torch.from_numpy(G)
 
     def _knot_gradient(self, rho, vp, vs, mm, grad):
@@ -223,6 +229,7 @@ class ModelSynthetics:
         ev = with_moment(self.event, [float(x) for x in mm.detach()])
         g = np.asarray(grad.detach().cpu().numpy(), dtype=np.float64)
         out = np.zeros(3 * n)
+        prev = eng.solver
         eng.set_solver("tangent")
         try:
             eng.upload(km.array_model(*p))
@@ -237,5 +244,5 @@ class ModelSynthetics:
                 for col, o in zip(cols, eng.batch_run([ev] * len(cols))):
                     out[col] = float(np.sum(g * o[:, 1:4, :]))
         finally:
-            eng.set_solver("batched")
+            eng.set_solver(prev)
         return torch.from_numpy(out)

@@ -130,6 +130,7 @@ class Engine:
     def __init__(self, device: int = 0, solver: str = "batched"):
         self.h = C.c_void_p()
         N.check(N.lib().ysg_create(C.byref(self.h), device), "ysg_create")
+        self.solver = solver
         self.set_solver(solver)
 
     def __del__(self):
@@ -145,6 +146,7 @@ class Engine:
         model direction given to upload_tangent)."""
         N.check(N.lib().ysg_set_solver(self.h, {"plain": 0, "batched": 1, "tangent": 2}[which]),
                 "set_solver")
+        self.solver = which
 
     def set_schedule(self, sched: int) -> None:
         """Batched-solver schedule: 0 tiles, 1 cost-sorted pair lists, 2 the same lists
