@@ -220,11 +220,20 @@ class Engine:
         N.check(N.lib().ysg_get_stream(self.h, C.byref(s)), "stream")
         return s.value or 0
 
-    def batch_run(self, events: list[Event]) -> list[np.ndarray]:
+    def batch_run(self, events: list[Event], outs: list[np.ndarray] | None = None) -> list[np.ndarray]:
+        """Run several events as one batch.  `outs` are caller-owned (nr, 4, nout)
+        float64 arrays, one per event; the same array may serve several events
+        (each overwrites it in turn), for batches whose traces exceed host memory."""
         nev = len(events)
         evs = (N.YsgEvent * nev)(*[e.raw.ev for e in events])
         tms = (N.YsgTime * nev)(*[e.raw.tm for e in events])
-        outs = [np.zeros((e.nr, 4, e.nout())) for e in events]
+        if outs is None:
+            outs = [np.zeros((e.nr, 4, e.nout())) for e in events]
+        if len(outs) != nev:
+            raise ValueError("one output array per event")
+        for e, o in zip(events, outs):
+            if o.shape != (e.nr, 4, e.nout()) or o.dtype != np.float64 or not o.flags.c_contiguous:
+                raise ValueError("output array must be C-contiguous float64 (nr, 4, nout)")
         ptrs = (N._dp * nev)(*[N.dptr(o) for o in outs])
         nouts = (C.c_int * nev)()
         N.check(N.lib().ysg_batch_run(self.h, nev, evs, tms, ptrs, nouts), "batch_run")
