@@ -293,25 +293,6 @@ int upload_items(ysg_handle* h, std::vector<Item>& items, const std::vector<Even
     return YSG_OK;
 }
 
-// Event records and coefficient pointers of slots 0..nev-1 on the device,
-// for the tangent solver's one launch over all slots.
-int upload_slot_tables(ysg_handle* h, int nev)
-{
-    std::vector<EventDev> evs((size_t)nev);
-    std::vector<cd*> coefs((size_t)nev);
-    for (int e = 0; e < nev; e++) {
-        evs[(size_t)e] = h->slots[(size_t)e].pev;
-        coefs[(size_t)e] = h->slots[(size_t)e].coef.as<cd>();
-    }
-    CK(h->evdev.ensure(evs.size() * sizeof(EventDev)));
-    CK(h->coefptr.ensure(coefs.size() * sizeof(cd*)));
-    CK(cudaMemcpyAsync(h->evdev.p, evs.data(), evs.size() * sizeof(EventDev), cudaMemcpyHostToDevice, h->st));
-    CK(cudaMemcpyAsync(h->coefptr.p, coefs.data(), coefs.size() * sizeof(cd*), cudaMemcpyHostToDevice, h->st));
-    CK(cudaStreamSynchronize(h->st));
-    h->h2d += (double)(evs.size() * sizeof(EventDev) + coefs.size() * sizeof(cd*));
-    return YSG_OK;
-}
-
 // Work items of the batched solver for slots 0..nev-1, longest first.
 int upload_batch_items(ysg_handle* h, int nev)
 {
@@ -451,14 +432,32 @@ int enqueue_solve(ysg_handle* h, int nev)
         // slot s takes direction s, or the one direction loaded
         if (h->ndir == 0 || (h->ndir != 1 && h->ndir != nev)) return YSG_ERR_ARG;
         long long maxp = 0;
+        bool packable = nev <= 65535;
         for (int e = 0; e < nev; e++) {
             const EventDev& d = h->slots[(size_t)e].pev;
             maxp = std::max<long long>(maxp, (long long)(d.lmax - d.lmin + 1) * d.nw);
+            packable = packable && d.lmax - d.lmin + 1 < (1 << 23) && d.nw < (1 << 24);
+        }
+        const unsigned long long* sorted = nullptr;
+        if (packable && h->nev_items == nev) {
+            // the batched solver's cost-sorted entry list of the same slots
+            StepCost sc;
+            for (int q = 0; q < NSYS_COUNT; q++) sc.flops[q] = kStepFlops[q];
+            sc.base = kPairBaseFlops;
+            unsigned long long* keys[2] = {h->keys0.as<unsigned long long>(), h->keys1.as<unsigned long long>()};
+            unsigned long long* vals[2] = {h->vals0.as<unsigned long long>(), h->vals1.as<unsigned long long>()};
+            unsigned long long* out = nullptr;
+            h->launches += 1;        // k_pair_cost (the radix sort is CUB's)
+            CK(launch_pair_schedule(h->kn.as<Knot>(), h->sg.as<Seg>(), h->hdr_dev.as<ModelHdr>(),
+                                    h->evdev.as<EventDev>(), h->offs.as<long long>(), nev, h->npairs, sc,
+                                    keys, vals, h->sort_tmp.p, h->sort_tmp.cap, &out, h->st));
+            sorted = out;
         }
         h->launches += 1;
         CK(launch_solve_tangent(h->kn.as<Knot>(), h->sg.as<Seg>(), h->dkn.as<Knot>(), h->dsg.as<Seg>(),
                                 h->ndir, h->hdr_dev.as<ModelHdr>(), h->evdev.as<EventDev>(),
-                                h->coefptr.as<cd*>(), nev, maxp, h->work.as<unsigned long long>(), h->st));
+                                h->coefptr.as<cd*>(), nev, maxp, sorted, sorted ? 2 * h->npairs : 0,
+                                h->work.as<unsigned long long>(), h->st));
     } else {
         const int s = h->cur_sched;
         const unsigned long long* pairs = nullptr;
@@ -732,7 +731,7 @@ int prepare_single(ysg_handle* h, const ysg_event* ev)
         if (!rc) rc = resolve_schedule(h, 1);
         return rc;
     }
-    if (h->solver == 2) return upload_slot_tables(h, 1);
+    if (h->solver == 2) return upload_batch_items(h, 1);
     return YSG_OK;
 }
 
@@ -1198,7 +1197,7 @@ int ysg_batch_run(ysg_handle* h, int nev, const ysg_event* evs, const ysg_time* 
         if (!rc) rc = resolve_schedule(h, nev);
         if (rc) return rc;
     } else if (h->solver == 2) {
-        int rc = upload_slot_tables(h, nev);
+        int rc = upload_batch_items(h, nev);
         if (rc) return rc;
     }
     h->nactive = nev;

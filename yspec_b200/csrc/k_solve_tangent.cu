@@ -12,11 +12,16 @@
 // coefficients gives the derivative of the traces.  The kernel writes the
 // derivative coefficients in the layout of the primal ones.
 //
-// One thread per (omega_j, l) pair, the stage vectors in local memory (the
-// dual solve needs twice the state of the primal one).  One launch serves
-// every slot of a batch: blockIdx.y is the slot, and slot s takes model
-// direction s (or direction 0 when a single direction is loaded), so many
-// directions of one event run as one batch of copies of it.
+// The stage vectors live in local memory (the dual solve needs twice the
+// state of the primal one).  One launch serves every slot of a batch, and
+// slot s takes model direction s (or direction 0 when a single direction is
+// loaded), so many directions of one event run as one batch of copies of it.
+// Two layouts: with `pairs`, one thread per entry of the cost-sorted list
+// of the batched solver (k_schedule.cu: the spheroidal and the toroidal part
+// of every pair of every slot, costliest first, equal paths side by side;
+// the cost of a solve is that of its value part, so the primal order serves
+// the tangent solve); without it, one thread per pair, l-major, blockIdx.y
+// the slot.
 #define YSG_TANGENT 1
 #include "ysg_kernels.h"
 #include "ysg_solvers.cuh"
@@ -30,16 +35,32 @@ __global__ void __launch_bounds__(128) k_solve_tangent(const Knot* __restrict__ 
                                                        const ModelHdr* __restrict__ mh,
                                                        const EventDev* __restrict__ evs,
                                                        cd* const* __restrict__ coefs,
+                                                       const unsigned long long* __restrict__ pairs,
+                                                       long long nentries,
                                                        unsigned long long* __restrict__ work)
 {
-    const int slot = blockIdx.y;
+    const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    int slot, li, j, part = 2;                // part: 0 spheroidal, 1 toroidal, 2 both
+    bool active;
+    if (pairs) {
+        const unsigned long long v = gid < nentries ? pairs[gid] : ~0ull;
+        active = v != ~0ull;                  // l < 2 has no toroidal entry
+        slot = active ? (int)(v >> 48) : 0;
+        part = (int)((v >> 47) & 1u);
+        li = (int)((v >> 24) & 0x7fffffu);
+        j = (int)(v & 0xffffffu) + 1;
+    } else {
+        slot = blockIdx.y;
+        const EventDev& e0 = evs[slot];
+        const long long total = (long long)(e0.lmax - e0.lmin + 1) * e0.nw;
+        active = gid < total;
+        li = active ? (int)(gid / e0.nw) : 0;
+        j = active ? (int)(gid - (long long)li * e0.nw) + 1 : 1;
+    }
     const int dir = ndir == 1 ? 0 : slot;
     const EventDev& ev = evs[slot];
     cd* const dcoef = coefs[slot];
     const int nknot = mh->nknot;
-    const int L = ev.lmax - ev.lmin + 1;
-    const long long total = (long long)L * ev.nw;
-    const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     Ctx c;
     c.kn = kn;
     c.mh = mh;
@@ -50,21 +71,24 @@ __global__ void __launch_bounds__(128) k_solve_tangent(const Knot* __restrict__ 
     c.dkn = dkn + (size_t)dir * (nknot + 2);     // knot records 0..nknot+1
     c.dsg = dsg + (size_t)dir * (nknot + 1);     // segment records 0..nknot
     for (int q = 0; q < NSYS; q++) c.nst[q] = 0;
-    if (gid < total) {
-        const int li = (int)(gid / ev.nw);
-        const int j = (int)(gid - (long long)li * ev.nw) + 1;
+    if (active) {
         const int l = ev.lmin + li;
         mcplx out[NCOEF];
-        if (l == 0) {
+        int q0 = 0, q1 = NCOEF;               // coefficients this thread writes
+        if (part == 1) {
+            pair_toroidal(c, ev, l, j, out + 10);
+            q0 = 10;
+        } else if (l == 0) {
             pair_radial(c, ev, j, out);
         } else {
-            if (l > 1) pair_toroidal(c, ev, l, j, out + 10);
+            if (part == 2 && l > 1) pair_toroidal(c, ev, l, j, out + 10);
             else
                 for (int q = 10; q < 15; q++) out[q] = mk(0.0);
             pair_spheroidal(c, ev, l, j, out, out + 5);
+            if (part == 0 && l > 1) q1 = 10;
         }
         const size_t o = (size_t)li * NCOEF * ev.nw + (j - 1);
-        for (int q = 0; q < NCOEF; q++) dcoef[o + (size_t)q * ev.nw] = out[q].d;
+        for (int q = q0; q < q1; q++) dcoef[o + (size_t)q * ev.nw] = out[q].d;
     }
     for (int q = 0; q < NSYS; q++) {
         unsigned long long v = c.nst[q];
@@ -76,15 +100,24 @@ __global__ void __launch_bounds__(128) k_solve_tangent(const Knot* __restrict__ 
 cudaError_t launch_solve_tangent(const Knot* kn, const Seg* sg, const Knot* dkn, const Seg* dsg,
                                  int ndir, const ModelHdr* mh, const EventDev* evs_dev,
                                  cd* const* coefs_dev, int nslot, long long max_pairs,
+                                 const unsigned long long* pairs, long long nentries,
                                  unsigned long long* work, cudaStream_t st)
 {
+    const int bs = 128;
+    if (pairs) {
+        if (nentries <= 0) return cudaSuccess;
+        const long long nb = (nentries + bs - 1) / bs;
+        if (nb > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
+        k_solve_tangent<<<(unsigned)nb, bs, 0, st>>>(kn, sg, dkn, dsg, ndir, mh, evs_dev, coefs_dev, pairs,
+                                                     nentries, work);
+        return cudaGetLastError();
+    }
     if (max_pairs <= 0 || nslot <= 0) return cudaSuccess;
     if (nslot > 65535) return cudaErrorInvalidConfiguration;
-    const int bs = 128;
     const long long nb = (max_pairs + bs - 1) / bs;
     if (nb > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
     k_solve_tangent<<<dim3((unsigned)nb, (unsigned)nslot), bs, 0, st>>>(kn, sg, dkn, dsg, ndir, mh, evs_dev,
-                                                                       coefs_dev, work);
+                                                                       coefs_dev, nullptr, 0, work);
     return cudaGetLastError();
 }
 

@@ -13,14 +13,17 @@ size_t solve_plain_smem(int nknot);
 cudaError_t launch_solve_plain(const Knot* kn, const Seg* sg, const ModelHdr& mh, const EventDev& ev,
                                cd* coef, unsigned long long* work, int* status, cudaStream_t st);
 
-// K1 tangent-linear: one thread per pair with dual numbers, one launch over
-// slots 0..nslot-1 (their EventDev records and coefficient buffers in
-// device arrays); slot s takes direction s of the ndir derivative tables
-// (nknot + 2 knot records and nknot + 1 segments each), or direction 0 when
-// ndir is 1, and receives the derivative coefficients.
+// K1 tangent-linear: dual numbers, one launch over slots 0..nslot-1 (their
+// EventDev records and coefficient buffers in device arrays); slot s takes
+// direction s of the ndir derivative tables (nknot + 2 knot records and
+// nknot + 1 segments each), or direction 0 when ndir is 1, and receives the
+// derivative coefficients.  With `pairs` (the nentries sorted entries of
+// launch_pair_schedule over the same slots) one thread per entry; without,
+// one thread per pair of each slot (max_pairs per slot).
 cudaError_t launch_solve_tangent(const Knot* kn, const Seg* sg, const Knot* dkn, const Seg* dsg,
                                  int ndir, const ModelHdr* mh, const EventDev* evs_dev,
                                  cd* const* coefs_dev, int nslot, long long max_pairs,
+                                 const unsigned long long* pairs, long long nentries,
                                  unsigned long long* work, cudaStream_t st);
 
 // K1 batched persistent: work items (event, l index, first frequency - 1)
