@@ -107,7 +107,10 @@ int ysg_model_tangent_upload(ysg_handle *h, const ysg_model *dm);
 /* ndir directions at once (dms[0..ndir-1], each as above).  With solver 2,
  * slot s of ysg_batch_run takes direction s, so a batch of ndir copies of
  * one event returns the derivatives of its traces along every direction
- * in one solve launch; a single direction serves every slot. */
+ * in one solve launch; a single direction serves every slot.  The tangent
+ * solve runs the batched solver's cost-sorted entry list: batches of more
+ * than 65535 slots, or events of 2^23 degrees or 2^24 frequencies, return
+ * YSG_ERR_LIMIT. */
 int ysg_model_tangents_upload(ysg_handle *h, int ndir, const ysg_model *dms);
 
 /* Spectra of one event: yspec.f90:250-426.  ur, ut, up are complex

@@ -431,32 +431,27 @@ int enqueue_solve(ysg_handle* h, int nev)
     } else if (h->solver == 2) {
         // slot s takes direction s, or the one direction loaded
         if (h->ndir == 0 || (h->ndir != 1 && h->ndir != nev)) return YSG_ERR_ARG;
-        long long maxp = 0;
-        bool packable = nev <= 65535;
-        for (int e = 0; e < nev; e++) {
+        // the batched solver's cost-sorted entry list of the same slots
+        // (its packing: slot < 2^16, l index < 2^23, frequency < 2^24)
+        bool packable = nev <= 65535 && h->nev_items == nev;
+        for (int e = 0; e < nev && packable; e++) {
             const EventDev& d = h->slots[(size_t)e].pev;
-            maxp = std::max<long long>(maxp, (long long)(d.lmax - d.lmin + 1) * d.nw);
-            packable = packable && d.lmax - d.lmin + 1 < (1 << 23) && d.nw < (1 << 24);
+            packable = d.lmax - d.lmin + 1 < (1 << 23) && d.nw < (1 << 24);
         }
-        const unsigned long long* sorted = nullptr;
-        if (packable && h->nev_items == nev) {
-            // the batched solver's cost-sorted entry list of the same slots
-            StepCost sc;
-            for (int q = 0; q < NSYS_COUNT; q++) sc.flops[q] = kStepFlops[q];
-            sc.base = kPairBaseFlops;
-            unsigned long long* keys[2] = {h->keys0.as<unsigned long long>(), h->keys1.as<unsigned long long>()};
-            unsigned long long* vals[2] = {h->vals0.as<unsigned long long>(), h->vals1.as<unsigned long long>()};
-            unsigned long long* out = nullptr;
-            h->launches += 1;        // k_pair_cost (the radix sort is CUB's)
-            CK(launch_pair_schedule(h->kn.as<Knot>(), h->sg.as<Seg>(), h->hdr_dev.as<ModelHdr>(),
-                                    h->evdev.as<EventDev>(), h->offs.as<long long>(), nev, h->npairs, sc,
-                                    keys, vals, h->sort_tmp.p, h->sort_tmp.cap, &out, h->st));
-            sorted = out;
-        }
-        h->launches += 1;
+        if (!packable) return YSG_ERR_LIMIT;
+        StepCost sc;
+        for (int q = 0; q < NSYS_COUNT; q++) sc.flops[q] = kStepFlops[q];
+        sc.base = kPairBaseFlops;
+        unsigned long long* keys[2] = {h->keys0.as<unsigned long long>(), h->keys1.as<unsigned long long>()};
+        unsigned long long* vals[2] = {h->vals0.as<unsigned long long>(), h->vals1.as<unsigned long long>()};
+        unsigned long long* sorted = nullptr;
+        h->launches += 2;            // k_pair_cost and the tangent solve (the radix sort is CUB's)
+        CK(launch_pair_schedule(h->kn.as<Knot>(), h->sg.as<Seg>(), h->hdr_dev.as<ModelHdr>(),
+                                h->evdev.as<EventDev>(), h->offs.as<long long>(), nev, h->npairs, sc, keys,
+                                vals, h->sort_tmp.p, h->sort_tmp.cap, &sorted, h->st));
         CK(launch_solve_tangent(h->kn.as<Knot>(), h->sg.as<Seg>(), h->dkn.as<Knot>(), h->dsg.as<Seg>(),
                                 h->ndir, h->hdr_dev.as<ModelHdr>(), h->evdev.as<EventDev>(),
-                                h->coefptr.as<cd*>(), nev, maxp, sorted, sorted ? 2 * h->npairs : 0,
+                                h->coefptr.as<cd*>(), sorted, 2 * h->npairs,
                                 h->work.as<unsigned long long>(), h->st));
     } else {
         const int s = h->cur_sched;

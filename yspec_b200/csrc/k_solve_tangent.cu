@@ -16,12 +16,11 @@
 // state of the primal one).  One launch serves every slot of a batch, and
 // slot s takes model direction s (or direction 0 when a single direction is
 // loaded), so many directions of one event run as one batch of copies of it.
-// Two layouts: with `pairs`, one thread per entry of the cost-sorted list
-// of the batched solver (k_schedule.cu: the spheroidal and the toroidal part
-// of every pair of every slot, costliest first, equal paths side by side;
-// the cost of a solve is that of its value part, so the primal order serves
-// the tangent solve); without it, one thread per pair, l-major, blockIdx.y
-// the slot.
+// One thread per entry of the cost-sorted list of the batched solver
+// (k_schedule.cu: the spheroidal and the toroidal part of every pair of
+// every slot, costliest first, equal paths side by side).  The cost of a
+// solve is that of its value part, so the primal order serves the tangent
+// solve.
 #define YSG_TANGENT 1
 #include "ysg_kernels.h"
 #include "ysg_solvers.cuh"
@@ -40,23 +39,12 @@ __global__ void __launch_bounds__(128) k_solve_tangent(const Knot* __restrict__ 
                                                        unsigned long long* __restrict__ work)
 {
     const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    int slot, li, j, part = 2;                // part: 0 spheroidal, 1 toroidal, 2 both
-    bool active;
-    if (pairs) {
-        const unsigned long long v = gid < nentries ? pairs[gid] : ~0ull;
-        active = v != ~0ull;                  // l < 2 has no toroidal entry
-        slot = active ? (int)(v >> 48) : 0;
-        part = (int)((v >> 47) & 1u);
-        li = (int)((v >> 24) & 0x7fffffu);
-        j = (int)(v & 0xffffffu) + 1;
-    } else {
-        slot = blockIdx.y;
-        const EventDev& e0 = evs[slot];
-        const long long total = (long long)(e0.lmax - e0.lmin + 1) * e0.nw;
-        active = gid < total;
-        li = active ? (int)(gid / e0.nw) : 0;
-        j = active ? (int)(gid - (long long)li * e0.nw) + 1 : 1;
-    }
+    const unsigned long long v = gid < nentries ? pairs[gid] : ~0ull;
+    const bool active = v != ~0ull;           // l < 2 has no toroidal entry
+    const int slot = active ? (int)(v >> 48) : 0;
+    const int part = (int)((v >> 47) & 1u);   // 0 spheroidal / radial, 1 toroidal
+    const int li = (int)((v >> 24) & 0x7fffffu);
+    const int j = (int)(v & 0xffffffu) + 1;
     const int dir = ndir == 1 ? 0 : slot;
     const EventDev& ev = evs[slot];
     cd* const dcoef = coefs[slot];
@@ -81,11 +69,9 @@ __global__ void __launch_bounds__(128) k_solve_tangent(const Knot* __restrict__ 
         } else if (l == 0) {
             pair_radial(c, ev, j, out);
         } else {
-            if (part == 2 && l > 1) pair_toroidal(c, ev, l, j, out + 10);
-            else
-                for (int q = 10; q < 15; q++) out[q] = mk(0.0);
+            for (int q = 10; q < 15; q++) out[q] = mk(0.0);
             pair_spheroidal(c, ev, l, j, out, out + 5);
-            if (part == 0 && l > 1) q1 = 10;
+            if (l > 1) q1 = 10;               // ww comes from the toroidal entry
         }
         const size_t o = (size_t)li * NCOEF * ev.nw + (j - 1);
         for (int q = q0; q < q1; q++) dcoef[o + (size_t)q * ev.nw] = out[q].d;
@@ -99,25 +85,15 @@ __global__ void __launch_bounds__(128) k_solve_tangent(const Knot* __restrict__ 
 
 cudaError_t launch_solve_tangent(const Knot* kn, const Seg* sg, const Knot* dkn, const Seg* dsg,
                                  int ndir, const ModelHdr* mh, const EventDev* evs_dev,
-                                 cd* const* coefs_dev, int nslot, long long max_pairs,
-                                 const unsigned long long* pairs, long long nentries,
-                                 unsigned long long* work, cudaStream_t st)
+                                 cd* const* coefs_dev, const unsigned long long* pairs,
+                                 long long nentries, unsigned long long* work, cudaStream_t st)
 {
     const int bs = 128;
-    if (pairs) {
-        if (nentries <= 0) return cudaSuccess;
-        const long long nb = (nentries + bs - 1) / bs;
-        if (nb > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
-        k_solve_tangent<<<(unsigned)nb, bs, 0, st>>>(kn, sg, dkn, dsg, ndir, mh, evs_dev, coefs_dev, pairs,
-                                                     nentries, work);
-        return cudaGetLastError();
-    }
-    if (max_pairs <= 0 || nslot <= 0) return cudaSuccess;
-    if (nslot > 65535) return cudaErrorInvalidConfiguration;
-    const long long nb = (max_pairs + bs - 1) / bs;
+    if (nentries <= 0) return cudaSuccess;
+    const long long nb = (nentries + bs - 1) / bs;
     if (nb > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
-    k_solve_tangent<<<dim3((unsigned)nb, (unsigned)nslot), bs, 0, st>>>(kn, sg, dkn, dsg, ndir, mh, evs_dev,
-                                                                       coefs_dev, nullptr, 0, work);
+    k_solve_tangent<<<(unsigned)nb, bs, 0, st>>>(kn, sg, dkn, dsg, ndir, mh, evs_dev, coefs_dev, pairs,
+                                                 nentries, work);
     return cudaGetLastError();
 }
 

@@ -17,14 +17,12 @@ cudaError_t launch_solve_plain(const Knot* kn, const Seg* sg, const ModelHdr& mh
 // EventDev records and coefficient buffers in device arrays); slot s takes
 // direction s of the ndir derivative tables (nknot + 2 knot records and
 // nknot + 1 segments each), or direction 0 when ndir is 1, and receives the
-// derivative coefficients.  With `pairs` (the nentries sorted entries of
-// launch_pair_schedule over the same slots) one thread per entry; without,
-// one thread per pair of each slot (max_pairs per slot).
+// derivative coefficients.  One thread per entry of `pairs`, the nentries
+// sorted entries of launch_pair_schedule over the same slots.
 cudaError_t launch_solve_tangent(const Knot* kn, const Seg* sg, const Knot* dkn, const Seg* dsg,
                                  int ndir, const ModelHdr* mh, const EventDev* evs_dev,
-                                 cd* const* coefs_dev, int nslot, long long max_pairs,
-                                 const unsigned long long* pairs, long long nentries,
-                                 unsigned long long* work, cudaStream_t st);
+                                 cd* const* coefs_dev, const unsigned long long* pairs,
+                                 long long nentries, unsigned long long* work, cudaStream_t st);
 
 // K1 batched persistent: work items (event, l index, first frequency - 1)
 // of one or more events, one thread per (omega,l) pair, stage vectors in
