@@ -25,7 +25,6 @@ at the base model, which is the setting the tangent solver differentiates.
 """
 from __future__ import annotations
 
-import ctypes as C
 import os
 
 import numpy as np
