@@ -109,6 +109,29 @@ def test_directions_in_one_batch_equal_single_runs(engine, workdir):
         assert np.linalg.norm(many[k] - one) <= 1e-12 * np.linalg.norm(one), k
 
 
+def test_direction_count_must_match_the_batch(engine, workdir):
+    """Loaded directions must be one (shared by every slot) or one per slot;
+    any other count is rejected before anything runs, and the engine keeps
+    working afterwards."""
+    p = small()
+    pf = p.write(workdir / "count.in")
+    km = KnotModel(p.model_file)
+    ev = Event(km.host, Params(pf))
+    dirs = [_direction(km, 30 + k) for k in range(3)]
+    engine.set_solver("tangent")
+    try:
+        engine.upload(km.array_model())
+        engine.upload_tangents([km.tangent(d) for d in dirs])
+        with pytest.raises(Exception):
+            engine.batch_run([ev, ev])
+        engine.upload_tangents([km.tangent(d) for d in dirs[:2]])
+        two = engine.batch_run([ev, ev])
+    finally:
+        engine.set_solver("batched")
+    one = adjoint.tangent_traces(engine, ev, km, dirs[1])
+    assert np.linalg.norm(two[1][:, 1:4, :] - one) <= 1e-12 * np.linalg.norm(one)
+
+
 def test_tangent_needs_a_direction(engine, workdir):
     p = small()
     pf = p.write(workdir / "nodir.in")
