@@ -319,14 +319,41 @@ __device__ __forceinline__ FluidCoef fluid_amat(const Ctx& c, double rr)
 // ---------------------------------------------------------------------------
 // Right-hand sides.  Each system is a tag type with N components and f().
 // ---------------------------------------------------------------------------
+// Complex multiply-accumulate s + x y (cmac) and s - x y (cmsc) as fused
+// multiply-adds: four for a complex factor, two for a real one, where a
+// product followed by a sum takes six and four.  The 14-component systems
+// accumulate their outputs term by term with them.  Other types (the dual
+// numbers of the tangent build) use the plain operators.
+__device__ __forceinline__ cd cmac(cd s, cd x, cd y)
+{
+    return cd{fma(x.x, y.x, fma(-x.y, y.y, s.x)), fma(x.x, y.y, fma(x.y, y.x, s.y))};
+}
+__device__ __forceinline__ cd cmsc(cd s, cd x, cd y)
+{
+    return cd{fma(-x.x, y.x, fma(x.y, y.y, s.x)), fma(-x.x, y.y, fma(-x.y, y.x, s.y))};
+}
+__device__ __forceinline__ cd cmac(cd s, double x, cd y) { return cd{fma(x, y.x, s.x), fma(x, y.y, s.y)}; }
+__device__ __forceinline__ cd cmsc(cd s, double x, cd y) { return cd{fma(-x, y.x, s.x), fma(-x, y.y, s.y)}; }
+__device__ __forceinline__ cd cmac(cd s, cd x, double y) { return cmac(s, y, x); }
+__device__ __forceinline__ cd cmsc(cd s, cd x, double y) { return cmsc(s, y, x); }
+template <class S, class X, class Y>
+__device__ __forceinline__ S cmac(S s, X x, Y y)
+{
+    return s + x * y;
+}
+template <class S, class X, class Y>
+__device__ __forceinline__ S cmsc(S s, X x, Y y)
+{
+    return s - x * y;
+}
 struct TorSys {
     static constexpr int N = 2, CLS = 0;
     template <class Out>
     __device__ static __forceinline__ void f(const Ctx& c, double r, const mcplx* y, Out d)
     {
         TorCoef a = tor_amat(c, r);       // module_int.f90:168-184
-        d[0] = a.t * y[0] + a.k * y[1];
-        d[1] = a.s * y[0] - a.t * y[1];
+        d[0] = cmac(a.t * y[0], a.k, y[1]);
+        d[1] = cmsc(a.s * y[0], a.t, y[1]);
     }
 };
 
@@ -336,8 +363,8 @@ struct RadSys {
     __device__ static __forceinline__ void f(const Ctx& c, double r, const mcplx* y, Out d)
     {
         RadCoef a = rad_amat(c, r);       // module_int.f90:357-392
-        d[0] = a.t * y[0] + a.k * y[1];
-        d[1] = a.s * y[0] - a.t * y[1];
+        d[0] = cmac(a.t * y[0], a.k, y[1]);
+        d[1] = cmsc(a.s * y[0], a.t, y[1]);
     }
 };
 
@@ -350,30 +377,20 @@ struct MinorSolidG {
         SolidCoef a = solid_amat<2>(c, r);
         mcplx a123 = a.t11 + (a.t22 + a.t33), a126 = a.t11 + (a.t22 - a.t33);
         mcplx a135 = a.t11 - (a.t22 - a.t33), a234 = (a.t22 + a.t33) - a.t11;
-        d[0] = a.k33 * m[3] - a.k22 * m[5] + a.k11 * m[9] + m[0] * a123;
-        d[1] = -(a.k22 * m[6]) + m[0] * a.s13 - m[2] * a.t21 + m[1] * a.t22 - m[3] * a.t31;
-        d[2] = -(a.k11 * m[10]) + m[0] * a.s23 + m[2] * a.t11 - m[1] * a.t12;
-        d[3] = a.k22 * m[8] - a.k11 * m[11] + m[3] * a126;
-        d[4] = -(a.k33 * m[7]) - m[0] * a.s12 + m[9] * a.t12 - m[5] * a.t21 + m[2] * a.t31 +
-               m[4] * a.t33;
-        d[5] = -(a.k33 * m[8]) - a.k11 * m[12] - m[0] * a.s22 - 2.0 * (m[4] * a.t12) +
-               m[5] * a135;
-        d[6] = m[2] * a.s12 + m[5] * a.s13 - m[1] * a.s22 - m[4] * a.s23 + m[10] * a.t12 -
-               m[6] * a.t22 + m[8] * a.t31;
-        d[7] = m[3] * a.s12 - m[2] * a.s13 - m[1] * a.s23 + m[11] * a.t12 - m[8] * a.t21 -
-               m[7] * a.t33;
-        d[8] = a.k11 * m[13] + m[3] * a.s22 - 2.0 * (m[2] * a.s23) - 2.0 * (m[7] * a.t12) -
-               m[8] * a234;
-        d[9] = -(a.k33 * m[11]) + a.k22 * m[12] + m[0] * a.s11 + 2.0 * (m[4] * a.t21) -
-               2.0 * (m[1] * a.t31) + m[9] * a234;
-        d[10] = -(m[2] * a.s11) + m[1] * a.s12 - m[4] * a.s13 - m[9] * a.s23 -
-                m[10] * a.t11 + m[6] * a.t21 - m[7] * a.t31;
-        d[11] = -(a.k22 * m[13]) - m[3] * a.s11 + 2.0 * (m[1] * a.s13) +
-                2.0 * (m[7] * a.t21) - m[11] * a135;
-        d[12] = a.k33 * m[13] - m[5] * a.s11 + 2.0 * (m[4] * a.s12) + m[9] * a.s22 +
-                2.0 * (m[6] * a.t31) - m[12] * a126;
-        d[13] = m[8] * a.s11 - 2.0 * (m[7] * a.s12) + 2.0 * (m[6] * a.s13) - m[11] * a.s22 +
-                2.0 * (m[10] * a.s23) - m[13] * a123;
+        d[0] = cmac(cmac(cmsc(a.k33 * m[3], a.k22, m[5]), a.k11, m[9]), m[0], a123);
+        d[1] = cmsc(cmac(cmsc(cmac(-(a.k22 * m[6]), m[0], a.s13), m[2], a.t21), m[1], a.t22), m[3], a.t31);
+        d[2] = cmsc(cmac(cmac(-(a.k11 * m[10]), m[0], a.s23), m[2], a.t11), m[1], a.t12);
+        d[3] = cmac(cmsc(a.k22 * m[8], a.k11, m[11]), m[3], a126);
+        d[4] = cmac(cmac(cmsc(cmac(cmsc(-(a.k33 * m[7]), m[0], a.s12), m[9], a.t12), m[5], a.t21), m[2], a.t31), m[4], a.t33);
+        d[5] = cmac(cmsc(cmsc(cmsc(-(a.k33 * m[8]), a.k11, m[12]), m[0], a.s22), (2.0 * m[4]), a.t12), m[5], a135);
+        d[6] = cmac(cmsc(cmac(cmsc(cmsc(cmac(m[2] * a.s12, m[5], a.s13), m[1], a.s22), m[4], a.s23), m[10], a.t12), m[6], a.t22), m[8], a.t31);
+        d[7] = cmsc(cmsc(cmac(cmsc(cmsc(m[3] * a.s12, m[2], a.s13), m[1], a.s23), m[11], a.t12), m[8], a.t21), m[7], a.t33);
+        d[8] = cmsc(cmsc(cmsc(cmac(a.k11 * m[13], m[3], a.s22), (2.0 * m[2]), a.s23), (2.0 * m[7]), a.t12), m[8], a234);
+        d[9] = cmac(cmsc(cmac(cmac(cmac(-(a.k33 * m[11]), a.k22, m[12]), m[0], a.s11), (2.0 * m[4]), a.t21), (2.0 * m[1]), a.t31), m[9], a234);
+        d[10] = cmsc(cmac(cmsc(cmsc(cmsc(cmac(-(m[2] * a.s11), m[1], a.s12), m[4], a.s13), m[9], a.s23), m[10], a.t11), m[6], a.t21), m[7], a.t31);
+        d[11] = cmsc(cmac(cmac(cmsc(-(a.k22 * m[13]), m[3], a.s11), (2.0 * m[1]), a.s13), (2.0 * m[7]), a.t21), m[11], a135);
+        d[12] = cmsc(cmac(cmac(cmac(cmsc(a.k33 * m[13], m[5], a.s11), (2.0 * m[4]), a.s12), m[9], a.s22), (2.0 * m[6]), a.t31), m[12], a126);
+        d[13] = cmsc(cmac(cmsc(cmac(cmsc(m[8] * a.s11, (2.0 * m[7]), a.s12), (2.0 * m[6]), a.s13), m[11], a.s22), (2.0 * m[10]), a.s23), m[13], a123);
     }
 };
 
@@ -386,11 +403,11 @@ struct MinorSolidNC {
     {
         SolidCoef a = solid_amat<KIND>(c, r);
         mcplx a11 = a.t11 + a.t22, a22 = a.t11 - a.t22;
-        d[0] = a11 * m[0] + a.k22 * m[2] - a.k11 * m[3];
-        d[1] = a.s12 * m[0] - a.t21 * m[2] + a.t12 * m[3];
-        d[2] = a.s22 * m[0] - 2.0 * (a.t12 * m[1]) + a22 * m[2] + a.k11 * m[4];
-        d[3] = -(a.s11 * m[0]) + (2.0 * a.t21) * m[1] - a22 * m[3] - a.k22 * m[4];
-        d[4] = -2.0 * (a.s12 * m[1]) + a.s11 * m[2] - a.s22 * m[3] - a11 * m[4];
+        d[0] = cmsc(cmac(a11 * m[0], a.k22, m[2]), a.k11, m[3]);
+        d[1] = cmac(cmsc(a.s12 * m[0], a.t21, m[2]), a.t12, m[3]);
+        d[2] = cmac(cmac(cmsc(a.s22 * m[0], (2.0 * a.t12), m[1]), a22, m[2]), a.k11, m[4]);
+        d[3] = cmsc(cmsc(cmac(-(a.s11 * m[0]), (2.0 * a.t21), m[1]), a22, m[3]), a.k22, m[4]);
+        d[4] = cmsc(cmsc(cmac(-((2.0 * a.s12) * m[1]), a.s11, m[2]), a.s22, m[3]), a11, m[4]);
     }
 };
 
@@ -402,11 +419,11 @@ struct MinorFluidG {
     {
         FluidCoef a = fluid_amat<2>(c, r);
         mcplx tp = a.t11 + a.t22, tm = a.t11 - a.t22;
-        d[0] = a.k22 * m[2] - a.k11 * m[3] + m[0] * tp;
-        d[1] = m[0] * a.s12 + m[3] * a.t12 - m[2] * a.t21;
-        d[2] = a.k11 * m[4] + m[0] * a.s22 - 2.0 * (m[1] * a.t12) + m[2] * tm;
-        d[3] = -(a.k22 * m[4]) - m[0] * a.s11 + (2.0 * a.t21) * m[1] - m[3] * tm;
-        d[4] = m[2] * a.s11 - 2.0 * (m[1] * a.s12) - m[3] * a.s22 - m[4] * tp;
+        d[0] = cmac(cmsc(a.k22 * m[2], a.k11, m[3]), m[0], tp);
+        d[1] = cmsc(cmac(m[0] * a.s12, m[3], a.t12), m[2], a.t21);
+        d[2] = cmac(cmsc(cmac(a.k11 * m[4], m[0], a.s22), (2.0 * m[1]), a.t12), m[2], tm);
+        d[3] = cmsc(cmac(cmsc(-(a.k22 * m[4]), m[0], a.s11), (2.0 * a.t21), m[1]), m[3], tm);
+        d[4] = cmsc(cmsc(cmsc(m[2] * a.s11, (2.0 * m[1]), a.s12), m[3], a.s22), m[4], tp);
     }
 };
 
@@ -418,8 +435,8 @@ struct MinorFluidNC {
     __device__ static __forceinline__ void f(const Ctx& c, double r, const mcplx* m, Out d)
     {
         FluidCoef a = fluid_amat<KIND>(c, r);
-        d[0] = a.t11 * m[0] + a.k11 * m[1];
-        d[1] = a.s11 * m[0] - a.t11 * m[1];
+        d[0] = cmac(a.t11 * m[0], a.k11, m[1]);
+        d[1] = cmsc(a.s11 * m[0], a.t11, m[1]);
     }
 };
 
@@ -434,26 +451,20 @@ struct BvecSolidG {
         const mcplx s11 = a.s11, s12 = a.s12, s22 = a.s22;
         const mreal t21 = a.t21, t22 = a.t22, t31 = a.t31, t33 = a.t33, k33 = a.k33;
         const mreal s13 = a.s13, s23 = a.s23;
-        d[0] = s11 * b[6] + s12 * (b[7] - b[2]) + s13 * b[8] - s22 * b[3] - s23 * b[4] -
-               (t11 + t22) * b[0] + t31 * b[5];
-        d[1] = s11 * b[9] + s12 * b[10] - s13 * (2.0 * b[2] + b[7]) - s23 * b[3] -
-               t21 * b[5] - (t11 + t33) * b[1];
-        d[2] = s12 * b[11] + s13 * b[12] + t12 * b[3] - t21 * b[6] - t31 * b[9];
-        d[3] = -(k22 * b[0]) - s11 * b[11] + s13 * b[13] + t21 * (b[2] - b[7]) +
-               (t22 - t11) * b[3] - t31 * b[10];
-        d[4] = -(k33 * b[1]) - s11 * b[12] - s12 * b[13] - t21 * b[8] +
-               t31 * (2.0 * b[2] + b[7]) + (t33 - t11) * b[4];
-        d[5] = s12 * b[9] - s13 * b[6] + s22 * b[10] - s23 * (b[2] + 2.0 * b[7]) -
-               t12 * b[1] - (t22 + t33) * b[5];
-        d[6] = k11 * b[0] + s22 * b[11] + s23 * b[12] - t12 * (b[2] - b[7]) + (t11 - t22) * b[6];
-        d[7] = -(s12 * b[11]) + s23 * b[13] - t12 * b[3] + t21 * b[6];
-        d[8] = -(k33 * b[5]) - s12 * b[12] - s22 * b[13] - t12 * b[4] - t22 * b[8] +
-               t31 * b[6] + t33 * b[8];
-        d[9] = k11 * b[1] + s23 * b[11] + t12 * b[10] + (t11 - t33) * b[9];
-        d[10] = k22 * b[5] - s13 * b[11] + t21 * b[9] + (t22 - t33) * b[10];
-        d[11] = -(k11 * b[3]) + k22 * b[6] + (t11 + t22) * b[11];
-        d[12] = -(k11 * b[4]) + k33 * b[9] + t12 * b[13] + (t11 + t33) * b[12];
-        d[13] = -(k22 * b[8]) + k33 * b[10] + t21 * b[12] - t31 * b[11] + (t22 + t33) * b[13];
+        d[0] = cmac(cmsc(cmsc(cmsc(cmac(cmac(s11 * b[6], s12, (b[7] - b[2])), s13, b[8]), s22, b[3]), s23, b[4]), (t11 + t22), b[0]), t31, b[5]);
+        d[1] = cmsc(cmsc(cmsc(cmsc(cmac(s11 * b[9], s12, b[10]), s13, (2.0 * b[2] + b[7])), s23, b[3]), t21, b[5]), (t11 + t33), b[1]);
+        d[2] = cmsc(cmsc(cmac(cmac(s12 * b[11], s13, b[12]), t12, b[3]), t21, b[6]), t31, b[9]);
+        d[3] = cmsc(cmac(cmac(cmac(cmsc(-(k22 * b[0]), s11, b[11]), s13, b[13]), t21, (b[2] - b[7])), (t22 - t11), b[3]), t31, b[10]);
+        d[4] = cmac(cmac(cmsc(cmsc(cmsc(-(k33 * b[1]), s11, b[12]), s12, b[13]), t21, b[8]), t31, (2.0 * b[2] + b[7])), (t33 - t11), b[4]);
+        d[5] = cmsc(cmsc(cmsc(cmac(cmsc(s12 * b[9], s13, b[6]), s22, b[10]), s23, (b[2] + 2.0 * b[7])), t12, b[1]), (t22 + t33), b[5]);
+        d[6] = cmac(cmsc(cmac(cmac(k11 * b[0], s22, b[11]), s23, b[12]), t12, (b[2] - b[7])), (t11 - t22), b[6]);
+        d[7] = cmac(cmsc(cmac(-(s12 * b[11]), s23, b[13]), t12, b[3]), t21, b[6]);
+        d[8] = cmac(cmac(cmsc(cmsc(cmsc(cmsc(-(k33 * b[5]), s12, b[12]), s22, b[13]), t12, b[4]), t22, b[8]), t31, b[6]), t33, b[8]);
+        d[9] = cmac(cmac(cmac(k11 * b[1], s23, b[11]), t12, b[10]), (t11 - t33), b[9]);
+        d[10] = cmac(cmac(cmsc(k22 * b[5], s13, b[11]), t21, b[9]), (t22 - t33), b[10]);
+        d[11] = cmac(cmac(-(k11 * b[3]), k22, b[6]), (t11 + t22), b[11]);
+        d[12] = cmac(cmac(cmac(-(k11 * b[4]), k33, b[9]), t12, b[13]), (t11 + t33), b[12]);
+        d[13] = cmac(cmsc(cmac(cmac(-(k22 * b[8]), k33, b[10]), t21, b[12]), t31, b[11]), (t22 + t33), b[13]);
     }
 };
 
@@ -465,10 +476,10 @@ struct BvecSolidNC {
     __device__ static __forceinline__ void f(const Ctx& c, double r, const mcplx* b, Out d)
     {
         SolidCoef a = solid_amat<KIND>(c, r);
-        d[0] = -(a.s11 * b[2]) - a.s12 * b[3] - a.t11 * b[0] - a.t21 * b[1];
-        d[1] = -(a.s12 * b[2]) - a.s22 * b[3] - a.t12 * b[0] - a.t22 * b[1];
-        d[2] = -(a.k11 * b[0]) + a.t11 * b[2] + a.t12 * b[3];
-        d[3] = -(a.k22 * b[1]) + a.t21 * b[2] + a.t22 * b[3];
+        d[0] = cmsc(cmsc(cmsc(-(a.s11 * b[2]), a.s12, b[3]), a.t11, b[0]), a.t21, b[1]);
+        d[1] = cmsc(cmsc(cmsc(-(a.s12 * b[2]), a.s22, b[3]), a.t12, b[0]), a.t22, b[1]);
+        d[2] = cmac(cmac(-(a.k11 * b[0]), a.t11, b[2]), a.t12, b[3]);
+        d[3] = cmac(cmac(-(a.k22 * b[1]), a.t21, b[2]), a.t22, b[3]);
     }
 };
 
