@@ -322,8 +322,8 @@ __device__ __forceinline__ FluidCoef fluid_amat(const Ctx& c, double rr)
 // Complex multiply-accumulate s + x y (cmac) and s - x y (cmsc) as fused
 // multiply-adds: four for a complex factor, two for a real one, where a
 // product followed by a sum takes six and four.  The 14-component systems
-// accumulate their outputs term by term with them.  Other types (the dual
-// numbers of the tangent build) use the plain operators.
+// accumulate their outputs term by term with them, in the tangent build
+// too (the value and the derivative part each fused).
 __device__ __forceinline__ cd cmac(cd s, cd x, cd y)
 {
     return cd{fma(x.x, y.x, fma(-x.y, y.y, s.x)), fma(x.x, y.y, fma(x.y, y.x, s.y))};
@@ -336,6 +336,25 @@ __device__ __forceinline__ cd cmac(cd s, double x, cd y) { return cd{fma(x, y.x,
 __device__ __forceinline__ cd cmsc(cd s, double x, cd y) { return cd{fma(-x, y.x, s.x), fma(-x, y.y, s.y)}; }
 __device__ __forceinline__ cd cmac(cd s, cd x, double y) { return cmac(s, y, x); }
 __device__ __forceinline__ cd cmsc(cd s, cd x, double y) { return cmsc(s, y, x); }
+// dual numbers: the value and d(s + x y) = ds + dx y + x dy, both fused
+__device__ __forceinline__ dcplx cmac(dcplx s, dcplx x, dcplx y)
+{
+    return dcplx(cmac(s.v, x.v, y.v), cmac(cmac(s.d, x.d, y.v), x.v, y.d));
+}
+__device__ __forceinline__ dcplx cmsc(dcplx s, dcplx x, dcplx y)
+{
+    return dcplx(cmsc(s.v, x.v, y.v), cmsc(cmsc(s.d, x.d, y.v), x.v, y.d));
+}
+__device__ __forceinline__ dcplx cmac(dcplx s, dreal x, dcplx y)
+{
+    return dcplx(cmac(s.v, x.v, y.v), cmac(cmac(s.d, x.d, y.v), x.v, y.d));
+}
+__device__ __forceinline__ dcplx cmsc(dcplx s, dreal x, dcplx y)
+{
+    return dcplx(cmsc(s.v, x.v, y.v), cmsc(cmsc(s.d, x.d, y.v), x.v, y.d));
+}
+__device__ __forceinline__ dcplx cmac(dcplx s, dcplx x, dreal y) { return cmac(s, y, x); }
+__device__ __forceinline__ dcplx cmsc(dcplx s, dcplx x, dreal y) { return cmsc(s, y, x); }
 template <class S, class X, class Y>
 __device__ __forceinline__ S cmac(S s, X x, Y y)
 {
