@@ -215,9 +215,10 @@ int ysg_set_schedule(ysg_handle *h, int sched);
  * each schedule from the last autotuning run (tune_ms may be NULL). */
 int ysg_last_schedule(ysg_handle *h, int *sched, float tune_ms[3]);
 
-/* Device times in ms of the last event's stages, measured with CUDA events
- * on the handle's stream: [0] Legendre table, [1] solves, [2] l-sum,
- * [3] filter + inverse FFT + post-processing. */
+/* Device times in ms of the last event's stages, measured with CUDA events:
+ * [0] Legendre table, [1] solves, [2] l-sum, [3] filter + inverse FFT +
+ * post-processing.  For a single event (not a batch) the Legendre table is
+ * built on a second stream beside the solves, so [0] overlaps [1]. */
 int ysg_last_timings(ysg_handle *h, float ms[4]);
 
 /* Counters of the last solve stage: number of (omega,l) pairs and the

@@ -93,7 +93,8 @@ struct Slot {
 struct ysg_handle {
     int device = 0;
     cudaStream_t st = nullptr;
-    cudaEvent_t ev[5] = {};
+    cudaEvent_t ev[6] = {};          // stage boundaries 0..4; 5 = end of an overlapped K2
+    bool leg_overlap = false;        // K2 of the last single event ran beside K1
     int solver = 1;
     // model
     DevBuf kn, sg, hdr_dev;
@@ -599,19 +600,36 @@ int enqueue_spectra(ysg_handle* h, int nev)
 {
     const int ns = side_count(nev);
     CK(record(h, 0));
-    int rc = ns ? fork_side(h, ns) : YSG_OK;
-    if (rc) return rc;
-    for (int e = 0; e < nev; e++) {
-        Slot& s = h->slots[(size_t)e];
+    int rc = YSG_OK;
+    // One event outside stream capture: the Legendre table, which only the
+    // l-sum reads, runs on side stream 1 beside the cost model and the
+    // solves (schedule 2 uses side stream 0); the l-sum waits for it.
+    h->leg_overlap = ns == 0 && !h->capturing;
+    if (h->leg_overlap) {
+        Slot& s = h->slots[0];
+        CK(cudaEventRecord(h->fork_ev, h->st));
+        CK(cudaStreamWaitEvent(h->side[1], h->fork_ev, 0));
         h->launches += s.nr > 0 ? 1 : 0;
         CK(launch_legendre(s.nr, s.lmax, s.delta.as<double>(), s.ct.as<double>(), s.stv.as<double>(),
-                           s.leg.as<double>(), stream_of(h, ns, e)));
+                           s.leg.as<double>(), h->side[1]));
+        CK(cudaEventRecord(h->ev[5], h->side[1]));
+        CK(cudaEventRecord(h->join_ev[1], h->side[1]));
+    } else {
+        rc = ns ? fork_side(h, ns) : YSG_OK;
+        if (rc) return rc;
+        for (int e = 0; e < nev; e++) {
+            Slot& s = h->slots[(size_t)e];
+            h->launches += s.nr > 0 ? 1 : 0;
+            CK(launch_legendre(s.nr, s.lmax, s.delta.as<double>(), s.ct.as<double>(), s.stv.as<double>(),
+                               s.leg.as<double>(), stream_of(h, ns, e)));
+        }
+        if (ns && (rc = join_side(h, ns))) return rc;
     }
-    if (ns && (rc = join_side(h, ns))) return rc;
     CK(record(h, 1));
     rc = enqueue_solve(h, nev);
     if (rc) return rc;
     CK(record(h, 2));
+    if (h->leg_overlap) CK(cudaStreamWaitEvent(h->st, h->join_ev[1], 0));
     if (ns && (rc = fork_side(h, ns))) return rc;
     for (int e = 0; e < nev; e++) {
         Slot& s = h->slots[(size_t)e];
@@ -687,7 +705,8 @@ int finish(ysg_handle* h, int nev, bool spectra, bool traces)
             pairs += (double)(d.lmax - d.lmin + 1) * d.nw;
         }
         h->pairs = pairs;
-        CK(cudaEventElapsedTime(&h->ms[0], h->ev[0], h->ev[1]));
+        // K2's time: to the end of the table, on its own stream when overlapped
+        CK(cudaEventElapsedTime(&h->ms[0], h->ev[0], h->ev[h->leg_overlap ? 5 : 1]));
         CK(cudaEventElapsedTime(&h->ms[1], h->ev[1], h->ev[2]));
         CK(cudaEventElapsedTime(&h->ms[2], h->ev[2], h->ev[3]));
         h->has_spectra = status == 0;
@@ -1028,6 +1047,7 @@ int ysg_event_coef(ysg_handle* h, const ysg_event* ev, double* coef)
     h->has_spectra = false;
     rc = prepare_single(h, ev);
     if (rc) return rc;
+    h->leg_overlap = false;          // no Legendre stage here
     CK(record(h, 0));
     CK(record(h, 1));
     rc = enqueue_solve(h, 1);
