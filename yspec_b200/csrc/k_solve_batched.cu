@@ -38,15 +38,17 @@ namespace ysg {
 // only).  The kernels that run 14-component systems need four slots of 14
 // complex values per thread: four 64-thread blocks fill the SM's shared
 // memory, each thread with the full 255 registers.  The toroidal-only
-// kernel steps a 2-component system: a small slab and a smaller register
-// budget (168 registers, no spills) let twelve warps share an SM.
+// kernel steps a 2-component system: a small slab and a register budget of
+// 96 let twenty warps share an SM.  Its few hundred bytes of spills cost
+// less than the occupancy gains: on c2 it beat 168 registers without spills
+// (twelve warps) and 128 registers (sixteen warps).
 template <int PART>
 struct SolveCfg {
     static constexpr int BLOCK = 64, MINB = 4, SLAB = 4 * 14;
 };
 template <>
 struct SolveCfg<1> {
-    static constexpr int BLOCK = 128, MINB = 3, SLAB = 4 * 2;
+    static constexpr int BLOCK = 128, MINB = 5, SLAB = 4 * 2;
 };
 
 template <int SCHED, int PART>
