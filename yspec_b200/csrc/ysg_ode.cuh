@@ -156,6 +156,53 @@ __device__ __forceinline__ mreal splr(const Ctx& c, const SplPt& s, int p)
 #endif
 }
 
+// Complex multiply-accumulate s + x y (cmac) and s - x y (cmsc) as fused
+// multiply-adds: four for a complex factor, two for a real one, where a
+// product followed by a sum takes six and four.  The 14-component systems
+// accumulate their outputs term by term with them, in the tangent build
+// too (the value and the derivative part each fused).
+__device__ __forceinline__ cd cmac(cd s, cd x, cd y)
+{
+    return cd{fma(x.x, y.x, fma(-x.y, y.y, s.x)), fma(x.x, y.y, fma(x.y, y.x, s.y))};
+}
+__device__ __forceinline__ cd cmsc(cd s, cd x, cd y)
+{
+    return cd{fma(-x.x, y.x, fma(x.y, y.y, s.x)), fma(-x.x, y.y, fma(-x.y, y.x, s.y))};
+}
+__device__ __forceinline__ cd cmac(cd s, double x, cd y) { return cd{fma(x, y.x, s.x), fma(x, y.y, s.y)}; }
+__device__ __forceinline__ cd cmsc(cd s, double x, cd y) { return cd{fma(-x, y.x, s.x), fma(-x, y.y, s.y)}; }
+__device__ __forceinline__ cd cmac(cd s, cd x, double y) { return cmac(s, y, x); }
+__device__ __forceinline__ cd cmsc(cd s, cd x, double y) { return cmsc(s, y, x); }
+// dual numbers: the value and d(s + x y) = ds + dx y + x dy, both fused
+__device__ __forceinline__ dcplx cmac(dcplx s, dcplx x, dcplx y)
+{
+    return dcplx(cmac(s.v, x.v, y.v), cmac(cmac(s.d, x.d, y.v), x.v, y.d));
+}
+__device__ __forceinline__ dcplx cmsc(dcplx s, dcplx x, dcplx y)
+{
+    return dcplx(cmsc(s.v, x.v, y.v), cmsc(cmsc(s.d, x.d, y.v), x.v, y.d));
+}
+__device__ __forceinline__ dcplx cmac(dcplx s, dreal x, dcplx y)
+{
+    return dcplx(cmac(s.v, x.v, y.v), cmac(cmac(s.d, x.d, y.v), x.v, y.d));
+}
+__device__ __forceinline__ dcplx cmsc(dcplx s, dreal x, dcplx y)
+{
+    return dcplx(cmsc(s.v, x.v, y.v), cmsc(cmsc(s.d, x.d, y.v), x.v, y.d));
+}
+__device__ __forceinline__ dcplx cmac(dcplx s, dcplx x, dreal y) { return cmac(s, y, x); }
+__device__ __forceinline__ dcplx cmsc(dcplx s, dcplx x, dreal y) { return cmsc(s, y, x); }
+template <class S, class X, class Y>
+__device__ __forceinline__ S cmac(S s, X x, Y y)
+{
+    return s + x * y;
+}
+template <class S, class X, class Y>
+__device__ __forceinline__ S cmsc(S s, X x, Y y)
+{
+    return s - x * y;
+}
+
 // ---------------------------------------------------------------------------
 // Coefficient matrices
 //
@@ -206,7 +253,7 @@ __device__ __forceinline__ RadCoef rad_amat(const Ctx& c, double rr)
     const mreal dc = rccon * norm2(qaa);
     const mreal inv = 1.0 / (rr * dc);
     mcplx cccon = conj(qaa) * (rr * inv);     // 1 / (C (1 + qa lno))
-    mcplx gamma = cacon - cncon - cfcon * cfcon * cccon;
+    mcplx gamma = cmsc(cacon - cncon, cfcon * cfcon, cccon);
     mreal ri = dc * inv;
     RadCoef a;
     a.t = (1.0 - 2.0 * cfcon * cccon) * ri;
@@ -238,7 +285,7 @@ __device__ __forceinline__ SolidCoef solid_amat(const Ctx& c, double rr)
     const mreal inv = 1.0 / (rr * (dc * dl));
     mcplx cccon = conj(qaa) * ((rr * dl) * inv);     // 1 / (C (1 + qa lno))
     mcplx fc = cfcon * cccon;
-    mcplx gamma = cacon - cncon - cfcon * fc;
+    mcplx gamma = cmsc(cacon - cncon, cfcon, fc);
     mreal ri = (dc * dl) * inv, ri2 = ri * ri;
     SolidCoef a;
     a.t11 = (1.0 - 2.0 * fc) * ri;
@@ -319,52 +366,6 @@ __device__ __forceinline__ FluidCoef fluid_amat(const Ctx& c, double rr)
 // ---------------------------------------------------------------------------
 // Right-hand sides.  Each system is a tag type with N components and f().
 // ---------------------------------------------------------------------------
-// Complex multiply-accumulate s + x y (cmac) and s - x y (cmsc) as fused
-// multiply-adds: four for a complex factor, two for a real one, where a
-// product followed by a sum takes six and four.  The 14-component systems
-// accumulate their outputs term by term with them, in the tangent build
-// too (the value and the derivative part each fused).
-__device__ __forceinline__ cd cmac(cd s, cd x, cd y)
-{
-    return cd{fma(x.x, y.x, fma(-x.y, y.y, s.x)), fma(x.x, y.y, fma(x.y, y.x, s.y))};
-}
-__device__ __forceinline__ cd cmsc(cd s, cd x, cd y)
-{
-    return cd{fma(-x.x, y.x, fma(x.y, y.y, s.x)), fma(-x.x, y.y, fma(-x.y, y.x, s.y))};
-}
-__device__ __forceinline__ cd cmac(cd s, double x, cd y) { return cd{fma(x, y.x, s.x), fma(x, y.y, s.y)}; }
-__device__ __forceinline__ cd cmsc(cd s, double x, cd y) { return cd{fma(-x, y.x, s.x), fma(-x, y.y, s.y)}; }
-__device__ __forceinline__ cd cmac(cd s, cd x, double y) { return cmac(s, y, x); }
-__device__ __forceinline__ cd cmsc(cd s, cd x, double y) { return cmsc(s, y, x); }
-// dual numbers: the value and d(s + x y) = ds + dx y + x dy, both fused
-__device__ __forceinline__ dcplx cmac(dcplx s, dcplx x, dcplx y)
-{
-    return dcplx(cmac(s.v, x.v, y.v), cmac(cmac(s.d, x.d, y.v), x.v, y.d));
-}
-__device__ __forceinline__ dcplx cmsc(dcplx s, dcplx x, dcplx y)
-{
-    return dcplx(cmsc(s.v, x.v, y.v), cmsc(cmsc(s.d, x.d, y.v), x.v, y.d));
-}
-__device__ __forceinline__ dcplx cmac(dcplx s, dreal x, dcplx y)
-{
-    return dcplx(cmac(s.v, x.v, y.v), cmac(cmac(s.d, x.d, y.v), x.v, y.d));
-}
-__device__ __forceinline__ dcplx cmsc(dcplx s, dreal x, dcplx y)
-{
-    return dcplx(cmsc(s.v, x.v, y.v), cmsc(cmsc(s.d, x.d, y.v), x.v, y.d));
-}
-__device__ __forceinline__ dcplx cmac(dcplx s, dcplx x, dreal y) { return cmac(s, y, x); }
-__device__ __forceinline__ dcplx cmsc(dcplx s, dcplx x, dreal y) { return cmsc(s, y, x); }
-template <class S, class X, class Y>
-__device__ __forceinline__ S cmac(S s, X x, Y y)
-{
-    return s + x * y;
-}
-template <class S, class X, class Y>
-__device__ __forceinline__ S cmsc(S s, X x, Y y)
-{
-    return s - x * y;
-}
 struct TorSys {
     static constexpr int N = 2, CLS = 0;
     template <class Out>
