@@ -92,13 +92,18 @@ __global__ void __launch_bounds__(128) k_pair_cost(const Knot* __restrict__ kn, 
     }
 }
 
+// The sort orders the key from bit 43 up (part, cost bucket, path class);
+// the entry index below it is a tie-break, and a stable radix sort keeps
+// equal keys in their input order, which is event-major already.
+constexpr int kSortBegin = 43;
+
 }  // namespace
 
 size_t pair_sort_tmp_bytes(long long npairs)
 {
     size_t bytes = 0;
     cub::DoubleBuffer<unsigned long long> k(nullptr, nullptr), v(nullptr, nullptr);
-    cub::DeviceRadixSort::SortPairsDescending(nullptr, bytes, k, v, (int)(2 * npairs));
+    cub::DeviceRadixSort::SortPairsDescending(nullptr, bytes, k, v, (int)(2 * npairs), kSortBegin, 64);
     return bytes;
 }
 
@@ -119,7 +124,7 @@ cudaError_t launch_pair_schedule(const Knot* kn, const Seg* sg, const ModelHdr* 
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     cub::DoubleBuffer<unsigned long long> k(keys[0], keys[1]), v(vals[0], vals[1]);
-    e = cub::DeviceRadixSort::SortPairsDescending(tmp, tmp_bytes, k, v, (int)(2 * npairs), 0, 64, st);
+    e = cub::DeviceRadixSort::SortPairsDescending(tmp, tmp_bytes, k, v, (int)(2 * npairs), kSortBegin, 64, st);
     if (e != cudaSuccess) return e;
     *sorted = v.Current();
     return cudaSuccess;
