@@ -112,7 +112,7 @@ def batch_compare(local: int, reps: int = 2) -> dict:
 def cpu_sample(pf: Path, stride: int, threads: int):
     """Oracle on every stride-th frequency of the event: (pairs, seconds)."""
     sys.path.insert(0, str(ROOT / "oracle"))
-    import yo  # the CPU restatement of the reference path (checker / baseline only)
+    import yo  # the CPU restatement of the reference path (test oracle / baseline only)
 
     P = yo.Problem(pf)
     nj = (P.nw - 1) // stride + 1

@@ -2,8 +2,8 @@
  * yo.h -- CPU oracle for the YSpec direct radial integration path.
  *
  * TEST INFRASTRUCTURE ONLY.  This is a plain-C FP64 restatement of the
- * reference Fortran (da380/YSpec, the Fortran sources under src/) used as the checker for the
- * CUDA product path.  Only tests/, __graft_entry__.smoke() and bench.py's
+ * reference Fortran (da380/YSpec, the Fortran sources under src/) against
+ * which the CUDA product path is tested.  Only tests/, __graft_entry__.smoke() and bench.py's
  * cpu_baseline / --impl reference legs may load it.  It is never part of the
  * product path.
  *

@@ -1,7 +1,7 @@
 """ctypes loader of the CPU oracle (oracle/liboracle.so).
 
-TEST INFRASTRUCTURE ONLY: imported by tests/, by __graft_entry__.smoke() as
-the checker, and by bench.py for the CPU baseline leg.  The product
+TEST INFRASTRUCTURE ONLY: imported by tests/, by __graft_entry__.smoke() to
+check the device traces, and by bench.py for the CPU baseline leg.  The product
 (yspec_b200) never imports it.  Parity status: unpinned (see yo.h).
 """
 from __future__ import annotations

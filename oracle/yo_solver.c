@@ -1006,7 +1006,7 @@ static void make_grid(const yo_model *m, double drr, double rs, double rr, int *
 }
 
 /* module_solver.f90:446-561 rad_solver_wg.  Only yout is returned: the    */
-/* potential pout is not used by the driver (yspec.f90:277-281).            */
+/* potential pout is not used by the main program (yspec.f90:277-281).      */
 void yo_rad_solver_wg(yo_ctx *c, yo_cd w, double rr, double rs, int ir, int is,
                       yo_cd yout[2][2])
 {

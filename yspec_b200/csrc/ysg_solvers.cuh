@@ -149,7 +149,7 @@ __device__ __forceinline__ int seg_npts(const GridSeg& s, double drr)
 }
 
 // module_solver.f90:446-561 rad_solver_wg.  The potential pout is not used
-// by the driver (yspec.f90:277-281) and is not formed.
+// by the main program (yspec.f90:277-281) and is not formed.
 __device__ inline void rad_solver_wg(Ctx& c, double rr, double rs, mcplx yout[2][2])
 {
     const ModelHdr* mh = c.mh;
