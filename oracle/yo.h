@@ -119,6 +119,27 @@ int yo_spectra(const yo_model *m, const yo_norms *n, const yo_params *p,
                int nthreads, int lsub_lo, int lsub_hi, int jsub,
                yo_counts *cnt);
 
+/* Spectra of a frequency shard: column c (0-based, c < count) of the
+ * (count, nr) column-major arrays holds omega_j, j = 1 + jofs + c jstride,
+ * as the device's jofs/jstride event fields define a shard. */
+int yo_spectra_shard(const yo_model *m, const yo_norms *n, const yo_params *p,
+                     const yo_grid *g, int jofs, int jstride, int count, yo_cd *ur,
+                     yo_cd *ut, yo_cd *up, int nthreads);
+
+/* yo_solve_pair for npair (ls[k], js[k]) pairs; coef is (15, npair)
+ * column-major (15 coefficients per pair, pair after pair). */
+int yo_coef_list(const yo_model *m, const yo_norms *n, const yo_params *p,
+                 const yo_grid *g, int npair, const int *ls, const int *js,
+                 yo_cd *coef, int nthreads);
+
+/* The solution of one two-point solver at radius rr (knot index ir) for
+ * unit jumps at rs (index is), omega = wr + i wi: kind 0 toroidal (2 x 2),
+ * 1 radial without and 2 with gravity (2 x 2), 3 spheroidal with full
+ * gravity (6 x 4), 4 without gravity and 5 Cowling (4 x 4); row-major.
+ * Used by the reciprocity and gravity-limit checks of the oracle. */
+int yo_green(const yo_model *m, const yo_norms *n, int kind, int l, double wr,
+             double wi, int ats, double rr, double rs, int ir, int is, yo_cd *out);
+
 /* Legendre/geometry table used by the l-sum (yspec.f90:144-174):
  * xa/xpa/xca are (lmax+1, 3, nr) column-major; delta/azst/azep are nr. */
 void yo_geometry(const yo_params *p, double *delta, double *azep,

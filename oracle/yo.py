@@ -82,6 +82,15 @@ def lib() -> C.CDLL:
                                     C.c_int, C.c_int, _dp, C.POINTER(Counts)]
         L.yo_spectra.argtypes = [C.POINTER(Model), C.POINTER(Norms), C.POINTER(Params), C.POINTER(Grid),
                                  _dp, _dp, _dp, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(Counts)]
+        L.yo_spectra_shard.argtypes = [C.POINTER(Model), C.POINTER(Norms), C.POINTER(Params),
+                                       C.POINTER(Grid), C.c_int, C.c_int, C.c_int, _dp, _dp, _dp,
+                                       C.c_int]
+        _ip = C.POINTER(C.c_int)
+        L.yo_coef_list.argtypes = [C.POINTER(Model), C.POINTER(Norms), C.POINTER(Params),
+                                   C.POINTER(Grid), C.c_int, _ip, _ip, _dp, C.c_int]
+        L.yo_green.argtypes = [C.POINTER(Model), C.POINTER(Norms), C.c_int, C.c_int, C.c_double,
+                               C.c_double, C.c_int, C.c_double, C.c_double, C.c_int, C.c_int, _dp]
+        L.yo_find_radius_index.argtypes = [C.POINTER(Model), C.c_double]
         L.yo_geometry.argtypes = [C.POINTER(Params), _dp, _dp, _dp]
         L.yo_legendre_table.argtypes = [_dp, C.c_int, C.c_int, _dp, _dp, _dp]
         L.yo_traces.argtypes = [C.POINTER(Norms), C.POINTER(Params), C.POINTER(Grid), _dp, _dp, _dp,
@@ -152,6 +161,48 @@ class Problem:
                          C.byref(self.grid), *[_p(b) for b in bufs], nthreads, lo, hi, jsub,
                          C.byref(counts) if counts else None)
         return tuple((b[..., 0] + 1j * b[..., 1])[:nr] for b in bufs)
+
+    def spectra_shard(self, jofs: int, jstride: int, count: int, nthreads: int = 0):
+        """Spectra (nr, count) of the frequencies j = 1 + jofs + c jstride."""
+        nr = self.nr
+        bufs = [np.zeros((max(nr, 1), count, 2)) for _ in range(3)]
+        rc = lib().yo_spectra_shard(C.byref(self.model), C.byref(self.norms), C.byref(self.params),
+                                    C.byref(self.grid), jofs, jstride, count,
+                                    *[_p(b) for b in bufs], nthreads)
+        if rc:
+            raise ValueError(f"oracle: spectra_shard rc {rc}")
+        return tuple((b[..., 0] + 1j * b[..., 1])[:nr] for b in bufs)
+
+    def coef_list(self, ls, js, nthreads: int = 0) -> np.ndarray:
+        """Coefficients (npair, 15) of the (l, j) pairs (j 1-based), on threads."""
+        ls = np.ascontiguousarray(ls, dtype=np.int32)
+        js = np.ascontiguousarray(js, dtype=np.int32)
+        if ls.shape != js.shape or ls.ndim != 1:
+            raise ValueError("ls and js: equal 1-d lengths")
+        buf = np.zeros((ls.size, 15, 2))
+        ip = C.POINTER(C.c_int)
+        rc = lib().yo_coef_list(C.byref(self.model), C.byref(self.norms), C.byref(self.params),
+                                C.byref(self.grid), ls.size, ls.ctypes.data_as(ip),
+                                js.ctypes.data_as(ip), _p(buf), nthreads)
+        if rc:
+            raise ValueError(f"oracle: coef_list rc {rc}")
+        return buf[..., 0] + 1j * buf[..., 1]
+
+    GREEN_SHAPE = {0: (2, 2), 1: (2, 2), 2: (2, 2), 3: (6, 4), 4: (4, 4), 5: (4, 4)}
+
+    def radius_index(self, r: float) -> int:
+        """find_radius_index (module_model.f90:537) of a normalised radius."""
+        return lib().yo_find_radius_index(C.byref(self.model), r)
+
+    def green(self, kind: int, l: int, w: complex, rr: float, rs: float, ats: int = 0) -> np.ndarray:
+        """Solution at normalised radius rr for unit jumps at rs (see yo_green)."""
+        shape = self.GREEN_SHAPE[kind]
+        buf = np.zeros(shape + (2,))
+        rc = lib().yo_green(C.byref(self.model), C.byref(self.norms), kind, l, w.real, w.imag, ats,
+                            rr, rs, self.radius_index(rr), self.radius_index(rs), _p(buf))
+        if rc:
+            raise ValueError(f"oracle: green rc {rc}")
+        return buf[..., 0] + 1j * buf[..., 1]
 
     def geometry(self):
         nr = self.nr

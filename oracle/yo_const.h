@@ -30,5 +30,6 @@
 #define YO_ERR_REC_MODEL 9      /* yspec.f90:214 */
 #define YO_ERR_REC_OCEAN 10     /* yspec.f90:215 */
 #define YO_ERR_IO 11
+#define YO_ERR_ARG 20           /* oracle-only: an argument out of range */
 
 #endif

@@ -192,6 +192,8 @@ typedef struct {
     const double *xa, *xpa, *xca;
     const yo_cd *eia;
     int lo, hi, jmax, jstride, next;
+    int jofs, ncol;                 /* job k takes j = 1 + jofs + (k-1) jstride; */
+                                    /* ncol > 0: stored in column k-1 of ncol    */
     pthread_mutex_t lock;
 } spectra_job;
 
@@ -201,10 +203,10 @@ typedef struct {
 } spectra_arg;
 
 /* one omega_j: every l in increasing order, then its l-sum contribution */
-static void spectra_one(const spectra_job *jb, int j, yo_counts *cnt)
+static void spectra_one(const spectra_job *jb, int j, int col, yo_counts *cnt)
 {
     const yo_params *p = jb->p;
-    int nr = p->nr, nw = jb->g->nw;
+    int nr = p->nr, nw = jb->ncol > 0 ? jb->ncol : jb->g->nw;
     size_t L1 = (size_t)p->lmax + 1;
     const double *xa = jb->xa, *xpa = jb->xpa, *xca = jb->xca;
     yo_cd *ur = jb->ur, *ut = jb->ut, *up = jb->up;
@@ -213,7 +215,7 @@ static void spectra_one(const spectra_job *jb, int j, yo_counts *cnt)
         yo_solve_pair(jb->m, jb->n, p, jb->g, l, j, coef, cnt);
         yo_cd *uu = coef, *vv = coef + 5, *ww = coef + 10;
         for (int k = 0; k < nr; k++) {
-            size_t o = (size_t)(j - 1) + (size_t)nw * (size_t)k;
+            size_t o = (size_t)col + (size_t)nw * (size_t)k;
             if (l == 0) {
                 ur[o] = ur[o] + uu[2] * xa[L1 * 3 * (size_t)k];
                 continue;
@@ -251,25 +253,22 @@ static void *spectra_worker(void *a)
         pthread_mutex_lock(&jb->lock);
         int k = ++jb->next;
         pthread_mutex_unlock(&jb->lock);
-        int j = 1 + (k - 1) * jb->jstride;
+        int j = 1 + jb->jofs + (k - 1) * jb->jstride;
         if (j > jb->jmax) break;
-        spectra_one(jb, j, arg->cnt);
+        spectra_one(jb, j, jb->ncol > 0 ? k - 1 : j - 1, arg->cnt);
     }
     return NULL;
 }
 
 /* (omega,l) loop + l-sum, yspec.f90:250-426.  For each omega_j the l-sum   */
 /* runs in increasing l, the reference's order for every (j,k).             */
-int yo_spectra(const yo_model *m, const yo_norms *n, const yo_params *p,
-               const yo_grid *g, yo_cd *ur, yo_cd *ut, yo_cd *up, int nthreads,
-               int lsub_lo, int lsub_hi, int jsub, yo_counts *cnt)
+static int spectra_run(const yo_model *m, const yo_norms *n, const yo_params *p,
+                       const yo_grid *g, yo_cd *ur, yo_cd *ut, yo_cd *up, int nthreads,
+                       int lo, int hi, int jofs, int jstride, int jmax, int ncol,
+                       yo_counts *cnt)
 {
-    int nr = p->nr, lmax = p->lmax, nw = g->nw;
-    int lo = p->lmin, hi = p->lmax;
-    if (lsub_hi >= 0) { lo = lsub_lo; hi = lsub_hi; }
-    int jmax = nw, jstride = 1;
-    if (jsub > 0 && jsub < nw) jmax = jsub;
-    if (jsub < 0) jstride = -jsub;
+    int nr = p->nr, lmax = p->lmax;
+    int nw = ncol > 0 ? ncol : g->nw;
     double *delta = (double *)malloc((size_t)nr * sizeof(double));
     double *azep = (double *)malloc((size_t)nr * sizeof(double));
     double *azst = (double *)malloc((size_t)nr * sizeof(double));
@@ -287,10 +286,11 @@ int yo_spectra(const yo_model *m, const yo_norms *n, const yo_params *p,
 
     int nth = nthreads > 0 ? nthreads : (int)sysconf(_SC_NPROCESSORS_ONLN);
     if (nth < 1) nth = 1;
-    if (nth > (jmax - 1) / jstride + 1) nth = (jmax - 1) / jstride + 1;
+    if (jmax <= jofs) nth = 1;
+    else if (nth > (jmax - 1 - jofs) / jstride + 1) nth = (jmax - 1 - jofs) / jstride + 1;
     yo_counts *tc = (yo_counts *)calloc((size_t)nth, sizeof(yo_counts));
     spectra_job job = {m, n, p, g, ur, ut, up, xa, xpa, xca, eia, lo, hi, jmax, jstride, 0,
-                       PTHREAD_MUTEX_INITIALIZER};
+                       jofs, ncol, PTHREAD_MUTEX_INITIALIZER};
     pthread_t *th = (pthread_t *)malloc((size_t)nth * sizeof(pthread_t));
     spectra_arg *args = (spectra_arg *)malloc((size_t)nth * sizeof(spectra_arg));
     for (int t = 0; t < nth; t++) {
@@ -313,6 +313,117 @@ int yo_spectra(const yo_model *m, const yo_norms *n, const yo_params *p,
         }
     }
     free(tc); free(delta); free(azep); free(azst); free(xa); free(xpa); free(xca); free(eia);
+    return 0;
+}
+
+int yo_spectra(const yo_model *m, const yo_norms *n, const yo_params *p,
+               const yo_grid *g, yo_cd *ur, yo_cd *ut, yo_cd *up, int nthreads,
+               int lsub_lo, int lsub_hi, int jsub, yo_counts *cnt)
+{
+    int lo = p->lmin, hi = p->lmax, nw = g->nw;
+    if (lsub_hi >= 0) { lo = lsub_lo; hi = lsub_hi; }
+    int jmax = nw, jstride = 1;
+    if (jsub > 0 && jsub < nw) jmax = jsub;
+    if (jsub < 0) jstride = -jsub;
+    return spectra_run(m, n, p, g, ur, ut, up, nthreads, lo, hi, 0, jstride, jmax, 0, cnt);
+}
+
+/* The spectra of a frequency shard: column c (0-based) holds omega_j with  */
+/* j = 1 + jofs + c jstride, c < count (the device's jofs/jstride fields).  */
+int yo_spectra_shard(const yo_model *m, const yo_norms *n, const yo_params *p,
+                     const yo_grid *g, int jofs, int jstride, int count, yo_cd *ur,
+                     yo_cd *ut, yo_cd *up, int nthreads)
+{
+    if (jofs < 0 || jstride < 1 || count < 1 || jofs + (count - 1) * jstride >= g->nw)
+        return YO_ERR_ARG;
+    return spectra_run(m, n, p, g, ur, ut, up, nthreads, p->lmin, p->lmax, jofs, jstride,
+                       jofs + (count - 1) * jstride + 1, count, NULL);
+}
+
+typedef struct {
+    const yo_model *m;
+    const yo_norms *n;
+    const yo_params *p;
+    const yo_grid *g;
+    int npair;
+    const int *ls, *js;
+    yo_cd *coef;
+    int next;
+    pthread_mutex_t lock;
+} coef_job;
+
+static void *coef_worker(void *a)
+{
+    coef_job *jb = (coef_job *)a;
+    for (;;) {
+        pthread_mutex_lock(&jb->lock);
+        int k = jb->next++;
+        pthread_mutex_unlock(&jb->lock);
+        if (k >= jb->npair) break;
+        yo_solve_pair(jb->m, jb->n, jb->p, jb->g, jb->ls[k], jb->js[k], jb->coef + 15 * (size_t)k,
+                      NULL);
+    }
+    return NULL;
+}
+
+/* yspec.f90:259-400 for a list of (l, omega_j) pairs, spread over threads */
+int yo_coef_list(const yo_model *m, const yo_norms *n, const yo_params *p, const yo_grid *g,
+                 int npair, const int *ls, const int *js, yo_cd *coef, int nthreads)
+{
+    for (int k = 0; k < npair; k++)
+        if (ls[k] < 0 || js[k] < 1 || js[k] > g->nw) return YO_ERR_ARG;
+    int nth = nthreads > 0 ? nthreads : (int)sysconf(_SC_NPROCESSORS_ONLN);
+    if (nth < 1) nth = 1;
+    if (nth > npair) nth = npair > 0 ? npair : 1;
+    coef_job job = {m, n, p, g, npair, ls, js, coef, 0, PTHREAD_MUTEX_INITIALIZER};
+    pthread_t *th = (pthread_t *)malloc((size_t)nth * sizeof(pthread_t));
+    for (int t = 0; t < nth; t++) pthread_create(&th[t], NULL, coef_worker, &job);
+    for (int t = 0; t < nth; t++) pthread_join(th[t], NULL);
+    free(th);
+    return 0;
+}
+
+/* The two-point solvers' outputs for one (omega, l): the solution at the   */
+/* receiver radius for unit jumps at the source radius (module_solver.f90).  */
+/* kind 0 tor_solver (2 x 2), 1 rad_solver_ng (2 x 2), 2 rad_solver_wg      */
+/* (2 x 2), 3 sph_solver / sph_solver_fic (6 x 4), 4 the no-gravity and 5   */
+/* the Cowling sph_solver variants (4 x 4).  out is row-major complex.      */
+int yo_green(const yo_model *m, const yo_norms *n, int kind, int l, double wr, double wi,
+             int ats, double rr, double rs, int ir, int is, yo_cd *out)
+{
+    yo_counts cnt;
+    memset(&cnt, 0, sizeof cnt);
+    yo_ctx c;
+    memset(&c, 0, sizeof c);
+    c.M = m;
+    c.N = n;
+    c.ats = (double)ats;
+    c.cnt = &cnt;
+    yo_cd w = wr + I_ * wi;
+    if (ir < 1 || is < 1 || ir > m->nsl || is > m->nsl || l < 0) return YO_ERR_ARG;
+    if (kind == 0) {
+        yo_cd y[2][2];
+        if (l < 2) return YO_ERR_ARG;
+        yo_tor_solver(&c, l, w, rr, rs, ir, is, y);
+        for (int a = 0; a < 2; a++) for (int b = 0; b < 2; b++) out[2 * a + b] = y[a][b];
+    } else if (kind == 1 || kind == 2) {
+        yo_cd y[2][2];
+        if (kind == 1) yo_rad_solver_ng(&c, w, rr, rs, ir, is, y);
+        else yo_rad_solver_wg(&c, w, rr, rs, ir, is, y);
+        for (int a = 0; a < 2; a++) for (int b = 0; b < 2; b++) out[2 * a + b] = y[a][b];
+    } else if (kind == 3) {
+        yo_cd y[6][4];
+        if (l < 1) return YO_ERR_ARG;
+        yo_sph_solver_g(&c, l, w, rr, rs, ir, is, m->fic, y);
+        for (int a = 0; a < 6; a++) for (int b = 0; b < 4; b++) out[4 * a + b] = y[a][b];
+    } else if (kind == 4 || kind == 5) {
+        yo_cd y[4][4];
+        if (l < 1) return YO_ERR_ARG;
+        yo_sph_solver_ngcow(&c, l, w, rr, rs, ir, is, m->fic, kind == 5, y);
+        for (int a = 0; a < 4; a++) for (int b = 0; b < 4; b++) out[4 * a + b] = y[a][b];
+    } else {
+        return YO_ERR_ARG;
+    }
     return 0;
 }
 

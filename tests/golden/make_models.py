@@ -1,6 +1,7 @@
-"""Generate the synthetic earth-model decks used by the tests and the benchmark.
+"""Generate the synthetic earth-model decks used by the tests and the benchmark,
+and copy the reference's own example inputs beside them.
 
-    python tests/golden/make_models.py [reference_examples_dir]
+    python tests/golden/make_models.py <reference examples directory>
 
 The decks are resamplings of the PREM decks bundled with the reference
 (examples/prem.200.isotropic, prem.200, prem.200.fic).  Each layer between
@@ -16,9 +17,13 @@ Outputs (committed; the generator only runs where the reference is mounted):
     model400.deck        400 knots, same structure               (config 5)
     model200_ocean.deck  200 knots, transversely isotropic, 3 km ocean
     model200_fic.deck    200 knots, fluid inner core, ocean
+    examples/            the reference's examples/input.txt and its five
+                         prem.200* decks, copied byte for byte (the only
+                         fixtures the reference ships)
 """
 from __future__ import annotations
 
+import shutil
 import sys
 from pathlib import Path
 
@@ -26,6 +31,10 @@ import numpy as np
 from scipy.interpolate import CubicSpline
 
 HERE = Path(__file__).resolve().parent
+
+
+EXAMPLES = ["input.txt", "prem.200", "prem.200.no", "prem.200.fic", "prem.200.isotropic",
+            "prem.200.noiso"]
 
 
 def read_deck(path: Path):
@@ -84,7 +93,10 @@ def write_deck(path: Path, title: str, tref: float, rows: np.ndarray, counts: li
 
 
 def main(argv: list[str]) -> int:
-    ex = Path(argv[1]) if len(argv) > 1 else Path("/root/reference/examples")
+    if len(argv) != 2:
+        print(__doc__)
+        return 2
+    ex = Path(argv[1])
     jobs = [("prem.200.isotropic", "model200.deck", 200, "synthetic200"),
             ("prem.200.isotropic", "model400.deck", 400, "synthetic400"),
             ("prem.200", "model200_ocean.deck", 200, "synthetic200_ocean"),
@@ -94,6 +106,10 @@ def main(argv: list[str]) -> int:
         new, counts = resample(rows, n)
         write_deck(HERE / dst, title, tref, new, counts)
         print(f"{dst}: {new.shape[0]} knots, layers {counts}")
+    (HERE / "examples").mkdir(exist_ok=True)
+    for name in EXAMPLES:
+        shutil.copyfile(ex / name, HERE / "examples" / name)
+        print(f"examples/{name}: copied")
     return 0
 
 

@@ -36,6 +36,18 @@ SCENARIOS = {
     "ocean_model": dict(model_file=str(W.GOLDEN / "model200_ocean.deck"), depth_r=3.0, ats=1),
     "fic_model": dict(model_file=str(W.GOLDEN / "model200_fic.deck"), depth_r=3.0, ats=1),
     "fic_nogravity": dict(model_file=str(W.GOLDEN / "model200_fic.deck"), depth_r=3.0, grav=0),
+    # sph_solver_cow_fic (module_solver.f90:1568-1740)
+    "fic_cowling": dict(model_file=str(W.GOLDEN / "model200_fic.deck"), depth_r=3.0, grav=1,
+                        ats=1),
+    # receiver below the source on the fluid-inner-core deck: the low-degree
+    # pairs start their solid minors inside the fluid inner core, as the
+    # reference's fic solvers do on that branch
+    "fic_receiver_below_source": dict(model_file=str(W.GOLDEN / "model200_fic.deck"),
+                                      depth_s=20.0, depth_r=250.0, ats=1, out=2, cor=1),
+    "fic_cowling_receiver_below": dict(model_file=str(W.GOLDEN / "model200_fic.deck"),
+                                       depth_s=20.0, depth_r=250.0, grav=1),
+    "fic_nogravity_receiver_below": dict(model_file=str(W.GOLDEN / "model200_fic.deck"),
+                                         depth_s=20.0, depth_r=250.0, grav=0, ats=1),
     "lmin_band": dict(lmin=5, lmax=35),
 }
 

@@ -240,3 +240,22 @@ def test_traces_match_independent_ifft(tmp_path):
         E_ = comp[1] * np.sin(azep[k]) + comp[2] * np.cos(azep[k])
         for c, want in ((1, comp[0]), (2, N_), (3, E_)):
             np.testing.assert_allclose(got[k, c], want, rtol=1e-11, atol=1e-11 * np.abs(want).max())
+
+
+def test_shard_and_pair_list_equal_full_runs(tmp_path):
+    # the sampled forms the size tests compare against are the same solves
+    p = W.config("c1", seed=3, lmax=30, fmax=6.0, f21=4.5, f22=5.5, dt=20.0, tout=40.0)[0]
+    p.receivers = p.receivers[:3]
+    P = yo.Problem(p.write(tmp_path / "s.in"))
+    nw = P.nw
+    full = P.spectra(nthreads=4)
+    count = len(range(2, nw, 3))
+    for a, b in zip(full, P.spectra_shard(2, 3, count, nthreads=3)):
+        np.testing.assert_array_equal(a[:, 2::3], b)
+    ls = np.array([0, 1, 2, 30, 17])
+    js = np.array([1, 2, nw, 5, 9])
+    got = P.coef_list(ls, js, nthreads=3)
+    for k in range(ls.size):
+        np.testing.assert_array_equal(got[k], P.coef(int(ls[k]), int(js[k])))
+    with pytest.raises(ValueError):
+        P.coef_list([3], [nw + 1])
