@@ -140,6 +140,11 @@ int yo_coef_list(const yo_model *m, const yo_norms *n, const yo_params *p,
 int yo_green(const yo_model *m, const yo_norms *n, int kind, int l, double wr,
              double wi, int ats, double rr, double rs, int ir, int is, yo_cd *out);
 
+/* Oracle-only convergence knob: every knot interval of the Runge-Kutta
+ * integration takes refine times the reference's step count (1 restores
+ * the reference's rule, module_int.f90:1903-1905).  Process-wide. */
+void yo_set_step_refine(int refine);
+
 /* Legendre/geometry table used by the l-sum (yspec.f90:144-174):
  * xa/xpa/xca are (lmax+1, 3, nr) column-major; delta/azst/azep are nr. */
 void yo_geometry(const yo_params *p, double *delta, double *azep,

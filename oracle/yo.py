@@ -91,6 +91,7 @@ def lib() -> C.CDLL:
         L.yo_green.argtypes = [C.POINTER(Model), C.POINTER(Norms), C.c_int, C.c_int, C.c_double,
                                C.c_double, C.c_int, C.c_double, C.c_double, C.c_int, C.c_int, _dp]
         L.yo_find_radius_index.argtypes = [C.POINTER(Model), C.c_double]
+        L.yo_set_step_refine.argtypes = [C.c_int]
         L.yo_geometry.argtypes = [C.POINTER(Params), _dp, _dp, _dp]
         L.yo_legendre_table.argtypes = [_dp, C.c_int, C.c_int, _dp, _dp, _dp]
         L.yo_traces.argtypes = [C.POINTER(Norms), C.POINTER(Params), C.POINTER(Grid), _dp, _dp, _dp,
@@ -241,6 +242,22 @@ class Problem:
 
     def run(self, nthreads: int = 0) -> np.ndarray:
         return self.traces(*self.spectra(nthreads=nthreads))
+
+
+class step_refine:
+    """Context manager: the oracle's integrations take `k` times the
+    reference's step count per knot interval (convergence checks only)."""
+
+    def __init__(self, k: int):
+        self.k = k
+
+    def __enter__(self):
+        lib().yo_set_step_refine(self.k)
+        return self
+
+    def __exit__(self, *exc):
+        lib().yo_set_step_refine(1)
+        return False
 
 
 def legendre(theta: float, l: int, m: int):

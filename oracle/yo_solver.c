@@ -379,6 +379,14 @@ static void rkck(yo_ctx *c, const yo_cd *y, const yo_cd *dydx, double x, double 
         yout[i] = y[i] + h * (c1 * dydx[i] + c3 * ak3[i] + c4 * ak4[i] + c6 * ak6[i]);
 }
 
+/* Step refinement for the oracle's own convergence checks: each knot       */
+/* interval takes (ns - 1) * refine steps instead of the reference's ns - 1. */
+/* 1 (the default) is the reference's rule.  Process-wide; not for use while */
+/* other threads run the oracle.                                             */
+static int g_step_refine = 1;
+
+void yo_set_step_refine(int refine) { g_step_refine = refine < 1 ? 1 : refine; }
+
 void yo_yint(yo_ctx *c, int i1, int i2, double r1, double r2, yo_cd *y, int n,
              yo_derivs derivs, int *scale)
 {
@@ -402,6 +410,7 @@ void yo_yint(yo_ctx *c, int i1, int i2, double r1, double r2, yo_cd *y, int n,
         c->il = i;
         double drr = steps(c, i);
         int ns = 2 + (int)floor(fabs(rr2 - rr1) / drr);
+        if (g_step_refine > 1) ns = (ns - 1) * g_step_refine + 1;
         drr = (rr2 - rr1) / (double)(ns - 1);
         for (int j = 1; j <= ns - 1; j++) {
             double rr = rr1 + (double)(j - 1) * drr;
@@ -1081,9 +1090,13 @@ void yo_sph_solver_g(yo_ctx *c, int l, yo_cd w, double rr, double rs, int ir, in
     rt = m->r[i1];
     if (i1 == 1 && (up || fic)) rt = fmin(0.1 * c->dr, 0.1 * m->r[2]);
     if (i1 >= it) { i1 = it - 1; rt = m->r[i1]; }
-    /* the receiver-below-source branch of sph_solver_fic starts a solid */
-    /* minor inside the (fluid) inner core, module_solver.f90:1323-1332    */
-    int ic_fluid_start = fic && up;
+    /* A fluid inner core starts from the fluid minor on both branches.   */
+    /* The receiver-below-source branch of sph_solver_fic                  */
+    /* (module_solver.f90:1323-1332) starts a solid minor there instead:   */
+    /* with mu = 0 the shear wavenumber is infinite, bfs's continued       */
+    /* fraction never converges and the reference does not return.  The   */
+    /* receiver-above branch's fluid start (:1252-1256) is taken for both. */
+    int ic_fluid_start = fic;
     if (i1 <= m->nic) {
         if (ic_fluid_start) {
             sph_minor_fluid_start(c, i1, rt, mf1);

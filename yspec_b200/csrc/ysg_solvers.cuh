@@ -256,12 +256,16 @@ __device__ inline void sph_solver_g(Ctx& c, double rr, double rs, int ir, int is
     if (i1 == 1 && (up || fic)) rt = fmin(0.1 * c.dr, 0.1 * kn[2].r);
     if (i1 >= it) { i1 = it - 1; rt = kn[i1].r; }
     if (i1 <= mh->nic) {
-        if (fic && up) {
+        if (fic) {
+            // A fluid inner core starts from the fluid minor on both branches.
+            // The reference's receiver-below-source branch of sph_solver_fic
+            // (:1323-1332) starts a solid minor there instead; with mu = 0 its
+            // shear wavenumber is infinite and bfs's continued fraction never
+            // converges, so the reference does not return for these pairs.
+            // The receiver-above branch's fluid start (:1252-1256) is taken for both.
             sph_minor_fluid_start(c, i1, rt, mf);
             yint<MinorFluidG>(c, i1, mh->noc, rt, kn[mh->noc].r, mf, &scale1);
         } else {
-            // the receiver-below-source branch of sph_solver_fic starts a
-            // solid minor inside the fluid inner core (:1323-1332), kept
             sph_minor_solid_start(c, i1, rt, ms1);
             yint<MinorSolidG>(c, i1, mh->nic, rt, kn[mh->nic].r, ms1, &scale1);
             s2f(ms1, mf);
