@@ -166,7 +166,12 @@ int ysg_get_stream(ysg_handle *h, void **stream);
  * (YSG_ERR_LIMIT beyond).  All calls share that array: calls that overlap
  * on the GPU race and must be serialised.  The first call on each device
  * looks up the array's device address and should come before any stream
- * capture. */
+ * capture; the address is cached per device for the primary context, so the
+ * entry point is not for use after cudaDeviceReset or from a separate
+ * driver-API context.  nt must be a power of two >= 8, as for
+ * ysg_event_traces.  An error pending from earlier work on the calling
+ * thread is cleared on entry; a failure of this call is described by
+ * ysg_last_cuda_error(). */
 int ysg_traces_noalloc(const ysg_time *tm, const double *d_ur, const double *d_ut,
                        const double *d_up, const double *d_azep, double *d_out, int *nout,
                        void *stream);

@@ -12,6 +12,7 @@ import ctypes as C
 import numpy as np
 import pytest
 
+import yo
 from conftest import rel_l2
 from yspec_b200 import Engine, Event, Model, Params, native as N, workloads as W
 
@@ -68,6 +69,10 @@ def test_noalloc_traces_equal_allocating_path(workdir, cfg):
             for c in range(1, 4):
                 err = rel_l2(got[k, c], want[k, c])
                 assert err <= TOL, f"call {call}: receiver {k} comp {c}: {err:.3e}"
+    ref = yo.Problem(pf).run(nthreads=4)               # and directly against the oracle
+    for k in range(ev.nr):
+        for c in range(1, 4):
+            assert rel_l2(got[k, c], ref[k, c]) <= TOL, (k, c)
 
 
 def test_noalloc_rejects_oversize():
@@ -75,3 +80,42 @@ def test_noalloc_rejects_oversize():
     f = _bind()
     rc = f(C.byref(t), 1, 1, 1, 1, 1, None, None)      # pointers are never touched
     assert rc == 7                                      # YSG_ERR_LIMIT
+
+
+def test_noalloc_rejects_short_transforms():
+    t = N.YsgTime(nt=4, i1=2, i2=3, nr=1, df=1.0, dt=1.0, ep=1.0, tout=1.0)
+    rc = _bind()(C.byref(t), 1, 1, 1, 1, 1, None, None)
+    assert rc == 1                                      # YSG_ERR_ARG, as ysg_event_traces
+
+
+def test_noalloc_many_receivers_short_transform():
+    """nt = 8 fits 43,690 receivers of rows in the array but only 21,845 in
+    one launch's grid (three rows per receiver): 22,000 receivers run in
+    grid-sized chunks, and receivers either side of a chunk boundary equal a
+    run of those receivers alone."""
+    import torch
+
+    dev = torch.device("cuda", 0)
+    nr, nt, i1, i2 = 22000, 8, 2, 4
+    nw = i2 - i1 + 1
+    rng = np.random.default_rng(3)
+    spec = [torch.from_numpy(rng.standard_normal((nr, nw, 2))).to(dev) for _ in range(3)]
+    az = torch.from_numpy(rng.uniform(0, 2 * np.pi, nr)).to(dev)
+    t = N.YsgTime(nt=nt, i1=i1, i2=i2, nr=nr, df=0.01, dt=5.0, ep=0.002, tout=30.0,
+                  f11=0.0, f12=0.0, f21=0.0, f22=0.0, t_norm=1.0, amp_norm=1.0)
+    f = _bind()
+    n = C.c_int()
+    rows = N.lib().ysg_trace_rows(C.byref(t))
+    out = torch.zeros((nr, 4, rows), dtype=torch.float64, device=dev)
+    rc = f(C.byref(t), *[x.data_ptr() for x in spec], az.data_ptr(), out.data_ptr(), C.byref(n), None)
+    assert rc == 0
+    torch.cuda.synchronize()
+    pick = [0, 21844, 21845, 21999]
+    t.nr = len(pick)
+    sub = [x[pick].contiguous() for x in spec]
+    out1 = torch.zeros((len(pick), 4, rows), dtype=torch.float64, device=dev)
+    rc = f(C.byref(t), *[x.data_ptr() for x in sub], az[pick].contiguous().data_ptr(),
+           out1.data_ptr(), C.byref(n), None)
+    assert rc == 0
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(out[pick].cpu().numpy(), out1.cpu().numpy())

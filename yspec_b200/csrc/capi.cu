@@ -140,12 +140,14 @@ struct ysg_handle {
 // the failing call's source line for ysg_last_cuda_error().
 thread_local char g_cuda_err[160] = "";
 
-int cuda_fail(cudaError_t e, int line)
+int ysg_cuda_fail_at(cudaError_t e, const char* file, int line)
 {
-    std::snprintf(g_cuda_err, sizeof g_cuda_err, "%s (%s) at capi.cu:%d", cudaGetErrorName(e),
-                  cudaGetErrorString(e), line);
+    std::snprintf(g_cuda_err, sizeof g_cuda_err, "%s (%s) at %s:%d", cudaGetErrorName(e),
+                  cudaGetErrorString(e), file, line);
     return YSG_ERR_CUDA;
 }
+
+int cuda_fail(cudaError_t e, int line) { return ysg_cuda_fail_at(e, "capi.cu", line); }
 
 #define CK(x)                                                  \
     do {                                                       \

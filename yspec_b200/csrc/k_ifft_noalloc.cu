@@ -20,7 +20,11 @@
 //
 // The device address of the array is looked up with cudaGetSymbolAddress
 // on the first call made on each device (with that device current) and
-// cached; that first call should come before any stream capture.  The
+// cached by device ordinal; that first call should come before any stream
+// capture.  The cache assumes the device's primary context, the one the
+// runtime API uses, for the life of the process: after cudaDeviceReset, or
+// from a separate driver-API context on the same device, the cached address
+// is stale and this entry point must not be used.  The
 // taper, FFT twiddles, e^{eps t} and the rotation angles are formed on the
 // device, so apart from the launches nothing is allocated or copied.
 #include <mutex>
@@ -30,9 +34,13 @@
 #include "yspec_gpu.h"
 #include "ysg_cplx.cuh"
 
+// Records a CUDA failure for ysg_last_cuda_error() (capi.cu).
+int ysg_cuda_fail_at(cudaError_t e, const char* file, int line);
+
 namespace {
 
 constexpr size_t kScratchComplex = (size_t)1 << 20;
+constexpr int kMaxRowsY = 65535;        // grid.y limit: 3 rows per receiver
 
 }  // namespace
 
@@ -171,11 +179,15 @@ cd* g_addr[128] = {};
 int scratch_address(cd** p)
 {
     int dev = -1;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 128) return YSG_ERR_CUDA;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return ysg_cuda_fail_at(e, "k_ifft_noalloc.cu", __LINE__);
+    if (dev < 0 || dev >= 128) return YSG_ERR_CUDA;
     std::lock_guard<std::mutex> lk(g_mu);
     if (!g_addr[dev]) {
         void* ptr = nullptr;
-        if (cudaGetSymbolAddress(&ptr, g_trace_scratch) != cudaSuccess || !ptr) return YSG_ERR_CUDA;
+        e = cudaGetSymbolAddress(&ptr, g_trace_scratch);
+        if (e != cudaSuccess) return ysg_cuda_fail_at(e, "k_ifft_noalloc.cu", __LINE__);
+        if (!ptr) return YSG_ERR_CUDA;
         g_addr[dev] = static_cast<cd*>(ptr);
     }
     *p = g_addr[dev];
@@ -190,13 +202,17 @@ extern "C" int ysg_traces_noalloc(const ysg_time* tm, const double* d_ur, const 
 {
     if (!tm) return YSG_ERR_ARG;
     const int n = tm->nt, nr = tm->nr;
-    if (n < 4 || (n & (n - 1)) || tm->i1 < 1 || tm->i2 < tm->i1 || tm->i2 > n || nr < 0)
+    // the same argument rules as the allocating time-series stage (k_ifft.cu)
+    if (n < 8 || (n & (n - 1)) || tm->i1 < 1 || tm->i2 < tm->i1 || tm->i2 > n || nr < 0)
         return YSG_ERR_ARG;
     if (nr > 0 && (!d_ur || !d_ut || !d_up || !d_azep || !d_out)) return YSG_ERR_ARG;
     if ((size_t)3 * n > kScratchComplex) return YSG_ERR_LIMIT;   // one receiver must fit
     const int rows_out = ysg_trace_rows(tm);
     if (nout) *nout = rows_out;
     if (nr == 0) return YSG_OK;
+    // an error left pending by earlier work on this thread is cleared here,
+    // so the check after the launches reports this call's own failures
+    (void)cudaGetLastError();
     cd* scr = nullptr;
     int rc = scratch_address(&scr);
     if (rc) return rc;
@@ -223,7 +239,8 @@ extern "C" int ysg_traces_noalloc(const ysg_time* tm, const double* d_ur, const 
     a.w3 = tm->f21;
     a.w4 = tm->f22;
     a.filter = !(a.w1 == 0.0 && a.w2 == 0.0 && a.w3 == 0.0 && a.w4 == 0.0);
-    const int per_chunk = (int)(kScratchComplex / ((size_t)3 * n));   // receivers per chunk
+    int per_chunk = (int)(kScratchComplex / ((size_t)3 * n));   // receivers per chunk
+    if (per_chunk > kMaxRowsY / 3) per_chunk = kMaxRowsY / 3;
     const int tile = n < kTile ? n : kTile;
     const int B2 = n / a.b1;
     int G = 512 / B2;
@@ -241,7 +258,8 @@ extern "C" int ysg_traces_noalloc(const ysg_time* tm, const double* d_ur, const 
         k_noalloc_a<<<dim3(n / tile, 3 * nk), tile / 2, 0, st>>>(a, ur, ut, up, scr);
         k_noalloc_b<<<dim3(a.b1 / G, 3 * nk), threads, (size_t)G * B2 * sizeof(cd), st>>>(a, G, scr, d_out);
         k_noalloc_rotate<<<dim3((rows_out + 255) / 256, nk), 256, 0, st>>>(a, nk, d_azep, d_out);
-        if (cudaGetLastError() != cudaSuccess) return YSG_ERR_CUDA;
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return ysg_cuda_fail_at(e, "k_ifft_noalloc.cu", __LINE__);
     }
     return YSG_OK;
 }
