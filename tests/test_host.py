@@ -183,3 +183,29 @@ def test_run_batch_reports_failing_file(workdir):
     assert rc == 101 and failed.value == 1
     rc = N.lib().ysh_run_batch(0, files, 0, 0, C.byref(failed))
     assert rc != 0
+
+
+def test_fortran_module_matches_the_c_abi():
+    """include/yspec_gpu.f90 (no Fortran compiler here): every bind(C) name is
+    exported by the library, and each derived type lists the C struct's
+    fields in the C order (ctypes mirrors of include/yspec_gpu.h)."""
+    import re
+
+    from yspec_b200 import native as N
+
+    src = (ROOT / "include" / "yspec_gpu.f90").read_text()
+    names = re.findall(r'bind\(C, name="(\w+)"\)', src)
+    assert len(names) >= 12
+    lib = N.lib()
+    for n in names:
+        if n != "strlen":
+            assert hasattr(lib, n), n
+    for ftype, ctype in (("ysg_model", N.YsgModel), ("ysg_event", N.YsgEvent), ("ysg_time", N.YsgTime)):
+        body = re.search(rf"type, bind\(C\) :: {ftype}\n(.*?)end type", src, re.S).group(1)
+        fields = []
+        for line in body.splitlines():
+            line = line.split("!")[0]
+            if "::" in line:
+                fields += [re.sub(r"\(.*\)", "", f).strip() for f in line.split("::")[1].split(",")]
+        want = [f.rstrip("_") for f, _ in ctype._fields_]
+        assert fields == want, (ftype, fields, want)

@@ -157,7 +157,8 @@ def _model_function():
     class _ModelFn(torch.autograd.Function):
         @staticmethod
         def forward(ctx, rho, vp, vs, mm, syn):
-            G = syn._greens(rho, vp, vs)
+            # the solves run on the engine's GPU; results follow the inputs' device
+            G = syn._greens(rho, vp, vs).to(device=mm.device, dtype=mm.dtype)
             ctx.save_for_backward(rho, vp, vs, mm, G)
             ctx.syn = syn
             return torch.einsum("i,iktn->ktn", mm, G) / syn.moment_norm
@@ -167,7 +168,7 @@ def _model_function():
             rho, vp, vs, mm, G = ctx.saved_tensors
             syn = ctx.syn
             g_mm = torch.einsum("ktn,iktn->i", grad, G) / syn.moment_norm
-            g = syn._knot_gradient(rho, vp, vs, mm, grad)
+            g = syn._knot_gradient(rho, vp, vs, mm, grad).to(device=rho.device, dtype=rho.dtype)
             n = syn.km.nknot
             return g[:n], g[n:2 * n], g[2 * n:], g_mm, None
 
