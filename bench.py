@@ -13,13 +13,16 @@ Multi-GPU: every rank runs its own copy of the event (replicas, weak scaling;
 the pairs are independent, no collective is on the data path).  Timing is on
 the device with CUDA events on the engine's stream, max over ranks.
 The reference arm (--impl reference) times the CPU restatement of the
-reference path on all host cores over a bounded frequency sample.
+reference path on all host cores over the whole event, every step.
 
 On one GPU the line also carries "batched_vs_plain": the 64-event uneven
 batch (fmax U(10, 50) mHz, lmax 15 fmax, depth U(0, 700) km, 1-1000
 receivers) run once as one batched solve launch inside a CUDA graph and
 once event by event with the plain one-thread-per-pair solver, one launch
-per event.
+per event; "c5_batch": the largest configuration (16 events x 10,000
+receivers) as one batch; "parity": the timed event's traces against the
+oracle's; "stage_roofline": the l-sum and time-series stages against their
+peaks.
 """
 from __future__ import annotations
 
@@ -109,8 +112,9 @@ def batch_compare(local: int, reps: int = 2) -> dict:
     return res
 
 
-def cpu_sample(pf: Path, stride: int, threads: int):
-    """Oracle on every stride-th frequency of the event: (pairs, seconds)."""
+def cpu_sample(pf: Path, stride: int, threads: int, keep: bool = False):
+    """Oracle on every stride-th frequency of the event: (pairs, seconds, nw, L),
+    and with keep=True also the oracle problem and its spectra."""
     sys.path.insert(0, str(ROOT / "oracle"))
     import yo  # the CPU restatement of the reference path (test oracle / baseline only)
 
@@ -118,9 +122,30 @@ def cpu_sample(pf: Path, stride: int, threads: int):
     nj = (P.nw - 1) // stride + 1
     L = P.params.lmax - P.params.lmin + 1
     t0 = time.perf_counter()
-    P.spectra(nthreads=threads, jsub=-stride)
+    spec = P.spectra(nthreads=threads, jsub=-stride)
     dt = time.perf_counter() - t0
+    if keep:
+        return nj * L, dt, P.nw, L, P, spec
     return nj * L, dt, P.nw, L
+
+
+def trace_parity(got, P, spec) -> dict:
+    """Largest relative L2 error per trace of the device traces (nr, 4, nout)
+    against the oracle's traces of the same event, and whether the time
+    columns are equal."""
+    import numpy as np
+
+    want = P.traces(*spec)
+    worst = 0.0
+    for k in range(want.shape[0]):
+        for c in range(1, 4):
+            den = float(np.linalg.norm(want[k, c]))
+            num = float(np.linalg.norm(got[k, c] - want[k, c]))
+            worst = max(worst, num / den if den > 0 else num)
+    return {"max_rel_l2_per_trace": worst, "bar": 1e-9, "ok": bool(worst <= 1e-9),
+            "time_column_equal": bool(np.array_equal(got[:, 0], want[:, 0])),
+            "checked": "traces of the timed end-to-end run against the oracle's traces of the "
+                       "whole event (every receiver and component)"}
 
 
 class Clocks:
@@ -236,6 +261,52 @@ def gradient_check(local: int) -> dict:
             "fd_rel_err": max(errs), "fd_check": "central differences along 2 random directions, step 1e-3"}
 
 
+def measured_peaks() -> dict:
+    """The pool's measured HBM copy bandwidth (GB/s), if the file is present."""
+    try:
+        d = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+        return {"hbm_gbs": float(d["hbm_gbs"]), "source": "MEASURED_PEAKS.json (measured)"}
+    except Exception:
+        return {"hbm_gbs": 6650.0, "source": "fallback: earlier measurement on this pool"}
+
+
+def c5_batch(local: int) -> dict:
+    """c5: 16 events x 10,000 receivers on the 400-knot model, lmax 1500,
+    100 mHz, 120 min at 0.5 s, as one ysg_batch_run (one solve stage over
+    39.4 M pairs, per-event l-sum and time series, one CUDA graph).  The
+    traces (74 GB) exceed the host's memory beside everything else, so every
+    event writes into one shared host buffer; all device-to-host copies are
+    still made and timed.  One warm-up batch, then one timed batch."""
+    import numpy as np
+    from yspec_b200 import Engine, Event, Model, Params, workloads as W
+
+    tmp = Path(tempfile.mkdtemp(prefix="ysc5_"))
+    ps = W.config("c5", seed=0)
+    model = Model(ps[0].model_file)
+    t0 = time.perf_counter()
+    evs = [Event(model, Params(p.write(tmp / f"e{i}.in"))) for i, p in enumerate(ps)]
+    setup_s = time.perf_counter() - t0
+    eng = Engine(local, solver="batched")
+    eng.set_schedule(2)
+    eng.upload(model)
+    buf = np.zeros((evs[0].nr, 4, evs[0].nout()))
+    eng.batch_run(evs, outs=[buf] * len(evs))           # warm-up: graph capture
+    t0 = time.perf_counter()
+    eng.batch_run(evs, outs=[buf] * len(evs))
+    wall = time.perf_counter() - t0
+    ms = eng.timings()
+    pairs = float(sum(e.L * e.nw for e in evs))
+    nrec = sum(e.nr for e in evs)
+    return {"workload": "c5: 16 events x 10,000 receivers, 400-knot model, lmax 1500, 100 mHz, "
+                        "120 min @ 0.5 s, attenuation + self-gravitation, one batch",
+            "pairs": int(pairs), "traces": nrec,
+            "stage_ms": dict(zip(["legendre", "solve", "lsum", "ifft"], ms)),
+            "wall_s": wall, "traces_per_s": nrec / wall, "solves_per_s_device": pairs / (ms[1] / 1e3),
+            "event_setup_s": setup_s,
+            "timing": "wall clock of one ysg_batch_run after a warm-up batch, including the "
+                      "device-to-host copy of every event's traces (73.7 GB)"}
+
+
 def run_reference(args) -> None:
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -243,7 +314,7 @@ def run_reference(args) -> None:
     threads = os.cpu_count() or 1
     with tempfile.TemporaryDirectory() as d:
         _, pf = make_event(Path(d))
-        stride = 8                                   # 103 of 820 frequencies per step
+        stride = 1                                   # the whole event, every step
         for _ in range(args.warmup):
             cpu_sample(pf, stride, threads)
         times, pairs = [], 0
@@ -253,13 +324,14 @@ def run_reference(args) -> None:
             pairs = n
     total = sum(times)
     value = pairs * args.steps / total
-    sample = f"every {stride}th of {nw} frequencies x all {L} degrees ({pairs} pairs) per step"
+    sample = f"the whole event per step: {nw} frequencies x {L} degrees ({pairs} pairs)"
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded PREM-like model, receivers, moment tensor)",
-        "config": {"workload": WORKLOAD, "pairs_per_event": 615820, "sample": sample},
+        "config": {"workload": WORKLOAD, "pairs_per_event": pairs, "sample": sample,
+                   "same_config": True},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
                          "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -360,6 +432,7 @@ def run_b200(args) -> None:
     barrier()
     e_ms = allmax(e_ms)
     e2e = world * pairs * args.steps / (e_ms / 1e3)
+    traces_last = out_pinned.numpy().reshape(nr, 4, nout).copy()
 
     if rank == 0:
         mean_solve = statistics.mean(solve_ms)
@@ -379,7 +452,7 @@ def run_b200(args) -> None:
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h), "ms_per_step": e_ms / args.steps},
             "gpu_launches": launches,
-            "roofline": {"bound": "tensor", "pipe": "fp64 (CUDA-core FMA rate = FP64 tensor rate on B200)",
+            "roofline": {"bound": "fp64", "pipe": "FP64 CUDA-core FMA pipe (the radial solves use no tensor cores)",
                          "kernel": "k_solve_batched" if args.solver == "batched" else "k_solve_plain",
                          "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak if peak else None,
@@ -389,13 +462,34 @@ def run_b200(args) -> None:
                              "k_solve_batched" if args.solver == "batched" else "k_solve_plain")},
             "clocks": clk,
         }
+        st = dict(zip(["legendre", "solve", "lsum", "ifft"], eng.timings()))
+        hbm = measured_peaks()
+        L, nw, nt = ev.L, ev.nw, ev.tm.nt
+        lsum_flops = 4.0 * nw * nr * (22 * (L - 2) + 9)
+        ifft_bytes = 3.0 * nr * (nw * 16 + nout * 8)
+        ifft_flops = 3.0 * nr * 5.0 * nt * (nt.bit_length() - 1)
+        line["stage_roofline"] = {
+            "lsum": {"kernel": "k_lsum_mma", "bound": "fp64 tensor (DMMA)",
+                     "achieved_tflops": lsum_flops / (st["lsum"] / 1e3) / 1e12,
+                     "frac_of_fp64_peak": lsum_flops / (st["lsum"] / 1e3) / 1e12 / peak,
+                     "flops": lsum_flops},
+            "ifft": {"kernels": "k_ifft_a2, k_ifft_b2, k_rotate",
+                     "achieved_gbs": ifft_bytes / (st["ifft"] / 1e3) / 1e9,
+                     "frac_of_hbm": ifft_bytes / (st["ifft"] / 1e3) / 1e9 / hbm["hbm_gbs"],
+                     "hbm_peak_gbs": hbm["hbm_gbs"], "hbm_peak_source": hbm["source"],
+                     "fft_tflops": ifft_flops / (st["ifft"] / 1e3) / 1e12,
+                     "fft_frac_of_fp64_peak": ifft_flops / (st["ifft"] / 1e3) / 1e12 / peak,
+                     "bytes": ifft_bytes, "fft_flops_5nlog2n": ifft_flops}}
         if world == 1 and not args.no_batch:
             line["batched_vs_plain"] = batch_compare(local)
         if world == 1 and not args.no_grad:
             line["gradient"] = gradient_check(local)
+        if world == 1 and not args.no_c5:
+            line["c5_batch"] = c5_batch(local)
         if world == 1 and not args.no_cpu:
             threads = os.cpu_count() or 1
-            n, dt, nw, L = cpu_sample(pf, 1, threads)
+            n, dt, nw, L, P, spec = cpu_sample(pf, 1, threads, keep=True)
+            line["parity"] = trace_parity(traces_last, P, spec)
             n1, dt1, _, _ = cpu_sample(pf, 41, 1)
             line["cpu_baseline"] = {"value": n / dt, "unit": UNIT, "cores": threads, "kind": "port",
                                     "sample": f"the whole event: {nw} frequencies x {L} degrees "
@@ -420,6 +514,7 @@ def main() -> int:
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-vs-plain comparison")
     ap.add_argument("--no-grad", action="store_true", help="skip the c4 model-gradient timing")
+    ap.add_argument("--no-c5", action="store_true", help="skip the c5 16-event batch")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

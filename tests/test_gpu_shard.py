@@ -62,3 +62,76 @@ def test_sharded_event_path_single_rank(workdir):
                 assert rel_l2(got[k, c], want[k, c]) <= 1e-9
     finally:
         dist.destroy_process_group()
+
+
+def _shard_worker(rank, world, port, pf, model_file, out):
+    import sys
+    from datetime import timedelta
+
+    import torch.distributed as dist
+    from conftest import ROOT
+
+    sys.path.insert(0, str(ROOT))
+    from yspec_b200 import Engine, Event, Model, Params, shard as S
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=120))
+    try:
+        m = Model(model_file)
+        ev = Event(m, Params(pf))
+        eng = Engine(0)
+        eng.set_schedule(0)
+        eng.upload(m)
+        got = S.run_event_sharded(eng, ev)
+        if rank == 0:
+            np.save(out, got)
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_sharded_event_two_ranks_share_one_gpu(workdir, world):
+    """run_event_sharded with world ranks (gloo, one process each, all on
+    cuda:0): frequency shards, the receiver exchange, per-rank time series of
+    its receivers and the row gather reproduce the one-rank sharded run bit
+    for bit, and the one-GPU traces to 1e-9.  The ranks' kernels never wait
+    on one another: the exchange runs on host copies."""
+    import torch.multiprocessing as mp
+    import torch.distributed as dist
+    from datetime import timedelta
+
+    p = W.config("c1", seed=8, lmax=30, fmax=5.0, f21=3.5, f22=4.5, dt=20.0, tout=40.0, ats=1)[0]
+    p.receivers = W.sphere_points(np.random.default_rng(4), 7)
+    pf = p.write(workdir / "sh2.in")
+    port = _port()
+    out = str(workdir / "sharded.npy")
+    mp.start_processes(_shard_worker, args=(world, port, str(pf), p.model_file, out), nprocs=world,
+                       join=True, start_method="spawn")
+    got = np.load(out)
+    m = Model(p.model_file)
+    ev = Event(m, Params(pf))
+    eng = Engine(0)
+    eng.set_schedule(0)
+    eng.upload(m)
+    want = eng.run(ev)
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(_port())
+    dist.init_process_group("gloo", rank=0, world_size=1, timeout=timedelta(seconds=60))
+    try:
+        one = shard.run_event_sharded(eng, ev)
+    finally:
+        dist.destroy_process_group()
+    np.testing.assert_array_equal(got, one)
+    for k in range(ev.nr):
+        for c in range(1, 4):
+            assert rel_l2(got[k, c], want[k, c]) <= 1e-9
+
+
+def _port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    return port
