@@ -85,6 +85,10 @@ void ysh_free_event(ysh_event *e);
  * nout lines of four E15.6 fields), byte-identical to the reference; the
  * receivers' files are formatted and written on several threads. */
 int ysh_write_traces(const char *pref_out, const double *out, int nout, int nr);
+
+/* One E15.6 field exactly as the writer forms it (15 characters and a NUL):
+ * the text gfortran's E15.6 edit descriptor gives for x. */
+void ysh_format_e15_6(double x, char field[16]);
 /* The whole program: parameter file -> traces on `device`.  When out is
  * non-NULL it receives a malloc'd (nout, 4, nr) array (free with
  * ysh_free). When write_files is nonzero the per-receiver files are written

@@ -209,3 +209,46 @@ def test_fortran_module_matches_the_c_abi():
                 fields += [re.sub(r"\(.*\)", "", f).strip() for f in line.split("::")[1].split(",")]
         want = [f.rstrip("_") for f, _ in ctype._fields_]
         assert fields == want, (ftype, fields, want)
+
+
+def _e15_6_reference(x: float) -> str:
+    """gfortran's E15.6 as the reference writes it: [-]0.dddddd E+ee, digits
+    from the correctly rounded %.5e of |x|."""
+    import math
+
+    ax = abs(x)
+    if ax == 0.0:
+        dig, e10 = "000000", 0
+    else:
+        t = f"{ax:.5e}"
+        dig = t[0] + t[2:7]
+        e10 = int(t.split("e")[1]) + 1
+    sg = "-" if math.copysign(1.0, x) < 0 else ""
+    ae = abs(e10)
+    body = (f"{sg}0.{dig}E{'-' if e10 < 0 else '+'}{ae:02d}" if ae <= 99
+            else f"{sg}0.{dig}{'-' if e10 < 0 else '+'}{ae:03d}")
+    return f"{body:>15.15}"
+
+
+def test_e15_6_formatter_exact():
+    """The writer's formatter (digits without snprintf where the rounding is
+    certain) against correctly rounded %.5e on values of every magnitude,
+    exact ties, values next to rounding boundaries and powers of ten."""
+    import struct
+
+    from yspec_b200 import native as N
+
+    rng = np.random.default_rng(5)
+    vals = list(rng.standard_normal(20000) * 10.0 ** rng.uniform(-40, 40, 20000))
+    vals += list(rng.standard_normal(20000) * 10.0 ** rng.integers(-12, 4, 20000))
+    vals += [0.0, -0.0, 1.0, -1.0, 5e-324, 2.2250738585072014e-308, 1.7976931348623157e308,
+             1234565.0, 1234575.0, 12345650.0, 0.5, 2.5e-5, 999999.5, 9999995.0, 99999.95]
+    for e in range(-30, 31):
+        for m in (1.0, 9.999995, 9.9999949999, 9.99999500001, 1.0000005, 1.00000049999, 1.2345650):
+            v = m * 10.0 ** e
+            vals += [v, -v, np.nextafter(v, 0.0), np.nextafter(v, np.inf)]
+    buf = C.create_string_buffer(16)
+    for x in vals:
+        x = float(x)
+        N.lib().ysh_format_e15_6(x, buf)
+        assert buf.value.decode() == _e15_6_reference(x), (x, struct.pack("<d", x).hex())

@@ -475,9 +475,93 @@ void e15_6(double x, char* field)
     std::snprintf(field, 16, "%15.15s", body);
 }
 
+// Powers of ten that a double holds exactly.
+const double kPow10[23] = {1e0,  1e1,  1e2,  1e3,  1e4,  1e5,  1e6,  1e7,  1e8,  1e9,  1e10, 1e11,
+                           1e12, 1e13, 1e14, 1e15, 1e16, 1e17, 1e18, 1e19, 1e20, 1e21, 1e22};
+
+// The six significant digits D (100000 <= D < 1000000) and the exponent
+// e10 of an E15.6 field for a finite ax > 0, formed without snprintf:
+// y = ax 10^(5 - E) with E = floor(log10 ax) takes one correctly rounded
+// product or quotient by an exact power of ten, so |y - exact| <= 1.2e-10;
+// D = round(y) is then certain unless the exact value lies within 1e-6 of
+// a rounding boundary (a half-integer, 1e5 or 1e6), or 10^(5 - E) is not
+// exact.  Those cases return false and take the snprintf path, so the
+// field is the same text either way.
+bool e15_digits(double ax, int* digits, int* e10)
+{
+    int E = (int)std::floor(std::log10(ax));
+    double y = 0.0;
+    for (int pass = 0; pass < 3; pass++) {
+        const int k = 5 - E;
+        if (k >= 0 && k <= 22) y = ax * kPow10[k];
+        else if (k < 0 && k >= -22) y = ax / kPow10[-k];
+        else return false;
+        if (y < 1e5) E--;
+        else if (y >= 1e6) E++;
+        else break;
+        if (pass == 2) return false;
+    }
+    if (y < 1e5 + 1e-4 || y > 1e6 - 0.5 - 1e-6) return false;
+    const double fl = std::floor(y), fr = y - fl;
+    if (std::fabs(fr - 0.5) < 1e-6) return false;
+    int d = (int)fl + (fr > 0.5 ? 1 : 0);
+    *digits = d;
+    *e10 = E + 1;
+    return true;
+}
+
+// e15_6 with the digits formed by e15_digits where it can.
+void e15_6_fast(double x, char* field)
+{
+    const double ax = std::fabs(x);
+    int d = 0, e10 = 0;
+    if (ax == 0.0) {
+        d = -1;                                        // all-zero digits, exponent 0
+    } else if (!(std::isfinite(ax) && e15_digits(ax, &d, &e10))) {
+        e15_6(x, field);
+        return;
+    }
+    char body[16];
+    int n = 0;
+    if (std::signbit(x)) body[n++] = '-';
+    body[n++] = '0';
+    body[n++] = '.';
+    if (d < 0) {
+        for (int i = 0; i < 6; i++) body[n++] = '0';
+    } else {
+        for (int i = 5; i >= 0; i--) {
+            body[n + i] = (char)('0' + d % 10);
+            d /= 10;
+        }
+        n += 6;
+    }
+    const int ae = e10 < 0 ? -e10 : e10;
+    if (ae <= 99) {
+        body[n++] = 'E';
+        body[n++] = e10 < 0 ? '-' : '+';
+        body[n++] = (char)('0' + ae / 10);
+        body[n++] = (char)('0' + ae % 10);
+    } else {
+        body[n++] = e10 < 0 ? '-' : '+';
+        body[n++] = (char)('0' + ae / 100);
+        body[n++] = (char)('0' + (ae / 10) % 10);
+        body[n++] = (char)('0' + ae % 10);
+    }
+    // right-justified in 15 columns; a longer body keeps its first 15 characters
+    if (n >= 15) {
+        std::memcpy(field, body, 15);
+    } else {
+        std::memset(field, ' ', (size_t)(15 - n));
+        std::memcpy(field + 15 - n, body, (size_t)n);
+    }
+    field[15] = 0;
+}
+
 }  // namespace
 
 extern "C" {
+
+void ysh_format_e15_6(double x, char field[16]) { e15_6_fast(x, field); }
 
 int ysh_event_setup(const ysh_model* m, const ysh_params* p, ysh_event* e)
 {
@@ -586,7 +670,7 @@ static bool write_one(const char* pref_out, const double* out, int nout, int k)
     const double* base = out + (size_t)nout * 4 * (size_t)(k - 1);
     for (int i = 0; i < nout; i++) {
         for (int c = 0; c < 4; c++) {
-            e15_6(base[(size_t)i + (size_t)nout * c], f);
+            e15_6_fast(base[(size_t)i + (size_t)nout * c], f);
             text.append(f, 15);
         }
         text += '\n';
