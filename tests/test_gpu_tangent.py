@@ -144,11 +144,17 @@ def test_tangent_needs_a_direction(engine, workdir):
     engine.set_solver("batched")
 
 
-def test_model_gradient_matches_finite_differences(engine, workdir):
+@pytest.mark.parametrize("size", ["small", "c4"])
+def test_model_gradient_matches_finite_differences(engine, workdir, size):
     """Misfit gradient over every knot parameter and the moment tensor,
-    against central differences of the misfit along 20 random directions."""
-    p = W.config("c4", seed=3, lmax=40, fmax=6.0, f21=4.5, f22=5.5, dt=20.0, tout=40.0)[0]
-    p.receivers = p.receivers[:6]
+    against central differences of the misfit along 20 random directions:
+    on a small event, and on c4 as stated (lmax 300, 20 mHz, 60 min at 5 s,
+    50 receivers, source at 150 km; 3 x 200 knot parameters)."""
+    if size == "small":
+        p = W.config("c4", seed=3, lmax=40, fmax=6.0, f21=4.5, f22=5.5, dt=20.0, tout=40.0)[0]
+        p.receivers = p.receivers[:6]
+    else:
+        p = W.config("c4", seed=0)[0]
     pf = p.write(workdir / "c4.in")
     km = KnotModel(p.model_file)
     ev = Event(km.host, Params(pf))
