@@ -249,8 +249,10 @@ __global__ void k_rotate(int nout, int nr, const double* __restrict__ cs, double
 // the other CTAs' shared memory (plain distributed-shared-memory loads),
 // runs those stages in registers and writes Re() of the outputs t = l + T j
 // below nout, divided by dt n, times e^{eps t} and the amplitude scale.
-// The theta row's outputs stay in registers until the phi row's are ready,
-// so the rotation to north / east (yspec.f90:466-473) happens in the same
+// The three rows of a receiver go through each phase together (three
+// quarter buffers per CTA), so one receiver costs two cluster barriers.  The
+// theta row's outputs stay in registers until the phi row's are ready, so
+// the rotation to north / east (yspec.f90:466-473) happens in the same
 // thread.  Every butterfly is the same operation, with the same twiddle, as
 // in the two-pass form, so the traces are identical to it.
 // ---------------------------------------------------------------------------
@@ -276,24 +278,30 @@ k_ifft_fused(TraceDev td, int k0, const cd* __restrict__ ur, const cd* __restric
     double* o = out + (size_t)td.nout * 4 * k;
     const double ca = cs[2 * (size_t)k], sa = cs[2 * (size_t)k + 1];
     cd v[8];
+    // phase 1 of the three rows (Z, theta, phi), each in its own quarter buffer
+    for (int s0 = 0; s0 < q; s0 += 3) {
+        const int m = min(3, q - s0);
+        const bool first = s0 == 0;
+#pragma unroll 1
+        for (int c = 0; c < 3; c++) {
+            const cd* spec = (c == 0 ? ur : (c == 1 ? ut : up)) + (size_t)k * td.nw;
+            cd* buf = fbuf + (size_t)c * T;
+            if (m == 3) round_a<3>(v, s0, first, false, td, base, nthr, spec, filt, tw, buf, nullptr);
+            else if (m == 2) round_a<2>(v, s0, first, false, td, base, nthr, spec, filt, tw, buf, nullptr);
+            else round_a<1>(v, s0, first, false, td, base, nthr, spec, filt, tw, buf, nullptr);
+        }
+    }
+    cl.sync();                                          // every quarter's phase 1 is in shared memory
+    int l0[LPT];
+#pragma unroll
+    for (int a = 0; a < LPT; a++) l0[a] = rank * (T / C) + (int)threadIdx.x * LPT + a;
 #pragma unroll 1
     for (int c = 0; c < 3; c++) {
-        const cd* spec = (c == 0 ? ur : (c == 1 ? ut : up)) + (size_t)k * td.nw;
-        for (int s0 = 0; s0 < q; s0 += 3) {
-            const int m = min(3, q - s0);
-            const bool first = s0 == 0;
-            if (m == 3) round_a<3>(v, s0, first, false, td, base, nthr, spec, filt, tw, fbuf, nullptr);
-            else if (m == 2) round_a<2>(v, s0, first, false, td, base, nthr, spec, filt, tw, fbuf, nullptr);
-            else round_a<1>(v, s0, first, false, td, base, nthr, spec, filt, tw, fbuf, nullptr);
-        }
-        cl.sync();                                      // every quarter's phase 1 is in shared memory
-        int l0[LPT];
 #pragma unroll
         for (int a = 0; a < LPT; a++) {
-            l0[a] = rank * (T / C) + (int)threadIdx.x * LPT + a;
             const cd* src[C];
 #pragma unroll
-            for (int j = 0; j < C; j++) src[j] = cl.map_shared_rank(fbuf, j);
+            for (int j = 0; j < C; j++) src[j] = cl.map_shared_rank(fbuf + (size_t)c * T, j);
 #pragma unroll
             for (int j = 0; j < C; j++) v[a * C + j] = src[j][l0[a]];
         }
@@ -317,8 +325,8 @@ k_ifft_fused(TraceDev td, int k0, const cd* __restrict__ ur, const cd* __restric
                     o[(size_t)3 * td.nout + t] = t1 * sa + y * ca;
                 }
             }
-        cl.sync();                                      // others are done reading this quarter
     }
+    cl.sync();                                          // others are done reading these quarters
 }
 
 template <int C>
@@ -326,7 +334,7 @@ cudaError_t launch_fused(const TraceDev& td, const cd* ur, const cd* ut, const c
                          const cd* tw, const double* expt, const double* cs, double* out, cudaStream_t s)
 {
     const int T = td.nt / C;
-    const size_t smem = (size_t)T * sizeof(cd);
+    const size_t smem = (size_t)3 * T * sizeof(cd);
     cudaError_t e = cudaFuncSetAttribute(k_ifft_fused<C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     if (e != cudaSuccess) return e;
