@@ -228,8 +228,14 @@ def gradient_check(local: int) -> dict:
     syn = adjoint.ModelSynthetics(eng, ev, km)
     P0 = km.params()
     mm0 = torch.tensor(p.mm, dtype=torch.float64)
+    # observed traces: the model with seeded 1% Gaussian-smoothed (3 knots)
+    # perturbations of rho, Vp and Vs at every knot
     rng = np.random.default_rng(11)
-    obs = syn(*(x * (1.0 + torch.from_numpy(rng.standard_normal(km.nknot)) * 1e-3) for x in P0), mm0).detach()
+    kern = np.exp(-0.5 * (np.arange(-9, 10) / 3.0) ** 2)
+    kern /= kern.sum()
+    Pobs = tuple(x * (1.0 + torch.from_numpy(np.convolve(rng.standard_normal(km.nknot), kern, mode="same")) * 1e-2)
+                 for x in P0)
+    obs = syn(*Pobs, mm0).detach()
     syn(*P0, mm0)                                   # warm-up (module loading, graphs)
     rho, vp, vs = (x.clone().requires_grad_() for x in P0)
     mm = mm0.clone().requires_grad_()
