@@ -20,6 +20,7 @@
 #include <fstream>
 #include <memory>
 #include <atomic>
+#include <chrono>
 #include <map>
 #include <string>
 #include <thread>
@@ -704,8 +705,17 @@ int ysh_write_traces(const char* pref_out, const double* out, int nout, int nr)
     return ok ? YSH_OK : YSH_ERR_IO;
 }
 
+// Wall-clock seconds, for the per-phase report of YSPEC_TIMING.
+static double wall_s()
+{
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
 int ysh_run(const char* param_file, int device, int write_files, double** out, int* nout, int* nr)
 {
+    const bool timing = std::getenv("YSPEC_TIMING") != nullptr;
+    const double t0 = wall_s();
+    double t1 = t0, t2 = t0, t3 = t0;
     if (out) *out = nullptr;
     ysh_params p;
     int rc = ysh_read_params(param_file, &p);
@@ -730,9 +740,21 @@ int ysh_run(const char* param_file, int device, int write_files, double** out, i
     if (!rc) {
         int rows = ysg_trace_rows(&e.tm);
         buf = (double*)std::malloc((size_t)rows * 4 * (size_t)std::max(p.nr, 1) * sizeof(double));
+        t1 = wall_s();
         rc = ysg_event_run(h, &e.ev, &e.tm, buf, &no);
+        t2 = wall_s();
     }
     if (!rc && write_files) rc = ysh_write_traces(p.pref_out, buf, no, p.nr);
+    t3 = wall_s();
+    if (timing && !rc) {
+        float ms[4] = {0, 0, 0, 0};
+        ysg_last_timings(h, ms);
+        std::fprintf(stderr,
+                     "yspec timing: setup %.3f s (parameters, model, geometry, device, upload), "
+                     "engine %.3f s (device stages ms: Legendre %.2f, solves %.2f, l-sum %.2f, "
+                     "time series %.2f), writer %.3f s (%d files x %d lines)\n",
+                     t1 - t0, t2 - t1, ms[0], ms[1], ms[2], ms[3], t3 - t2, write_files ? p.nr : 0, no);
+    }
     if (!rc && out) {
         *out = buf;
         buf = nullptr;

@@ -2,7 +2,9 @@
 // B200 engine: same argument, parameter file, model deck and per-receiver
 // ASCII output files as the reference.  Set YSPEC_DEVICE to pick the GPU.
 // `yspec a.in b.in ...` runs several events; those sharing a model deck
-// are solved as one batch (each still writes its own files).
+// are solved as one batch (each still writes its own files).  With
+// YSPEC_TIMING set, a single-event run reports the wall time of its set-up,
+// engine and writer phases on stderr.
 #include <cstdio>
 #include <cstdlib>
 
