@@ -677,8 +677,7 @@ int enqueue_traces(ysg_handle* h, int nev, int ns)
         const TraceDev& td = s.ptd;
         const size_t nspec = (size_t)td.nw * std::max(td.nr, 1);
         const cd* d_ur = s.spec.as<cd>();
-        if (td.nr > 0)                       // fused: one per 65535 receivers; else A, B, rotation
-            h->launches += ifft_fused_supported(td.nt) ? (td.nr + 65534) / 65535 : 3 * ((td.nr + 21844) / 21845);
+        h->launches += td.nr > 0 ? 3 : 0;   // pass A, pass B, rotation
         CK(launch_ifft(td, d_ur, d_ur + nspec, d_ur + 2 * nspec, s.filt.as<double>(), s.tw.as<cd>(),
                        s.expt.as<double>(), s.cs.as<double>(), h->scratch[ns ? e % ns : 0].as<cd>(),
                        s.out.as<double>(), stream_of(h, ns, e)));

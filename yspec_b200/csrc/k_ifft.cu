@@ -16,8 +16,6 @@
 // builds the row on the fly; pass B applies the post-processing and writes
 // the real traces.  Intermediate rows live in a scratch buffer.  Inside a
 // pass each thread runs up to three stages at a time in registers (below).
-#include <cooperative_groups.h>
-
 #include "ysg_kernels.h"
 
 namespace ysg {
@@ -234,123 +232,7 @@ __global__ void k_rotate(int nout, int nr, const double* __restrict__ cs, double
     o[(size_t)3 * nout + i] = t1 * sa + t2 * ca;
 }
 
-// ---------------------------------------------------------------------------
-// Fused form: one thread-block cluster per receiver runs the whole network
-// of each of its three rows on chip, then post-processes and rotates, with
-// no scratch row in global memory.
-//
-// A cluster of C CTAs (C = n / 4096, at least 1) splits a row of n = 2^p
-// positions (bit-reversed storage) into C contiguous quarters of T = n / C.
-// Phase 1: CTA c runs stages 0 .. log2(T)-1 inside its quarter, in rounds of
-// up to three stages per thread in registers with shared-memory exchanges
-// (the rounds of pass A above, over a tile of T).  Phase 2: the last log2(C)
-// stages pair positions l + T j across quarters (same l, j = 0 .. C-1): after
-// a cluster barrier each thread reads the C values of its l straight from
-// the other CTAs' shared memory (plain distributed-shared-memory loads),
-// runs those stages in registers and writes Re() of the outputs t = l + T j
-// below nout, divided by dt n, times e^{eps t} and the amplitude scale.
-// The three rows of a receiver go through each phase together (three
-// quarter buffers per CTA), so one receiver costs two cluster barriers.  The
-// theta row's outputs stay in registers until the phi row's are ready, so
-// the rotation to north / east (yspec.f90:466-473) happens in the same
-// thread.  Every butterfly is the same operation, with the same twiddle, as
-// in the two-pass form, so the traces are identical to it.
-// ---------------------------------------------------------------------------
-constexpr int FUSED_T_MAX = 4096;        // positions per CTA
-
-template <int C>
-__global__ void __launch_bounds__(FUSED_T_MAX / 8) __cluster_dims__(C, 1, 1)
-k_ifft_fused(TraceDev td, int k0, const cd* __restrict__ ur, const cd* __restrict__ ut,
-             const cd* __restrict__ up, const double* __restrict__ filt, const cd* __restrict__ tw,
-             const double* __restrict__ expt, const double* __restrict__ cs, double* __restrict__ out)
-{
-    namespace cg = cooperative_groups;
-    extern __shared__ cd fbuf[];
-    cg::cluster_group cl = cg::this_cluster();
-    const int n = td.nt, p = td.log2n, ln2 = p - 1;
-    const int T = n / C, nthr = T / 8;
-    const int q = p - lg2(C);                           // stages run in phase 1
-    const int rank = (int)cl.block_rank();
-    const int k = k0 + blockIdx.y;                      // receiver
-    const unsigned base = (unsigned)(rank * T);
-    constexpr int LPT = 8 / C;                          // low indices per thread in phase 2
-    double keep[8];                                     // theta outputs until phi is done
-    double* o = out + (size_t)td.nout * 4 * k;
-    const double ca = cs[2 * (size_t)k], sa = cs[2 * (size_t)k + 1];
-    cd v[8];
-    // phase 1 of the three rows (Z, theta, phi), each in its own quarter buffer
-    for (int s0 = 0; s0 < q; s0 += 3) {
-        const int m = min(3, q - s0);
-        const bool first = s0 == 0;
-#pragma unroll 1
-        for (int c = 0; c < 3; c++) {
-            const cd* spec = (c == 0 ? ur : (c == 1 ? ut : up)) + (size_t)k * td.nw;
-            cd* buf = fbuf + (size_t)c * T;
-            if (m == 3) round_a<3>(v, s0, first, false, td, base, nthr, spec, filt, tw, buf, nullptr);
-            else if (m == 2) round_a<2>(v, s0, first, false, td, base, nthr, spec, filt, tw, buf, nullptr);
-            else round_a<1>(v, s0, first, false, td, base, nthr, spec, filt, tw, buf, nullptr);
-        }
-    }
-    cl.sync();                                          // every quarter's phase 1 is in shared memory
-    int l0[LPT];
-#pragma unroll
-    for (int a = 0; a < LPT; a++) l0[a] = rank * (T / C) + (int)threadIdx.x * LPT + a;
-#pragma unroll 1
-    for (int c = 0; c < 3; c++) {
-#pragma unroll
-        for (int a = 0; a < LPT; a++) {
-            const cd* src[C];
-#pragma unroll
-            for (int j = 0; j < C; j++) src[j] = cl.map_shared_rank(fbuf + (size_t)c * T, j);
-#pragma unroll
-            for (int j = 0; j < C; j++) v[a * C + j] = src[j][l0[a]];
-        }
-        if constexpr (C > 1) fft_round<(C == 8 ? 3 : (C == 4 ? 2 : 1))>(v, q, l0, T, ln2, tw);
-#pragma unroll
-        for (int a = 0; a < LPT; a++)
-#pragma unroll
-            for (int j = 0; j < C; j++) {
-                const int t = l0[a] + T * j;
-                if (t >= td.nout) continue;
-                // data/(dt*n), * e^{eps t}, * amplitude scale (yspec.f90:439-460)
-                const double y = ((v[a * C + j].x / td.scale) * expt[t]) * td.amp_norm;
-                if (c == 0) {
-                    o[(size_t)td.nout + t] = y;
-                    o[t] = ((double)t * td.dt) * td.t_norm;
-                } else if (c == 1) {
-                    keep[a * C + j] = y;
-                } else {
-                    const double t1 = keep[a * C + j];
-                    o[(size_t)2 * td.nout + t] = -(t1 * ca) + y * sa;
-                    o[(size_t)3 * td.nout + t] = t1 * sa + y * ca;
-                }
-            }
-    }
-    cl.sync();                                          // others are done reading these quarters
-}
-
-template <int C>
-cudaError_t launch_fused(const TraceDev& td, const cd* ur, const cd* ut, const cd* up, const double* filt,
-                         const cd* tw, const double* expt, const double* cs, double* out, cudaStream_t s)
-{
-    const int T = td.nt / C;
-    const size_t smem = (size_t)3 * T * sizeof(cd);
-    cudaError_t e = cudaFuncSetAttribute(k_ifft_fused<C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
-    if (e != cudaSuccess) return e;
-    const int chunk = 65535;                            // receivers per launch (grid.y)
-    for (int k0 = 0; k0 < td.nr; k0 += chunk) {
-        const int nk = td.nr - k0 < chunk ? td.nr - k0 : chunk;
-        k_ifft_fused<C><<<dim3(C, nk), T / 8, smem, s>>>(td, k0, ur, ut, up, filt, tw, expt, cs, out);
-        e = cudaGetLastError();
-        if (e != cudaSuccess) return e;
-    }
-    return cudaSuccess;
-}
-
-bool ifft_fused_supported(int nt) { return nt >= 256 && nt <= 8 * FUSED_T_MAX; }
-
-size_t ifft_scratch_bytes(int nt, int nr) { return ifft_fused_supported(nt) ? 0 : (size_t)3 * nr * nt * sizeof(cd); }
+size_t ifft_scratch_bytes(int nt, int nr) { return (size_t)3 * nr * nt * sizeof(cd); }
 
 cudaError_t launch_ifft(const TraceDev& td, const cd* ur, const cd* ut, const cd* up,
                         const double* filt, const cd* tw, const double* expt, const double* cs_azep,
@@ -359,13 +241,6 @@ cudaError_t launch_ifft(const TraceDev& td, const cd* ur, const cd* ut, const cd
     if (td.nr <= 0) return cudaSuccess;
     const int n = td.nt;
     if (n < 8 || n > (1 << 20)) return cudaErrorInvalidValue;
-    if (ifft_fused_supported(n)) {
-        const int C = n <= FUSED_T_MAX ? 1 : n / FUSED_T_MAX;
-        if (C == 1) return launch_fused<1>(td, ur, ut, up, filt, tw, expt, cs_azep, out, s);
-        if (C == 2) return launch_fused<2>(td, ur, ut, up, filt, tw, expt, cs_azep, out, s);
-        if (C == 4) return launch_fused<4>(td, ur, ut, up, filt, tw, expt, cs_azep, out, s);
-        return launch_fused<8>(td, ur, ut, up, filt, tw, expt, cs_azep, out, s);
-    }
     // one row per receiver and component in grid.y (at most 65535): receivers
     // go in chunks; each chunk's rows start at the top of the scratch buffer
     const int chunk = 65535 / 3;

@@ -77,10 +77,6 @@ struct TraceDev {
     double dt, scale, t_norm, amp_norm;
 };
 size_t ifft_scratch_bytes(int nt, int nr);
-// nt for which K4 runs as one fused cluster kernel (no scratch rows): one
-// launch per 65535 receivers; other nt take the two-pass form (three
-// launches per 21845 receivers).
-bool ifft_fused_supported(int nt);
 cudaError_t launch_ifft(const TraceDev& td, const cd* ur, const cd* ut, const cd* up,
                         const double* filt, const cd* tw, const double* expt,
                         const double* cs_azep, cd* scratch, double* out, cudaStream_t s);

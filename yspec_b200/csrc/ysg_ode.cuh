@@ -631,7 +631,7 @@ __device__ __forceinline__ void rkck_step_loop(const Ctx& c, cd* y, double x, do
             const double f0 = ck_fold[s][0], f1 = ck_fold[s][1], f2 = ck_fold[s][2],
                          f3 = ck_fold[s][3];
             cd* const a1 = kb + S;
-#pragma unroll 1
+#pragma unroll 2
             for (int i = 0; i < N; i++) {
                 const int o = i * KS;
                 a1[o] = f0 * kb[o] + f1 * a1[o] + f2 * kb[2 * S + o] + f3 * kb[3 * S + o];
