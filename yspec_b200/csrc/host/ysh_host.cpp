@@ -732,6 +732,9 @@ int ysh_run(const char* param_file, int device, int write_files, double** out, i
     double* buf = nullptr;
     int no = 0;
     if (!rc) rc = ysg_create(&h, device);
+    // one run per handle: no autotuning (it would solve the event once per
+    // schedule); schedule 2 is the autotuner's choice on every measured workload
+    if (!rc) rc = ysg_set_schedule(h, 2);
     if (!rc) {
         ysg_model view;
         ysh_model_view(m, &view);
@@ -789,6 +792,9 @@ int ysh_run_batch(int nfiles, const char* const* param_files, int device, int wr
     for (int i = 0; i < nread && !rc; i++) groups[ps[(size_t)i].model_file].push_back(i);
     ysg_handle* h = nullptr;
     if (!rc) rc = ysg_create(&h, device);
+    // one run per handle: no autotuning (it would solve the event once per
+    // schedule); schedule 2 is the autotuner's choice on every measured workload
+    if (!rc) rc = ysg_set_schedule(h, 2);
     for (auto it = groups.begin(); it != groups.end() && !rc; ++it) {
         const std::vector<int>& ids = it->second;
         ysh_model* m = nullptr;
