@@ -10,7 +10,10 @@ self-gravitation, acceleration output with potential/tilt corrections,
 200-knot PREM-like model, source depth U(0, 700) km: 615,820 (omega,l) pairs.
 
 Multi-GPU: every rank runs its own copy of the event (replicas, weak scaling;
-the pairs are independent, no collective is on the data path).  Timing is on
+the pairs are independent, no collective is on the data path).  With
+--shard, one event is split over the ranks instead: frequency shards, one
+NCCL all-to-all to receiver shards, a row gather of the traces (strong
+scaling).  Timing is on
 the device with CUDA events on the engine's stream, max over ranks.
 The reference arm (--impl reference) times the CPU restatement of the
 reference path on all host cores over the whole event, every step.
@@ -349,6 +352,72 @@ def run_reference(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+def run_sharded(args) -> None:
+    """One c2 event split over the ranks (yspec_b200.shard.run_event_sharded):
+    each rank solves an interleaved frequency shard for every receiver, one
+    NCCL all-to-all moves the spectra to receiver shards, each rank runs the
+    time series of its receivers, rank 0 gathers the traces.  Total work is
+    fixed as N grows (strong scaling).  A step is one whole event; the
+    timed span is bracketed by barriers and device synchronisations and
+    measured with CUDA events, max over ranks."""
+    import socket
+    from datetime import timedelta
+
+    import torch
+    import torch.distributed as dist
+
+    from yspec_b200 import Engine, Event, Model, Params, shard as S
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world == 1 and "MASTER_PORT" not in os.environ:
+        sk = socket.socket()
+        sk.bind(("127.0.0.1", 0))
+        os.environ["MASTER_ADDR"], os.environ["MASTER_PORT"] = "127.0.0.1", str(sk.getsockname()[1])
+        sk.close()
+        os.environ.setdefault("RANK", "0")
+        os.environ.setdefault("WORLD_SIZE", "1")
+    dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
+    tmp = Path(tempfile.mkdtemp(prefix=f"ysshard{rank}_"))
+    p, pf = make_event(tmp)
+    model = Model(p.model_file)
+    eng = Engine(local, solver="batched")
+    eng.set_schedule(2)
+    eng.upload(model)
+    ev = Event(model, Params(pf))
+    pairs = float(ev.L * ev.nw)
+    for _ in range(args.warmup):
+        S.run_event_sharded(eng, ev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    dist.barrier()
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(args.steps):
+        out = S.run_event_sharded(eng, ev)
+    torch.cuda.synchronize()
+    e1.record()
+    e1.synchronize()
+    ms = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device="cuda")
+    dist.all_reduce(ms, op=dist.ReduceOp.MAX)
+    ms = float(ms.item())
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": pairs * args.steps / (ms / 1e3), "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded PREM-like model, receivers, moment tensor)",
+            "config": {"workload": WORKLOAD, "pairs_per_event": int(pairs), "receivers": ev.nr,
+                       "parallelism": f"frequency shards x{world}, NCCL all-to-all to receiver shards, "
+                                      "row gather of the traces on rank 0"},
+            "e2e": {"value": pairs * args.steps / (ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": int(out.nbytes) if out is not None else 0},
+        }
+        print(json.dumps(line), flush=True)
+    dist.destroy_process_group()
+
+
 def run_b200(args) -> None:
     import torch
     import torch.distributed as dist
@@ -525,9 +594,13 @@ def main() -> int:
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-vs-plain comparison")
     ap.add_argument("--no-grad", action="store_true", help="skip the c4 model-gradient timing")
     ap.add_argument("--no-c5", action="store_true", help="skip the c5 16-event batch")
+    ap.add_argument("--shard", action="store_true",
+                    help="one event split over the N GPUs (frequency shards, all-to-all) instead of replicas")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
+    elif args.shard:
+        run_sharded(args)
     else:
         run_b200(args)
     return 0

@@ -126,3 +126,23 @@ def test_schedules_agree(engine, workdir):
     single = engine.run(evs[1])
     np.testing.assert_array_equal(single, runs[1][1])
     engine.set_schedule(-1)
+
+
+def test_c3_batch_at_size_matches_oracle(engine, workdir):
+    """The benchmarked 64-event uneven batch (c3) in one ysg_batch_run; six
+    of its events checked against the oracle run of each alone: the three
+    lowest bands (10.3-10.9 mHz), a shallow 30 km source, a 13.7 mHz band,
+    and the 48 mHz, lmax 722 event."""
+    ps = W.config("c3", seed=0)
+    model = Model(ps[0].model_file)
+    pfs = [p.write(workdir / f"c3_{i}.in") for i, p in enumerate(ps)]
+    engine.set_solver("batched")
+    engine.upload(model)
+    got = engine.batch_run([Event(model, Params(pf)) for pf in pfs])
+    for i in (26, 62, 19, 10, 45, 4):
+        want = yo.Problem(pfs[i]).run(nthreads=16)
+        assert got[i].shape == want.shape, i
+        np.testing.assert_array_equal(got[i][:, 0], want[:, 0])
+        for k in range(want.shape[0]):
+            for c in range(1, 4):
+                assert rel_l2(got[i][k, c], want[k, c]) <= TOL, (i, k, c)
