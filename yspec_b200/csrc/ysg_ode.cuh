@@ -12,7 +12,6 @@
 // Quantities that steer integer decisions (start level, step counts, grid
 // points of the l = 0 gravity solve) are formed with explicitly rounded
 // operations so they agree bit for bit with the reference's unfused FP64.
-#pragma once
 #include "ysg_dual.cuh"
 #include "ysg_model.cuh"
 
@@ -27,7 +26,9 @@
 // number (ysg_dual.cuh) and the solve returns, beside its value, the
 // derivative along one direction of the model (the tangent-linear solver).
 // Each form gets its own inline namespace so the translation units never
-// share a definition.
+// share a definition, and a translation unit may include this header once
+// per form (the reverse sweep uses the plain and the tangent form): the
+// include guard is per form.
 #ifndef YSG_SMEM_STAGES
 #define YSG_SMEM_STAGES 0
 #endif
@@ -37,15 +38,93 @@
 #ifndef YSG_TANGENT
 #define YSG_TANGENT 0
 #endif
+#undef YSG_VARIANT
+#undef YSG_ODE_BODY
 #if YSG_TANGENT
 #define YSG_VARIANT v_tangent
+#ifndef YSG_ODE_DONE_v_tangent
+#define YSG_ODE_DONE_v_tangent
+#define YSG_ODE_BODY
+#endif
 #elif YSG_COUNT_ONLY
 #define YSG_VARIANT v_count
+#ifndef YSG_ODE_DONE_v_count
+#define YSG_ODE_DONE_v_count
+#define YSG_ODE_BODY
+#endif
 #elif YSG_SMEM_STAGES
 #define YSG_VARIANT v_smem
+#ifndef YSG_ODE_DONE_v_smem
+#define YSG_ODE_DONE_v_smem
+#define YSG_ODE_BODY
+#endif
 #else
 #define YSG_VARIANT v_local
+#ifndef YSG_ODE_DONE_v_local
+#define YSG_ODE_DONE_v_local
+#define YSG_ODE_BODY
 #endif
+#endif
+// Helpers on plain and dual complex values only: the same in every form,
+// so they sit outside the per-form namespaces (argument-dependent lookup
+// on cd would otherwise see one copy per form included).
+#ifndef YSG_ODE_COMMON
+#define YSG_ODE_COMMON
+namespace ysg {
+
+__device__ __forceinline__ double norm2(cd a) { return a.x * a.x + a.y * a.y; }
+
+// Complex multiply-accumulate s + x y (cmac) and s - x y (cmsc) as fused
+// multiply-adds: four for a complex factor, two for a real one, where a
+// product followed by a sum takes six and four.  The 14-component systems
+// accumulate their outputs term by term with them, in the tangent build
+// too (the value and the derivative part each fused).
+__device__ __forceinline__ cd cmac(cd s, cd x, cd y)
+{
+    return cd{fma(x.x, y.x, fma(-x.y, y.y, s.x)), fma(x.x, y.y, fma(x.y, y.x, s.y))};
+}
+__device__ __forceinline__ cd cmsc(cd s, cd x, cd y)
+{
+    return cd{fma(-x.x, y.x, fma(x.y, y.y, s.x)), fma(-x.x, y.y, fma(-x.y, y.x, s.y))};
+}
+__device__ __forceinline__ cd cmac(cd s, double x, cd y) { return cd{fma(x, y.x, s.x), fma(x, y.y, s.y)}; }
+__device__ __forceinline__ cd cmsc(cd s, double x, cd y) { return cd{fma(-x, y.x, s.x), fma(-x, y.y, s.y)}; }
+__device__ __forceinline__ cd cmac(cd s, cd x, double y) { return cmac(s, y, x); }
+__device__ __forceinline__ cd cmsc(cd s, cd x, double y) { return cmsc(s, y, x); }
+// dual numbers: the value and d(s + x y) = ds + dx y + x dy, both fused
+__device__ __forceinline__ dcplx cmac(dcplx s, dcplx x, dcplx y)
+{
+    return dcplx(cmac(s.v, x.v, y.v), cmac(cmac(s.d, x.d, y.v), x.v, y.d));
+}
+__device__ __forceinline__ dcplx cmsc(dcplx s, dcplx x, dcplx y)
+{
+    return dcplx(cmsc(s.v, x.v, y.v), cmsc(cmsc(s.d, x.d, y.v), x.v, y.d));
+}
+__device__ __forceinline__ dcplx cmac(dcplx s, dreal x, dcplx y)
+{
+    return dcplx(cmac(s.v, x.v, y.v), cmac(cmac(s.d, x.d, y.v), x.v, y.d));
+}
+__device__ __forceinline__ dcplx cmsc(dcplx s, dreal x, dcplx y)
+{
+    return dcplx(cmsc(s.v, x.v, y.v), cmsc(cmsc(s.d, x.d, y.v), x.v, y.d));
+}
+__device__ __forceinline__ dcplx cmac(dcplx s, dcplx x, dreal y) { return cmac(s, y, x); }
+__device__ __forceinline__ dcplx cmsc(dcplx s, dcplx x, dreal y) { return cmsc(s, y, x); }
+template <class S, class X, class Y>
+__device__ __forceinline__ S cmac(S s, X x, Y y)
+{
+    return s + x * y;
+}
+template <class S, class X, class Y>
+__device__ __forceinline__ S cmsc(S s, X x, Y y)
+{
+    return s - x * y;
+}
+
+}  // namespace ysg
+#endif  // YSG_ODE_COMMON
+
+#ifdef YSG_ODE_BODY
 
 namespace ysg {
 inline namespace YSG_VARIANT {
@@ -156,53 +235,6 @@ __device__ __forceinline__ mreal splr(const Ctx& c, const SplPt& s, int p)
 #endif
 }
 
-// Complex multiply-accumulate s + x y (cmac) and s - x y (cmsc) as fused
-// multiply-adds: four for a complex factor, two for a real one, where a
-// product followed by a sum takes six and four.  The 14-component systems
-// accumulate their outputs term by term with them, in the tangent build
-// too (the value and the derivative part each fused).
-__device__ __forceinline__ cd cmac(cd s, cd x, cd y)
-{
-    return cd{fma(x.x, y.x, fma(-x.y, y.y, s.x)), fma(x.x, y.y, fma(x.y, y.x, s.y))};
-}
-__device__ __forceinline__ cd cmsc(cd s, cd x, cd y)
-{
-    return cd{fma(-x.x, y.x, fma(x.y, y.y, s.x)), fma(-x.x, y.y, fma(-x.y, y.x, s.y))};
-}
-__device__ __forceinline__ cd cmac(cd s, double x, cd y) { return cd{fma(x, y.x, s.x), fma(x, y.y, s.y)}; }
-__device__ __forceinline__ cd cmsc(cd s, double x, cd y) { return cd{fma(-x, y.x, s.x), fma(-x, y.y, s.y)}; }
-__device__ __forceinline__ cd cmac(cd s, cd x, double y) { return cmac(s, y, x); }
-__device__ __forceinline__ cd cmsc(cd s, cd x, double y) { return cmsc(s, y, x); }
-// dual numbers: the value and d(s + x y) = ds + dx y + x dy, both fused
-__device__ __forceinline__ dcplx cmac(dcplx s, dcplx x, dcplx y)
-{
-    return dcplx(cmac(s.v, x.v, y.v), cmac(cmac(s.d, x.d, y.v), x.v, y.d));
-}
-__device__ __forceinline__ dcplx cmsc(dcplx s, dcplx x, dcplx y)
-{
-    return dcplx(cmsc(s.v, x.v, y.v), cmsc(cmsc(s.d, x.d, y.v), x.v, y.d));
-}
-__device__ __forceinline__ dcplx cmac(dcplx s, dreal x, dcplx y)
-{
-    return dcplx(cmac(s.v, x.v, y.v), cmac(cmac(s.d, x.d, y.v), x.v, y.d));
-}
-__device__ __forceinline__ dcplx cmsc(dcplx s, dreal x, dcplx y)
-{
-    return dcplx(cmsc(s.v, x.v, y.v), cmsc(cmsc(s.d, x.d, y.v), x.v, y.d));
-}
-__device__ __forceinline__ dcplx cmac(dcplx s, dcplx x, dreal y) { return cmac(s, y, x); }
-__device__ __forceinline__ dcplx cmsc(dcplx s, dcplx x, dreal y) { return cmsc(s, y, x); }
-template <class S, class X, class Y>
-__device__ __forceinline__ S cmac(S s, X x, Y y)
-{
-    return s + x * y;
-}
-template <class S, class X, class Y>
-__device__ __forceinline__ S cmsc(S s, X x, Y y)
-{
-    return s - x * y;
-}
-
 // ---------------------------------------------------------------------------
 // Coefficient matrices
 //
@@ -214,7 +246,6 @@ __device__ __forceinline__ S cmsc(S s, X x, Y y)
 // The moduli are O(1) after normalisation, so this stays far from overflow
 // and agrees with the separate divisions to a few ulps.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ double norm2(cd a) { return a.x * a.x + a.y * a.y; }
 
 // module_int.f90:134-164 tor_amat (t real, k and s complex)
 struct TorCoef { mreal t; mcplx k, s; };
@@ -727,6 +758,7 @@ __device__ __forceinline__ void rescale(mcplx* y, int* scale)
 
 // module_int.f90:1847-1968 yint
 #if YSG_SMEM_STAGES || YSG_TANGENT
+#undef YSG_YINT_ATTR
 #define YSG_YINT_ATTR __noinline__
 #else
 #define YSG_YINT_ATTR
@@ -1196,3 +1228,4 @@ __device__ __forceinline__ void sph_ysol_ngcow(const mcplx* m, const mcplx* b, m
 
 }  // inline namespace
 }  // namespace ysg
+#endif  // YSG_ODE_BODY

@@ -1,0 +1,497 @@
+// ysg_pair_adjoint.cuh -- reverse sweep of one (omega, l) solve.
+//
+// The adjoint of pair_toroidal / pair_spheroidal (ysg_solvers.cuh) for the
+// self-gravitating solve with a solid inner core, no ocean and the receiver
+// at or above the source (tor_solver and sph_solver_g on their
+// receiver-above branch, module_solver.f90:25-142 and :640-823): given the
+// adjoints of the pair's uu / vv / ww coefficients, it adds the pair's
+// contribution to dL/dc[i][p][k] (the power-form spline segments, see
+// ysg_adjoint.cuh).  No reference counterpart: the reference has no
+// derivatives.
+//
+// Pieces:
+//   - the Cash-Karp integrations: yint_adj (ysg_adjoint.cuh), each one
+//     replayed from its stored starting state when its adjoint is needed;
+//   - the minor algebra (b_solid_start, sph_ysol, the secular determinant,
+//     the solid / fluid transforms) is linear in each argument and free of
+//     the model: its transposes are formed by applying the forward functions
+//     to unit vectors;
+//   - the start vectors and the source vectors depend on the thirteen model
+//     values at one radius: their derivatives come from the tangent-linear
+//     form of the same functions, once per parameter, along "unit" model
+//     directions (every knot value of parameter p moved by one, which moves
+//     the spline value at every radius by one);
+//   - grav(ir), the knot value of the potential / tilt correction, is the c0
+//     coefficient of segment ir.
+#pragma once
+#include "ysg_adjoint.cuh"
+#include "ysg_solvers.cuh"
+
+// the tangent-linear form of the same headers (namespace ysg::v_tangent)
+#pragma push_macro("YSG_TANGENT")
+#undef YSG_TANGENT
+#define YSG_TANGENT 1
+#include "ysg_solvers.cuh"
+#pragma pop_macro("YSG_TANGENT")
+
+namespace ysg {
+inline namespace v_local {
+
+// Unit model directions, one per parameter: knot records with v[p][0] = 1
+// for parameter p and zero elsewhere (and the segments of the same).
+struct UnitDirs {
+    const Knot* kn[NPARAM];
+    const Seg* sg[NPARAM];
+};
+
+__device__ inline void tangent_ctx(const Ctx& c, const UnitDirs& u, int p, v_tangent::Ctx& t)
+{
+    t.kn = c.kn;
+    t.mh = c.mh;
+    t.ll = c.ll;
+    t.llp1 = c.llp1;
+    t.il = c.il;
+    for (int q = 0; q < NSYS; q++) t.nst[q] = 0;
+    t.sg = c.sg;
+    t.kb = nullptr;
+    t.dkn = u.kn[p];
+    t.dsg = u.sg[p];
+    t.zeta = c.zeta;
+    t.zeta2 = c.zeta2;
+    t.zeta2m2 = c.zeta2m2;
+    t.szeta2m2 = c.szeta2m2;
+    t.nu = c.nu;
+    t.dr = c.dr;
+    t.ats = c.ats;
+    t.pib = c.pib;
+    t.omega = c.omega;
+    t.omega2 = c.omega2;
+    t.omegai = c.omegai;
+    t.omegai2 = c.omegai2;
+    t.lno = c.lno;
+}
+
+// vb_p += Re(sum_k yb_k dy_k / dv_p) for the start vectors at (i1, rt) and
+// the moments of the result go to G.  WHICH: 0 toroidal (2), 1 solid minor
+// (14), 2 fluid minor (5).
+template <int WHICH>
+__device__ inline void start_adj(const Ctx& c, const UnitDirs& u, int i1, double rt, const cd* yb, SegGrad& G)
+{
+    constexpr int N = WHICH == 0 ? 2 : (WHICH == 1 ? 14 : 5);
+    double vb[NPARAM];
+    for (int p = 0; p < NPARAM; p++) {
+        v_tangent::Ctx t;
+        tangent_ctx(c, u, p, t);
+        v_tangent::mcplx y[N];
+        if (WHICH == 0) v_tangent::tor_ystart(t, i1, rt, y);
+        else if (WHICH == 1) v_tangent::sph_minor_solid_start(t, i1, rt, y);
+        else v_tangent::sph_minor_fluid_start(t, i1, rt, y);
+        double s = 0.0;
+        for (int k = 0; k < N; k++) s += re(yb[k] * y[k].d);
+        vb[p] = s;
+    }
+    G.add(i1, rt - c.kn[i1].r, vb);
+}
+
+// Source vectors at (is, rs): svtb (5 x 2) and svsb (5 x 6) are the
+// adjoints of the toroidal and spheroidal source vectors (either may be
+// null).
+__device__ inline void source_adj(const Ctx& c, const UnitDirs& u, int is, double rs, const double* mm,
+                                  const cd (*svtb)[2], const cd (*svsb)[6], SegGrad& G)
+{
+    double vb[NPARAM];
+    for (int p = 0; p < NPARAM; p++) {
+        v_tangent::Ctx t;
+        tangent_ctx(c, u, p, t);
+        double s = 0.0;
+        if (svtb) {
+            v_tangent::mcplx svt[5][2];
+            v_tangent::source_vector_tor(t, is, rs, mm, svt);
+            for (int q = 0; q < 5; q++)
+                for (int b = 0; b < 2; b++) s += re(svtb[q][b] * svt[q][b].d);
+        }
+        if (svsb) {
+            v_tangent::mcplx svs[5][6];
+            v_tangent::source_vector_sph(t, is, rs, mm, svs);
+            for (int q = 0; q < 5; q++)
+                for (int b = 0; b < 6; b++) s += re(svsb[q][b] * svs[q][b].d);
+        }
+        vb[p] = s;
+    }
+    G.add(is, rs - c.kn[is].r, vb);
+}
+
+// ---------------------------------------------------------------------------
+// Transposes of the minor algebra (module_int.f90:1563-1837), through the
+// forward functions applied to unit vectors.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void unit(cd* e, int n, int j)
+{
+    for (int k = 0; k < n; k++) e[k] = mk(0.0);
+    e[j] = mk(1.0);
+}
+
+// y = sph_ysol(m, b): mb += dy/dm^T yb, bb += dy/db^T yb
+__device__ inline void ysol_adj(const cd* m, const cd* b, const cd* yb, cd* mb, cd* bb)
+{
+    cd e[14], y[6];
+    for (int j = 0; j < 14; j++) {
+        unit(e, 14, j);
+        sph_ysol(e, b, y);
+        cd s = mk(0.0);
+        for (int k = 0; k < 6; k++) s = s + yb[k] * y[k];
+        mb[j] = mb[j] + s;
+        sph_ysol(m, e, y);
+        s = mk(0.0);
+        for (int k = 0; k < 6; k++) s = s + yb[k] * y[k];
+        bb[j] = bb[j] + s;
+    }
+}
+
+// d = delta_solid(a, b)
+__device__ inline void delta_adj(const cd* a, const cd* b, cd db, cd* ab, cd* bb)
+{
+    cd e[14];
+    for (int j = 0; j < 14; j++) {
+        unit(e, 14, j);
+        ab[j] = ab[j] + db * delta_solid(e, b);
+        bb[j] = bb[j] + db * delta_solid(a, e);
+    }
+}
+
+// b = b_solid_start(m, s) for a fixed jump s: mb += (db/dm)^T bb
+__device__ inline void bstart_adj(const cd* s, const cd* bb, cd* mb)
+{
+    cd e[14], b[14];
+    for (int j = 0; j < 14; j++) {
+        unit(e, 14, j);
+        b_solid_start(e, s, b);
+        cd t = mk(0.0);
+        for (int k = 0; k < 14; k++) t = t + bb[k] * b[k];
+        mb[j] = mb[j] + t;
+    }
+}
+
+// mf = s2f(ms): msb += s2f^T mfb;  ms = f2s(mf): mfb += f2s^T msb
+__device__ inline void s2f_adj(const cd* mfb, cd* msb)
+{
+    cd e[14], f[5];
+    for (int j = 0; j < 14; j++) {
+        unit(e, 14, j);
+        s2f(e, f);
+        cd t = mk(0.0);
+        for (int k = 0; k < 5; k++) t = t + mfb[k] * f[k];
+        msb[j] = msb[j] + t;
+    }
+}
+__device__ inline void f2s_adj(const cd* msb, cd* mfb)
+{
+    cd e[5], m[14];
+    for (int j = 0; j < 5; j++) {
+        unit(e, 5, j);
+        f2s(e, m);
+        cd t = mk(0.0);
+        for (int k = 0; k < 14; k++) t = t + msb[k] * m[k];
+        mfb[j] = mfb[j] + t;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// tor_solver, receiver at or above the source (module_solver.f90:25-142)
+// ---------------------------------------------------------------------------
+// The forward solve again, keeping what the reverse sweep needs; yb is the
+// adjoint of yout.  Returns false if a step log overflowed.
+__device__ inline bool tor_solver_adj(Ctx& c, const UnitDirs& u, double rr, double rs, int ir, int is,
+                                      const cd yb_out[2][2], StepLog& L, SegGrad& G)
+{
+    const ModelHdr* mh = c.mh;
+    const Knot* kn = c.kn;
+    int scale1 = 0, scale2 = 0, scale3 = 0;
+    cd y1[2], y2[2], y3[2], y1s[2];
+    const int it = is;
+    int i1 = tor_start_level(c, c.ll, c.omega.x, it);
+    if (i1 == it && i1 > mh->noc + 1) i1 = i1 - 1;
+    const double rt = kn[i1].r;
+    const bool cmb_start = i1 == mh->noc + 1;
+    if (cmb_start) { y1[0] = mk(1.0); y1[1] = mk(0.0); }
+    else tor_ystart(c, i1, rt, y1);
+    y1s[0] = y1[0];
+    y1s[1] = y1[1];
+    yint<TorSys>(c, i1, is, rt, rs, y1, &scale1);
+    y3[0] = y1[0];
+    y3[1] = y1[1];
+    if (rr != rs) yint<TorSys>(c, is, ir, rs, rr, y3, &scale3);
+    y2[0] = mk(1.0);
+    y2[1] = mk(0.0);
+    const bool down2 = rr != kn[mh->nsl].r;
+    if (down2) yint<TorSys>(c, mh->nsl - 1, ir, kn[mh->nsl].r, rr, y2, &scale2);
+    const cd D = y2[1] * y3[0] - y2[0] * y3[1];
+    const cd delta = 1.0 / D;
+    const cd b0 = y1[1], b1 = -y1[0];
+    const cd dy0 = delta * y2[0], dy1 = delta * y2[1];
+    // reverse: yout[a][0] = -(dy_a b0), yout[a][1] = -(dy_a b1), times huge^scale3
+    const double F = huge_pow(scale3);
+    cd yb[2][2];
+    for (int a = 0; a < 2; a++)
+        for (int b = 0; b < 2; b++) yb[a][b] = F * yb_out[a][b];
+    const cd dyb0 = -(yb[0][0] * b0 + yb[0][1] * b1), dyb1 = -(yb[1][0] * b0 + yb[1][1] * b1);
+    const cd b0b = -(yb[0][0] * dy0 + yb[1][0] * dy1), b1b = -(yb[0][1] * dy0 + yb[1][1] * dy1);
+    cd y1b[2] = {-b1b, b0b};
+    const cd deltab = dyb0 * y2[0] + dyb1 * y2[1];
+    cd y2b[2] = {dyb0 * delta, dyb1 * delta};
+    const cd Db = deltab * (-(delta * delta));
+    y2b[1] = y2b[1] + Db * y3[0];
+    y2b[0] = y2b[0] - Db * y3[1];
+    cd y3b[2] = {Db * y2[1], -(Db * y2[0])};
+    // the surface solution starts from a fixed vector: only its model gradient
+    const cd e2[2] = {mk(1.0), mk(0.0)};
+    if (down2 && !yint_adj<TorT>(c, mh->nsl - 1, ir, kn[mh->nsl].r, rr, e2, y2b, true, L, G)) return false;
+    // y3 starts from y1 at the source
+    if (rr != rs && !yint_adj<TorT>(c, is, ir, rs, rr, y1, y3b, true, L, G)) return false;
+    y1b[0] = y1b[0] + y3b[0];
+    y1b[1] = y1b[1] + y3b[1];
+    if (!yint_adj<TorT>(c, i1, is, rt, rs, y1s, y1b, true, L, G)) return false;
+    if (!cmb_start) start_adj<0>(c, u, i1, rt, y1b, G);
+    return true;
+}
+
+// ---------------------------------------------------------------------------
+// sph_solver_g, solid inner core, no ocean, receiver at or above the source
+// (module_solver.f90:640-823): yb_out (6 x 4) is the adjoint of yout.
+// ---------------------------------------------------------------------------
+__device__ inline bool sph_solver_g_adj(Ctx& c, const UnitDirs& u, double rr, double rs, int ir, int is,
+                                        const cd yb_out[6][4], StepLog& L, SegGrad& G)
+{
+    const ModelHdr* mh = c.mh;
+    const Knot* kn = c.kn;
+    int scale1 = 0, scale2 = 0, scale3 = 0;
+    const int it = is;
+    const double rtop = rs;
+    int i1 = sph_start_level(c, c.ll, c.omega.x, it);
+    double rt = kn[i1].r;
+    if (i1 == 1) rt = fmin(0.1 * c.dr, 0.1 * kn[2].r);
+    if (i1 >= it) { i1 = it - 1; rt = kn[i1].r; }
+    // the chain from the start level to the source; branch 0: solid inner
+    // core start, 1: fluid outer core start, 2: mantle start
+    const int branch = i1 <= mh->nic ? 0 : (i1 <= mh->noc ? 1 : 2);
+    cd st[14], ms1[14], mf[5], mfs[5], ms_a[14], mf_a[5];
+    if (branch == 0) {
+        sph_minor_solid_start(c, i1, rt, st);
+        for (int k = 0; k < 14; k++) ms1[k] = st[k];
+        yint<MinorSolidG>(c, i1, mh->nic, rt, kn[mh->nic].r, ms1, &scale1);
+        for (int k = 0; k < 14; k++) ms_a[k] = ms1[k];           // before s2f
+        s2f(ms1, mf);
+        for (int k = 0; k < 5; k++) mfs[k] = mf[k];
+        yint<MinorFluidG>(c, mh->nic + 1, mh->noc, kn[mh->nic].r, kn[mh->noc].r, mf, &scale1);
+        for (int k = 0; k < 5; k++) mf_a[k] = mf[k];             // before f2s
+        f2s(mf, ms1);
+    } else if (branch == 1) {
+        sph_minor_fluid_start(c, i1, rt, mf);
+        for (int k = 0; k < 5; k++) mfs[k] = mf[k];
+        yint<MinorFluidG>(c, i1, mh->noc, rt, kn[mh->noc].r, mf, &scale1);
+        for (int k = 0; k < 5; k++) mf_a[k] = mf[k];
+        f2s(mf, ms1);
+    } else {
+        sph_minor_solid_start(c, i1, rt, st);
+        for (int k = 0; k < 14; k++) ms1[k] = st[k];
+    }
+    cd msm[14];                                                  // solid state entering the last leg
+    for (int k = 0; k < 14; k++) msm[k] = ms1[k];
+    const int mi1 = branch == 2 ? i1 : mh->noc + 1;
+    const double mr1 = branch == 2 ? rt : kn[mh->noc + 1].r;
+    yint<MinorSolidG>(c, mi1, it, mr1, rtop, ms1, &scale1);
+    cd ms3[14], ms2[14];
+    for (int k = 0; k < 14; k++) ms3[k] = ms1[k];
+    if (rr > rs) yint<MinorSolidG>(c, is, ir, rs, rr, ms3, &scale3);
+    cd e1[14];
+    unit(e1, 14, 0);
+    for (int k = 0; k < 14; k++) ms2[k] = e1[k];
+    yint<MinorSolidG>(c, mh->nknot - 1, ir, kn[mh->nknot].r, rr, ms2, &scale2);
+    const cd delta = delta_solid(ms3, ms2);
+    const int jump[4] = {0, 1, 3, 4};
+    cd ms1b[14], ms2b[14], ms3b[14];
+    for (int k = 0; k < 14; k++) ms1b[k] = ms2b[k] = ms3b[k] = mk(0.0);
+    cd deltab = mk(0.0);
+    for (int i = 0; i < 4; i++) {
+        cd s[6];
+        unit(s, 6, jump[i]);
+        int scale4 = 0;
+        cd b0[14], b[14], ys[6];
+        b_solid_start(ms1, s, b0);
+        for (int k = 0; k < 14; k++) b[k] = b0[k];
+        yint<BvecSolidG>(c, is, ir, rs, rr, b, &scale4);
+        sph_ysol(ms2, b, ys);
+        // yout[k][i] = (-ys[k] / delta) huge^(scale3 - scale4)
+        const double F = huge_pow(scale3 - scale4);
+        cd ysb[6];
+        for (int k = 0; k < 6; k++) {
+            const cd yk = F * yb_out[k][i];
+            ysb[k] = -(yk / delta);
+            deltab = deltab + yk * (ys[k] / (delta * delta));
+        }
+        cd bb[14];
+        for (int k = 0; k < 14; k++) bb[k] = mk(0.0);
+        ysol_adj(ms2, b, ysb, ms2b, bb);
+        if (!yint_adj<BvecSolidGT>(c, is, ir, rs, rr, b0, bb, true, L, G)) return false;
+        bstart_adj(s, bb, ms1b);
+    }
+    delta_adj(ms3, ms2, deltab, ms3b, ms2b);
+    if (!yint_adj<MinorSolidGT>(c, mh->nknot - 1, ir, kn[mh->nknot].r, rr, e1, ms2b, true, L, G)) return false;
+    if (rr > rs) {
+        if (!yint_adj<MinorSolidGT>(c, is, ir, rs, rr, ms1, ms3b, true, L, G)) return false;
+    }
+    for (int k = 0; k < 14; k++) ms1b[k] = ms1b[k] + ms3b[k];
+    // back along the chain to the start level
+    if (!yint_adj<MinorSolidGT>(c, mi1, it, mr1, rtop, msm, ms1b, true, L, G)) return false;
+    if (branch == 2) {
+        start_adj<1>(c, u, i1, rt, ms1b, G);
+        return true;
+    }
+    cd mfb[5];
+    for (int k = 0; k < 5; k++) mfb[k] = mk(0.0);
+    f2s_adj(ms1b, mfb);
+    if (branch == 1) {
+        if (!yint_adj<MinorFluidGT>(c, i1, mh->noc, rt, kn[mh->noc].r, mfs, mfb, true, L, G)) return false;
+        start_adj<2>(c, u, i1, rt, mfb, G);
+        return true;
+    }
+    if (!yint_adj<MinorFluidGT>(c, mh->nic + 1, mh->noc, kn[mh->nic].r, kn[mh->noc].r, mfs, mfb, true, L, G))
+        return false;
+    cd msb[14];
+    for (int k = 0; k < 14; k++) msb[k] = mk(0.0);
+    s2f_adj(mfb, msb);
+    if (!yint_adj<MinorSolidGT>(c, i1, mh->nic, rt, kn[mh->nic].r, st, msb, true, L, G)) return false;
+    start_adj<1>(c, u, i1, rt, msb, G);
+    (void)ms_a;
+    (void)mf_a;
+    return true;
+}
+
+// ---------------------------------------------------------------------------
+// The per-pair epilogues of yspec.f90:301-316 and :344-400.
+// ---------------------------------------------------------------------------
+// The class of events the reverse sweep covers: self-gravitation, a solid
+// inner core, no ocean, the receiver at or above the source.
+__device__ __forceinline__ bool pair_adj_supported(const ModelHdr* mh, const EventDev& ev)
+{
+    return ev.grav == 2 && mh->fic == 0 && mh->ocean == 0 && ev.rr >= ev.rs;
+}
+
+// wwb: adjoints of ww(1:5) of pair (l >= 2, j)
+__device__ inline bool pair_toroidal_adj(Ctx& c, const UnitDirs& u, const EventDev& ev, int l, int j,
+                                         const cd* wwb, StepLog& L, SegGrad& G)
+{
+    const cd w = omega_of(ev, j);
+    set_l(c, l);
+    set_omega(c, w);
+    cd svt[5][2], ytor[2][2];
+    source_vector_tor(c, ev.is, ev.rs, ev.mm, svt);
+    tor_solver(c, ev.rr, ev.rs, ev.ir, ev.is, ytor);
+    const cd f = out_factor(ev.out, w);
+    if (ev.out != 0)
+        for (int a = 0; a < 2; a++)
+            for (int b = 0; b < 2; b++) ytor[a][b] = f * ytor[a][b];
+    const double zeta = (double)sqrtf((float)(l * (l + 1)));
+    const double zr = zeta * ev.rr;
+    // ww[q] = (svt[q][0] ytor[0][0] + svt[q][1] ytor[0][1]) / zr
+    cd svtb[5][2], yb[2][2] = {{mk(0.0), mk(0.0)}, {mk(0.0), mk(0.0)}};
+    for (int q = 0; q < 5; q++) {
+        const cd g = wwb[q] / zr;
+        svtb[q][0] = g * ytor[0][0];
+        svtb[q][1] = g * ytor[0][1];
+        yb[0][0] = yb[0][0] + g * svt[q][0];
+        yb[0][1] = yb[0][1] + g * svt[q][1];
+    }
+    if (ev.out != 0)
+        for (int a = 0; a < 2; a++)
+            for (int b = 0; b < 2; b++) yb[a][b] = f * yb[a][b];
+    source_adj(c, u, ev.is, ev.rs, ev.mm, svtb, nullptr, G);
+    set_l(c, l);
+    set_omega(c, w);
+    return tor_solver_adj(c, u, ev.rr, ev.rs, ev.ir, ev.is, yb, L, G);
+}
+
+// uub, vvb: adjoints of uu(1:5), vv(1:5) of pair (l >= 1, j)
+__device__ inline bool pair_spheroidal_adj(Ctx& c, const UnitDirs& u, const EventDev& ev, int l, int j,
+                                           const cd* uub, const cd* vvb, StepLog& L, SegGrad& G)
+{
+    const cd w = omega_of(ev, j);
+    set_l(c, l);
+    set_omega(c, w);
+    alpha_steps(c);
+    cd svs[5][6], ysph[6][4], y0[6][4];
+    source_vector_sph(c, ev.is, ev.rs, ev.mm, svs);
+    sph_solver_g(c, ev.rr, ev.rs, ev.ir, ev.is, ysph);
+    for (int a = 0; a < 6; a++)
+        for (int b = 0; b < 4; b++) y0[a][b] = ysph[a][b];
+    const double zeta = (double)sqrtf((float)(l * (l + 1)));
+    const cd mw2 = -(w * w);
+    const double gr = ev.grav_ir;
+    if (ev.out == 1) {
+        const cd f = imul(w);
+        for (int b = 0; b < 4; b++)
+            for (int a = 0; a < 3; a++) ysph[a][b] = f * ysph[a][b];
+    } else if (ev.out == 2) {
+        if (ev.cor == 0) {
+            for (int b = 0; b < 4; b++)
+                for (int a = 0; a < 3; a++) ysph[a][b] = mw2 * ysph[a][b];
+        } else {
+            for (int b = 0; b < 4; b++) {
+                const cd c1 = (-((double)(l + 1) * ysph[2][b] + (2.0 * gr) * ysph[0][b])) / ev.rr;
+                const cd c2 = (zeta * (ysph[2][b] + gr * ysph[0][b])) / ev.rr;
+                ysph[0][b] = mw2 * ysph[0][b] + c1;
+                ysph[1][b] = mw2 * ysph[1][b] + c2;
+            }
+        }
+    }
+    const double zr = zeta * ev.rr;
+    const int col[4] = {0, 1, 3, 4};
+    // uu[q] = sum_b ysph[0][b] svs[q][col b] / rr;  vv[q] = sum_b ysph[1][b] svs[q][col b] / zr
+    cd svsb[5][6], yb[6][4];
+    for (int q = 0; q < 5; q++)
+        for (int b = 0; b < 6; b++) svsb[q][b] = mk(0.0);
+    for (int a = 0; a < 6; a++)
+        for (int b = 0; b < 4; b++) yb[a][b] = mk(0.0);
+    for (int q = 0; q < 5; q++) {
+        const cd gu = uub[q] / ev.rr, gv = vvb[q] / zr;
+        for (int b = 0; b < 4; b++) {
+            svsb[q][col[b]] = svsb[q][col[b]] + gu * ysph[0][b] + gv * ysph[1][b];
+            yb[0][b] = yb[0][b] + gu * svs[q][col[b]];
+            yb[1][b] = yb[1][b] + gv * svs[q][col[b]];
+        }
+    }
+    // output scaling and the potential / tilt correction (yspec.f90:376-391)
+    if (ev.out == 1) {
+        const cd f = imul(w);
+        for (int b = 0; b < 4; b++)
+            for (int a = 0; a < 3; a++) yb[a][b] = f * yb[a][b];
+    } else if (ev.out == 2) {
+        if (ev.cor == 0) {
+            for (int b = 0; b < 4; b++)
+                for (int a = 0; a < 3; a++) yb[a][b] = mw2 * yb[a][b];
+        } else {
+            double gb = 0.0;
+            for (int b = 0; b < 4; b++) {
+                const cd a0 = yb[0][b], a1 = yb[1][b];
+                // y0' = mw2 y0 - ((l+1) y2 + 2 g y0) / rr;  y1' = mw2 y1 + zeta (y2 + g y0) / rr
+                yb[0][b] = a0 * (mw2 - (2.0 * gr) / ev.rr) + a1 * (zeta * gr / ev.rr);
+                yb[1][b] = a1 * mw2;
+                yb[2][b] = yb[2][b] + a0 * (-(double)(l + 1) / ev.rr) + a1 * (zeta / ev.rr);
+                gb += re(a0 * (-2.0 * y0[0][b] / ev.rr)) + re(a1 * (zeta * y0[0][b] / ev.rr));
+            }
+            // grav(ir) is the c0 coefficient of segment ir
+            double vb[NPARAM];
+            for (int p = 0; p < NPARAM; p++) vb[p] = 0.0;
+            vb[P_GRAV] = gb;
+            G.add(ev.ir, 0.0, vb);
+        }
+    }
+    source_adj(c, u, ev.is, ev.rs, ev.mm, nullptr, svsb, G);
+    set_l(c, l);
+    set_omega(c, w);
+    alpha_steps(c);
+    return sph_solver_g_adj(c, u, ev.rr, ev.rs, ev.ir, ev.is, yb, L, G);
+}
+
+}  // namespace v_local
+}  // namespace ysg

@@ -5,8 +5,53 @@
 // variants (:640-1740) and source_vector_{tor,rad,sph} (:145-215, :566-627,
 // :1747-1847), plus the per-(omega,l) epilogue of yspec.f90:263-400 (output
 // type scaling, potential/tilt correction, uu/vv/ww coefficients).
-#pragma once
 #include "ysg_ode.cuh"
+// one copy per build form, as ysg_ode.cuh
+#undef YSG_SOLVERS_BODY
+#if YSG_TANGENT
+#ifndef YSG_SOLVERS_DONE_v_tangent
+#define YSG_SOLVERS_DONE_v_tangent
+#define YSG_SOLVERS_BODY
+#endif
+#elif YSG_COUNT_ONLY
+#ifndef YSG_SOLVERS_DONE_v_count
+#define YSG_SOLVERS_DONE_v_count
+#define YSG_SOLVERS_BODY
+#endif
+#elif YSG_SMEM_STAGES
+#ifndef YSG_SOLVERS_DONE_v_smem
+#define YSG_SOLVERS_DONE_v_smem
+#define YSG_SOLVERS_BODY
+#endif
+#else
+#ifndef YSG_SOLVERS_DONE_v_local
+#define YSG_SOLVERS_DONE_v_local
+#define YSG_SOLVERS_BODY
+#endif
+#endif
+// Helpers on the event and plain complex values only, the same in every
+// form, so they sit outside the per-form namespaces.
+#ifndef YSG_SOLVERS_COMMON
+#define YSG_SOLVERS_COMMON
+namespace ysg {
+
+__device__ __forceinline__ cd omega_of(const EventDev& ev, int j)
+{
+    // w = wmin + (j-1)*dw - i*ep, formed without contraction (yspec.f90:261)
+    const int k = ev.jofs + (j - 1) * ev.jstride;       // index in the full band
+    return mk(__dadd_rn(ev.wmin, __dmul_rn((double)k, ev.dw)), -ev.ep);
+}
+
+__device__ __forceinline__ cd out_factor(int out, cd w)
+{
+    // multiply by i*w (velocity) or -w*w (acceleration), yspec.f90:284-288
+    return out == 1 ? imul(w) : (out == 2 ? -(w * w) : mk(1.0));
+}
+
+}  // namespace ysg
+#endif  // YSG_SOLVERS_COMMON
+
+#ifdef YSG_SOLVERS_BODY
 
 namespace ysg {
 inline namespace YSG_VARIANT {
@@ -489,19 +534,6 @@ __device__ __forceinline__ mreal grav_at_receiver(const Ctx& c, const EventDev& 
 #endif
 }
 
-__device__ __forceinline__ cd omega_of(const EventDev& ev, int j)
-{
-    // w = wmin + (j-1)*dw - i*ep, formed without contraction (yspec.f90:261)
-    const int k = ev.jofs + (j - 1) * ev.jstride;       // index in the full band
-    return mk(__dadd_rn(ev.wmin, __dmul_rn((double)k, ev.dw)), -ev.ep);
-}
-
-__device__ __forceinline__ cd out_factor(int out, cd w)
-{
-    // multiply by i*w (velocity) or -w*w (acceleration), yspec.f90:284-288
-    return out == 1 ? imul(w) : (out == 2 ? -(w * w) : mk(1.0));
-}
-
 // l == 0: radial mode, yspec.f90:263-293
 __device__ inline void pair_radial(Ctx& c, const EventDev& ev, int j, mcplx* coef)
 {
@@ -590,3 +622,4 @@ __device__ inline void pair_spheroidal(Ctx& c, const EventDev& ev, int l, int j,
 
 }  // inline namespace
 }  // namespace ysg
+#endif  // YSG_SOLVERS_BODY
