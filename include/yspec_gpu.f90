@@ -16,7 +16,7 @@ module yspec_gpu
 
   integer(c_int), parameter :: YSG_OK = 0, YSG_ERR_ARG = 1, YSG_ERR_CUDA = 2, &
        YSG_ERR_NO_MODEL = 3, YSG_ERR_NO_SPECTRA = 4, YSG_ERR_DEVICE_WAIT = 5, &
-       YSG_ERR_NO_DEVICE = 6, YSG_ERR_LIMIT = 7
+       YSG_ERR_NO_DEVICE = 6, YSG_ERR_LIMIT = 7, YSG_ERR_UNSUPPORTED = 8
 
   ! module_model.f90:118-160 after read_model: pointers to nknot doubles each;
   ! val/cs: rho, acon, ccon, fcon, lcon, ncon, kappa, mu, qkappa, qmu, grav,
@@ -104,6 +104,18 @@ module yspec_gpu
        type(c_ptr), intent(in) :: outs(*)
        integer(c_int), intent(out) :: nouts(*)
      end function ysg_batch_run
+
+     ! dL/dval(p, i), dL/dcs(p, i) of L = sum gout * traces (reverse mode):
+     ! gout(nout, 4, nr) as ysg_event_run's out; gval, gcs (nknot, 13)
+     integer(c_int) function ysg_event_gradient(h, ev, tm, gout, gval, gcs) &
+          bind(C, name="ysg_event_gradient")
+       import :: c_int, c_ptr, c_double, ysg_event, ysg_time
+       type(c_ptr), value :: h
+       type(ysg_event), intent(in) :: ev
+       type(ysg_time), intent(in) :: tm
+       real(c_double), intent(in) :: gout(*)
+       real(c_double), intent(out) :: gval(*), gcs(*)
+     end function ysg_event_gradient
 
      ! 0 plain, 1 batched persistent (default), 2 tangent-linear
      integer(c_int) function ysg_set_solver(h, which) bind(C, name="ysg_set_solver")

@@ -37,7 +37,8 @@ enum {
     YSG_ERR_NO_SPECTRA = 4,   /* traces requested before spectra */
     YSG_ERR_DEVICE_WAIT = 5,  /* a bounded device-side wait gave up */
     YSG_ERR_NO_DEVICE = 6,    /* no CUDA device */
-    YSG_ERR_LIMIT = 7         /* size beyond a fixed capacity */
+    YSG_ERR_LIMIT = 7,        /* size beyond a fixed capacity */
+    YSG_ERR_UNSUPPORTED = 8   /* a path the reverse-mode solver does not cover */
 };
 
 typedef struct ysg_handle ysg_handle;
@@ -112,6 +113,25 @@ int ysg_model_tangent_upload(ysg_handle *h, const ysg_model *dm);
  * than 65535 slots, or events of 2^23 degrees or 2^24 frequencies, return
  * YSG_ERR_LIMIT. */
 int ysg_model_tangents_upload(ysg_handle *h, int ndir, const ysg_model *dms);
+
+/* Gradient of the misfit functional L = sum gout * traces of one event
+ * with respect to the uploaded model (reverse mode: the discrete adjoint of
+ * every (omega, l) solve, after the transposes of the time stage and of the
+ * l-sum).  gout is (nout, 4, nr) column-major like ysg_event_run's out
+ * (column 0, time, is ignored): dL/d(trace sample).  gval and gcs receive
+ * dL/dval[p][i] and dL/dcs[p][i] at gval[p * nknot + i] (13 * nknot
+ * doubles each): the gradient with respect to the knot values and spline
+ * second derivatives of ysg_model, the arrays read_model forms
+ * (module_model.f90:175-383).  As for the tangent-linear solver, start
+ * levels, step counts and rescaling are those of the uploaded model (they
+ * are piecewise constant in it) and alpha / beta are not differentiated.
+ * Covers self-gravitation (grav 2) with a solid inner core, no ocean and
+ * the receivers at or above the source; other events return
+ * YSG_ERR_UNSUPPORTED.  No reference counterpart: the reference has no
+ * derivatives.  Stage times (ysg_last_timings): Legendre table, reverse
+ * sweeps, l-sum transpose, time-stage transpose. */
+int ysg_event_gradient(ysg_handle *h, const ysg_event *ev, const ysg_time *tm, const double *gout,
+                       double *gval, double *gcs);
 
 /* Spectra of one event: yspec.f90:250-426.  ur, ut, up are complex
  * (nw, nr) column-major host arrays (interleaved re/im), or NULL to keep

@@ -15,16 +15,21 @@ batched solve launch, one CUDA graph).  `MomentTensorSynthetics` is a
 torch.autograd.Function over them.  Its backward is the exact adjoint of
 the linear map, dL/dmm_i = <dL/dtraces, G_i> / moment_norm.
 
-Gradients with respect to the earth model (per-knot rho, Vp, Vs) come from
+Gradients with respect to the earth model (per-knot rho, Vp, Vs) come in
+reverse mode by default: Engine.gradient (ysg_event_gradient) carries the
+trace adjoint back through the time stage and the l-sum (their transposes)
+and through every (omega, l) solve (its discrete adjoint, k_solve_adjoint.cu)
+to dL/d(knot arrays), and torch autograd takes it through the model chain
+(model_chain.KnotModel.arrays) to rho, Vp and Vs: one reverse sweep per
+pair, whatever the number of parameters.  The forward-mode alternative is
 the tangent-linear solver (k_solve_tangent.cu): the per-pair solve compiled
 with dual numbers returns the derivative of every coefficient along one
-direction of the model, and the stages after it are linear, so a run with
-solver "tangent" returns the derivative of the traces along that direction
-(forward mode).  `ModelSynthetics` sweeps the 3 nknot knot parameters in
-its backward pass and contracts each derivative with the incoming gradient.
-The model arrays and their derivatives come from model_chain.KnotModel;
-start levels and step counts stay those of the deck's model (they are
-piecewise constant in the parameters).
+direction of the model, so a run with solver "tangent" returns the
+derivative of the traces along that direction; `ModelSynthetics(...,
+method="tangent")` sweeps the 3 nknot knot parameters that way, and events
+the reverse solver does not cover fall back to it.  Start levels and step
+counts stay those of the deck's model in both (they are piecewise constant
+in the parameters).
 """
 from __future__ import annotations
 
@@ -188,14 +193,22 @@ class ModelSynthetics:
 
     Forward: the six unit-moment responses of the model at (rho, vp, vs), one
     batched launch, combined with mm.  Backward: mm exactly as
-    MomentTensorSynthetics; each knot parameter by a tangent-linear solve
-    along it (3 nknot directions, or those of `knots` only: the others get
-    zero), `chunk` directions per batched launch.
+    MomentTensorSynthetics; the knot parameters by the reverse sweep
+    (method "adjoint": one Engine.gradient call and autograd through the
+    model chain), or by a tangent-linear solve per knot parameter (method
+    "tangent", `chunk` directions per batched launch; also the fallback for
+    events the reverse sweep does not cover).  With `knots`, only those
+    knots' parameters get a gradient, the others zero.
     """
 
-    def __init__(self, engine: Engine, event: Event, knot_model, knots=None, chunk: int = 64):
+    def __init__(self, engine: Engine, event: Event, knot_model, knots=None, chunk: int = 64,
+                 method: str = "adjoint"):
+        if method not in ("adjoint", "tangent"):
+            raise ValueError("method must be 'adjoint' or 'tangent'")
         self.engine, self.event, self.km = engine, event, knot_model
         self.chunk = chunk
+        self.method = method
+        self.last_method = None
         self.moment_norm = norms()["moment_norm"]
         n = knot_model.nknot
         self.columns = (list(range(3 * n)) if knots is None else
@@ -220,6 +233,50 @@ class ModelSynthetics:
 
     def _knot_gradient(self, rho, vp, vs, mm, grad):
         """sum over traces of grad * d(traces)/d(parameter), per knot parameter."""
+        if self.method == "adjoint":
+            try:
+                out = self._knot_gradient_reverse(rho, vp, vs, mm, grad)
+                self.last_method = "adjoint"
+                return out
+            except N.YspecError as e:
+                if e.status != N.YSG_ERR_UNSUPPORTED:
+                    raise
+        self.last_method = "tangent"
+        return self._knot_gradient_tangent(rho, vp, vs, mm, grad)
+
+    def _knot_gradient_reverse(self, rho, vp, vs, mm, grad):
+        """Reverse mode: dL/d(knot arrays) from Engine.gradient, then the
+        transpose of the model chain by autograd."""
+        import torch
+
+        from .model_chain import PARAMS
+
+        km, eng = self.km, self.engine
+        p = (rho.detach().cpu(), vp.detach().cpu(), vs.detach().cpu())
+        ev = with_moment(self.event, [float(x) for x in mm.detach()])
+        g = np.asarray(grad.detach().cpu().numpy(), dtype=np.float64)
+        gout = np.zeros((g.shape[0], 4, g.shape[2]))
+        gout[:, 1:4, :] = g
+        eng.upload(km.array_model(*p))
+        gval, gcs = eng.gradient(ev, gout)
+        # autograd runs backward passes with gradients off; the chain's own
+        # graph is needed here
+        with torch.enable_grad():
+            pp = tuple(x.clone().requires_grad_() for x in p)
+            arrs = km.arrays(*pp)
+            s = sum((torch.from_numpy(gval[i]) * arrs[name]).sum() +
+                    (torch.from_numpy(gcs[i]) * arrs[name + "_cs"]).sum() for i, name in enumerate(PARAMS))
+            gr = torch.autograd.grad(s, pp, allow_unused=True)
+        n = km.nknot
+        out = torch.cat([x if x is not None else torch.zeros(n, dtype=torch.float64) for x in gr])
+        if len(self.columns) != 3 * n:
+            keep = torch.zeros(3 * n, dtype=torch.bool)
+            keep[self.columns] = True
+            out = torch.where(keep, out, torch.zeros_like(out))
+        return out.detach()
+
+    def _knot_gradient_tangent(self, rho, vp, vs, mm, grad):
+        """Forward mode: one tangent-linear solve per knot parameter."""
         import torch
 
         km, eng = self.km, self.engine

@@ -129,6 +129,7 @@ class Engine:
 
     def __init__(self, device: int = 0, solver: str = "batched"):
         self.h = C.c_void_p()
+        self._nknot = 0
         N.check(N.lib().ysg_create(C.byref(self.h), device), "ysg_create")
         self.solver = solver
         self.set_solver(solver)
@@ -165,6 +166,7 @@ class Engine:
         returns a filled N.YsgModel (yspec_b200.model_chain.ArrayModel)."""
         v = model.view()
         N.check(N.lib().ysg_model_upload(self.h, C.byref(v)), "model_upload")
+        self._nknot = v.nknot
 
     def upload_tangent(self, dmodel) -> None:
         """Derivative of the uploaded model along one direction (an object with
@@ -238,6 +240,23 @@ class Engine:
         nouts = (C.c_int * nev)()
         N.check(N.lib().ysg_batch_run(self.h, nev, evs, tms, ptrs, nouts), "batch_run")
         return outs
+
+    def gradient(self, event: Event, gout: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
+        """Reverse mode: the gradient of L = sum(gout * traces) with respect to
+        the uploaded model's knot arrays.  gout is (nr, 4, nout) like run()'s
+        output (column 0, time, ignored).  Returns (gval, gcs), each (13, nknot):
+        dL/d(knot value) and dL/d(spline second derivative) per parameter, in
+        the order of model_chain.PARAMS.  Raises for paths the reverse solver
+        does not cover (status 8)."""
+        g = np.ascontiguousarray(gout, dtype=np.float64)
+        if g.shape != (event.nr, 4, event.nout()):
+            raise ValueError("gout must be (nr, 4, nout)")
+        n = self._nknot
+        gval = np.zeros((13, n))
+        gcs = np.zeros((13, n))
+        N.check(N.lib().ysg_event_gradient(self.h, C.byref(event.raw.ev), C.byref(event.raw.tm), N.dptr(g),
+                                           N.dptr(gval), N.dptr(gcs)), "event_gradient")
+        return gval, gcs
 
     def coef(self, event: Event) -> np.ndarray:
         buf = np.zeros((event.L, 15, event.nw, 2))

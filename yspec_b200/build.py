@@ -38,6 +38,7 @@ SOURCES = [
     CSRC / "k_solve_plain.cu",
     CSRC / "k_solve_batched.cu",
     CSRC / "k_solve_tangent.cu",
+    CSRC / "k_solve_adjoint.cu",
     CSRC / "k_schedule.cu",
     CSRC / "k_legendre.cu",
     CSRC / "k_lsum.cu",

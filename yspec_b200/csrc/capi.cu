@@ -101,9 +101,15 @@ struct ysg_handle {
     ModelHdr hdr{};
     std::vector<double> grav_host;   // knot gravity for the tilt correction
     std::vector<double> r_host;      // knot radii of the uploaded model
+    std::vector<double> alpha_host;  // knot alpha (step counts) of the uploaded model
     bool has_model = false;
     DevBuf dkn, dsg;                 // model derivatives (directions) for the tangent solver
     int ndir = 0;                    // directions loaded; 0 = none
+    // reverse mode: unit directions of the model (built on first use after
+    // an upload), time-stage basis, adjoint buffers and sweep work space
+    DevBuf ukn, usg;
+    bool has_units = false;
+    DevBuf abasis, about, ascr, acs0, agout, asbar, acoefb, agrad, alogs;
     // events
     std::vector<Slot> slots;
     int nactive = 0;                 // slots of the last prepare / batch
@@ -831,6 +837,66 @@ void build_tables(int n, const double* r, const double* const* val, const double
     for (int p = 0; p < NPARAM; p++) seg[(size_t)n].c[p][0] = rec[(size_t)n].v[p][0];
 }
 
+// Unit model directions of the reverse sweep (UnitDirs), one knot and one
+// segment table per parameter, built once per uploaded model.
+int ensure_units(ysg_handle* h)
+{
+    if (h->has_units) return YSG_OK;
+    const int n = h->hdr.nknot;
+    const size_t nk = (size_t)n + 2, ns = (size_t)n + 1;
+    std::vector<Knot> rec_all(nk * NPARAM);
+    std::vector<Seg> seg_all(ns * NPARAM);
+    const std::vector<double> one((size_t)n, 1.0), zero((size_t)n, 0.0);
+    for (int p = 0; p < NPARAM; p++) {
+        const double* val[NPARAM];
+        const double* cs[NPARAM];
+        for (int q = 0; q < NPARAM; q++) {
+            val[q] = q == p ? one.data() : zero.data();
+            cs[q] = zero.data();
+        }
+        std::vector<Knot> rec;
+        std::vector<Seg> seg;
+        build_tables(n, h->r_host.data(), val, cs, nullptr, nullptr, rec, seg);
+        std::copy(rec.begin(), rec.end(), rec_all.begin() + (ptrdiff_t)(nk * p));
+        std::copy(seg.begin(), seg.end(), seg_all.begin() + (ptrdiff_t)(ns * p));
+    }
+    CK(h->ukn.ensure(rec_all.size() * sizeof(Knot)));
+    CK(h->usg.ensure(seg_all.size() * sizeof(Seg)));
+    CK(cudaMemcpyAsync(h->ukn.p, rec_all.data(), rec_all.size() * sizeof(Knot), cudaMemcpyHostToDevice, h->st));
+    CK(cudaMemcpyAsync(h->usg.p, seg_all.data(), seg_all.size() * sizeof(Seg), cudaMemcpyHostToDevice, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    h->has_units = true;
+    return YSG_OK;
+}
+
+// Capacities of the reverse sweep's logs for an event.  Steps: a yint takes
+// 2 + floor(length / drr) - 1 steps on each interval it crosses, with
+// drr = max(alpha_i, alpha_i+1) / (4 Re omega) (module_int.f90:2121-2138),
+// never more than on the whole interval at the band's largest frequency;
+// one more per interval covers rounding.  Grid points of the l = 0 gravity
+// solve: floor(length / dr) + 2 per piece, at most three pieces per interval
+// (split at the source and the receiver), dr = alpha_min / (4 Re omega) or
+// 1/4 at omega = 0 (module_model.f90:578-787 with module_int.f90:1145-1166).
+void adj_bounds(const ysg_handle* h, const EventDev& d, int* nmax, int* gmax)
+{
+    const int n = h->hdr.nknot;
+    const double* r = h->r_host.data();
+    const double* al = h->alpha_host.data();
+    const double w = d.wmin + (double)(d.jofs + (d.nw - 1) * d.jstride) * d.dw;
+    const double amin = al[h->hdr.imin_alpha - 1];
+    const double dr = w > 0.0 ? std::min(0.25, amin / (4.0 * w)) : 0.25;
+    double steps = 0.0, pts = 0.0;
+    for (int i = 1; i <= n - 1; i++) {
+        const double hh = r[i] - r[i - 1];
+        if (hh == 0.0) continue;
+        const double drr = std::max(al[i - 1], al[i]) / (4.0 * w);
+        steps += 2.0 + std::floor(hh / drr);
+        pts += 8.0 + std::floor(hh / dr);
+    }
+    *nmax = (int)std::min(steps + 2.0, 1.0e8);
+    *gmax = (int)std::min(pts + 4.0, 1.0e8);
+}
+
 }  // namespace
 
 extern "C" {
@@ -848,6 +914,7 @@ const char* ysg_status_string(int s)
         case YSG_ERR_DEVICE_WAIT: return "a bounded device-side wait gave up";
         case YSG_ERR_NO_DEVICE: return "no CUDA device";
         case YSG_ERR_LIMIT: return "size beyond a fixed capacity";
+        case YSG_ERR_UNSUPPORTED: return "path not covered by the reverse-mode solver";
         default: return "unknown status";
     }
 }
@@ -889,7 +956,8 @@ void ysg_destroy(ysg_handle* h)
     for (Slot& s : h->slots) s.release();
     for (DevBuf* b : {&h->kn, &h->sg, &h->hdr_dev, &h->offs, &h->keys0, &h->keys1, &h->vals0,
                       &h->vals1, &h->sort_tmp, &h->work, &h->status, &h->items, &h->counter,
-                      &h->evdev, &h->coefptr})
+                      &h->evdev, &h->coefptr, &h->dkn, &h->dsg, &h->ukn, &h->usg, &h->abasis,
+                      &h->about, &h->ascr, &h->acs0, &h->agout, &h->asbar, &h->acoefb, &h->agrad, &h->alogs})
         b->release();
     for (DevBuf& b : h->scratch) b.release();
     for (auto& e : h->ev)
@@ -983,8 +1051,10 @@ int ysg_model_upload(ysg_handle* h, const ysg_model* m)
     h->hdr = hd;
     h->grav_host.assign(m->val[P_GRAV], m->val[P_GRAV] + n);
     h->r_host.assign(m->r, m->r + n);
+    h->alpha_host.assign(m->alpha, m->alpha + n);
     h->has_model = true;
     h->ndir = 0;
+    h->has_units = false;
     h->has_spectra = false;
     for (Slot& s : h->slots) s.ev_ready = s.tm_ready = false;
     return YSG_OK;
@@ -1061,6 +1131,180 @@ int ysg_event_coef(ysg_handle* h, const ysg_event* ev, double* coef)
     rc = finish(h, 1, true, false);
     h->has_spectra = false;
     return rc;
+}
+
+int ysg_event_gradient(ysg_handle* h, const ysg_event* ev, const ysg_time* tm, const double* gout, double* gval,
+                       double* gcs)
+{
+    int rc = check_event(h, ev);
+    if (rc) return rc;
+    if (!tm || !gval || !gcs || tm->nr != ev->nr || (ev->nr > 0 && !gout)) return YSG_ERR_ARG;
+    if (ev->grav != 2 || h->hdr.fic != 0 || h->hdr.ocean != 0 || ev->rr < ev->rs) return YSG_ERR_UNSUPPORTED;
+    const int L = ev->lmax - ev->lmin + 1;
+    if (L >= (1 << 23) || L > 65535 || ev->nw >= (1 << 24) || ev->nr > 65535) return YSG_ERR_LIMIT;
+    cudaSetDevice(h->device);
+    h->has_spectra = false;
+    h->launches = 0;
+    h->h2d = h->d2h = 0.0;
+    Slot& s = slot0(h);
+    rc = upload_event(h, s, ev);
+    if (!rc) rc = upload_time(h, s, tm, ev->nw);
+    if (!rc) rc = upload_batch_items(h, 1);
+    if (!rc) rc = ensure_units(h);
+    if (rc) return rc;
+    h->nactive = 1;
+    const int n = h->hdr.nknot, nw = ev->nw, nr = ev->nr;
+    const TraceDev& td = s.ptd;
+    const int nout = td.nout;
+    int nmax = 0, gmax = 0;
+    adj_bounds(h, s.pev, &nmax, &gmax);
+    // sweep work space: every resident thread of the l >= 1 sweeps (step
+    // logs only) and one thread per frequency of the l = 0 sweeps (step and
+    // grid logs), within a quarter of the free memory
+    int nblk = solve_adjoint_blocks();
+    if (nblk <= 0) return YSG_ERR_CUDA;
+    size_t free_b = 0, total_b = 0;
+    CK(cudaMemGetInfo(&free_b, &total_b));
+    const size_t per = adj_log_bytes(nmax, 0), per_r = adj_log_bytes(nmax, gmax);
+    const size_t Tr = ev->lmin == 0 ? (size_t)(nw + ADJ_THREADS - 1) / ADJ_THREADS * ADJ_THREADS : 0;
+    const size_t budget = (free_b + h->alogs.cap) / 4;
+    while (nblk > 1 && (size_t)nblk * ADJ_THREADS * per + Tr * per_r > budget) nblk--;
+    if ((size_t)nblk * ADJ_THREADS * per + Tr * per_r > budget) return YSG_ERR_LIMIT;
+    const size_t T = (size_t)nblk * ADJ_THREADS;
+    const size_t nspec = (size_t)nw * std::max(nr, 1);
+    const size_t ngrad = (size_t)(n + 1) * NPARAM * 4;
+    CK(h->abasis.ensure((size_t)2 * nw * nw * sizeof(cd)));
+    CK(h->about.ensure((size_t)nout * 4 * 2 * nw * sizeof(double)));
+    CK(h->ascr.ensure(std::max<size_t>(ifft_scratch_bytes(td.nt, 2 * nw), 16)));
+    CK(h->acs0.ensure((size_t)2 * 2 * nw * sizeof(double)));
+    CK(h->agout.ensure(std::max<size_t>((size_t)nout * 4 * nr * sizeof(double), 16)));
+    CK(h->asbar.ensure(3 * nspec * sizeof(cd)));
+    CK(h->acoefb.ensure((size_t)L * NCOEF * nw * sizeof(cd)));
+    CK(h->agrad.ensure(ngrad * sizeof(double)));
+    CK(h->alogs.ensure(T * per + Tr * per_r));
+    std::vector<double> cs0((size_t)4 * nw);
+    for (int b = 0; b < 2 * nw; b++) {
+        cs0[2 * (size_t)b] = 1.0;
+        cs0[2 * (size_t)b + 1] = 0.0;
+    }
+    CK(cudaMemcpyAsync(h->acs0.p, cs0.data(), cs0.size() * sizeof(double), cudaMemcpyHostToDevice, h->st));
+    if (nr > 0)
+        CK(cudaMemcpyAsync(h->agout.p, gout, (size_t)nout * 4 * nr * sizeof(double), cudaMemcpyHostToDevice, h->st));
+    h->h2d += (double)(cs0.size() * sizeof(double) + (size_t)nout * 4 * nr * sizeof(double));
+    // work space layout per launch: complex arrays, then doubles, then ints
+    unsigned char* base = h->alogs.as<unsigned char>();
+    auto take = [&](size_t bytes) {
+        unsigned char* q = base;
+        base += bytes;
+        return q;
+    };
+    auto carve = [&](size_t nt, int ng) {
+        AdjLogs w{};
+        w.nthreads = (int)nt;
+        w.nmax = nmax;
+        w.gmax = ng;
+        w.ly = reinterpret_cast<cd*>(take((size_t)nmax * 14 * nt * sizeof(cd)));
+        w.gy = reinterpret_cast<cd*>(take((size_t)ng * 4 * nt * sizeof(cd)));
+        w.lx = reinterpret_cast<double*>(take((size_t)nmax * nt * sizeof(double)));
+        w.lh = reinterpret_cast<double*>(take((size_t)nmax * nt * sizeof(double)));
+        w.lf = reinterpret_cast<double*>(take((size_t)nmax * nt * sizeof(double)));
+        w.gr = reinterpret_cast<double*>(take((size_t)ng * nt * sizeof(double)));
+        w.lil = reinterpret_cast<int*>(take((size_t)nmax * nt * sizeof(int)));
+        w.gi = reinterpret_cast<int*>(take((size_t)ng * nt * sizeof(int)));
+        return w;
+    };
+    const AdjLogs w = carve(T, 0);
+    const AdjLogs wr = Tr ? carve(Tr, gmax) : AdjLogs{};
+    UnitDirs u;
+    for (int p = 0; p < NPARAM; p++) {
+        u.kn[p] = h->ukn.as<Knot>() + (size_t)p * (n + 2);
+        u.sg[p] = h->usg.as<Seg>() + (size_t)p * (n + 1);
+    }
+    h->leg_overlap = false;
+    CK(record(h, 0));
+    if (nr > 0) {
+        h->launches += 1;
+        CK(launch_legendre(nr, s.lmax, s.delta.as<double>(), s.ct.as<double>(), s.stv.as<double>(),
+                           s.leg.as<double>(), h->st));
+    }
+    CK(record(h, 1));
+    // time stage on the basis, then its transpose and the l-sum's
+    h->launches += nr > 0 ? 6 : 0;   // basis, pass A, pass B, rotation, spectrum and l-sum transposes
+    if (nr > 0) {
+        CK(launch_time_basis(td, h->abasis.as<cd>(), s.filt.as<double>(), s.tw.as<cd>(), s.expt.as<double>(),
+                             h->acs0.as<double>(), h->ascr.as<cd>(), h->about.as<double>(), h->st));
+        CK(launch_spec_adjoint(nw, nr, nout, h->about.as<double>(), h->agout.as<double>(), s.cs.as<double>(),
+                               h->asbar.as<cd>(), h->st));
+    }
+    CK(record(h, 2));
+    if (nr > 0)
+        CK(launch_lsum_adjoint(nw, nr, ev->lmin, ev->lmax, s.leg.as<double>(), s.E.as<cd>(), h->asbar.as<cd>(),
+                               h->acoefb.as<cd>(), h->st));
+    else
+        CK(cudaMemsetAsync(h->acoefb.p, 0, (size_t)L * NCOEF * nw * sizeof(cd), h->st));
+    CK(record(h, 3));
+    // the pair schedule's cost-sorted entries, then the reverse sweeps
+    StepCost sc;
+    for (int q = 0; q < NSYS_COUNT; q++) sc.flops[q] = kStepFlops[q];
+    sc.base = kPairBaseFlops;
+    unsigned long long* keys[2] = {h->keys0.as<unsigned long long>(), h->keys1.as<unsigned long long>()};
+    unsigned long long* vals[2] = {h->vals0.as<unsigned long long>(), h->vals1.as<unsigned long long>()};
+    unsigned long long* sorted = nullptr;
+    h->launches += 2;                // k_pair_cost and the sweeps (the radix sort is CUB's)
+    CK(launch_pair_schedule(h->kn.as<Knot>(), h->sg.as<Seg>(), h->hdr_dev.as<ModelHdr>(), h->evdev.as<EventDev>(),
+                            h->offs.as<long long>(), 1, h->npairs, sc, keys, vals, h->sort_tmp.p, h->sort_tmp.cap,
+                            &sorted, h->st));
+    CK(cudaMemsetAsync(h->agrad.p, 0, ngrad * sizeof(double), h->st));
+    CK(cudaMemsetAsync(h->status.p, 0, sizeof(int), h->st));
+    // the l = 0 sweeps (few, long) beside the others on a side stream
+    if (Tr) {
+        rc = fork_side(h, 1);
+        if (rc) return rc;
+        h->launches += 1;
+        CK(launch_radial_adjoint(h->kn.as<Knot>(), h->sg.as<Seg>(), h->hdr_dev.as<ModelHdr>(),
+                                 h->evdev.as<EventDev>(), u, h->acoefb.as<cd>(), wr, h->agrad.as<double>(),
+                                 h->status.as<int>(), h->side[0]));
+    }
+    CK(launch_solve_adjoint(h->kn.as<Knot>(), h->sg.as<Seg>(), h->hdr_dev.as<ModelHdr>(), h->evdev.as<EventDev>(), u,
+                            h->acoefb.as<cd>(), sorted, 2 * h->npairs, w, h->agrad.as<double>(),
+                            reinterpret_cast<unsigned long long*>(h->counter.p), h->status.as<int>(), h->st));
+    if (Tr && (rc = join_side(h, 1))) return rc;
+    CK(record(h, 4));
+    std::vector<double> g(ngrad);
+    int status = 0;
+    CK(cudaMemcpyAsync(g.data(), h->agrad.p, ngrad * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+    CK(cudaMemcpyAsync(&status, h->status.p, sizeof status, cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    h->d2h += (double)(ngrad * sizeof(double) + sizeof status);
+    float t[4];
+    CK(cudaEventElapsedTime(&t[0], h->ev[0], h->ev[1]));
+    CK(cudaEventElapsedTime(&t[3], h->ev[1], h->ev[2]));
+    CK(cudaEventElapsedTime(&t[2], h->ev[2], h->ev[3]));
+    CK(cudaEventElapsedTime(&t[1], h->ev[3], h->ev[4]));
+    for (int i = 0; i < 4; i++) h->ms[i] = t[i];
+    h->pairs = (double)L * nw;
+    h->flops = 0.0;
+    if (status) return YSG_ERR_LIMIT;
+    // dL/dc[i][p][k] -> knot values and spline second derivatives, through
+    // the segment formulas of build_tables
+    std::fill(gval, gval + (size_t)NPARAM * n, 0.0);
+    std::fill(gcs, gcs + (size_t)NPARAM * n, 0.0);
+    const double* r = h->r_host.data();
+    for (int i = 1; i <= n; i++)
+        for (int p = 0; p < NPARAM; p++) {
+            const double* c = &g[((size_t)i * NPARAM + p) * 4];
+            double* gv = gval + (size_t)p * n;
+            double* gc = gcs + (size_t)p * n;
+            gv[i - 1] += c[0];
+            if (i == n) continue;
+            const double hh = r[i] - r[i - 1];
+            if (hh == 0.0) continue;
+            gv[i] += c[1] / hh;
+            gv[i - 1] -= c[1] / hh;
+            gc[i - 1] += -c[1] * hh / 3.0 + 0.5 * c[2] - c[3] / (6.0 * hh);
+            gc[i] += -c[1] * hh / 6.0 + c[3] / (6.0 * hh);
+        }
+    return YSG_OK;
 }
 
 int ysg_legendre_table(ysg_handle* h, int nr, int lmax, const double* delta, const double* ct,

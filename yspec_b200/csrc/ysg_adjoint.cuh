@@ -200,12 +200,56 @@ __device__ inline void fluid_amat_adj(const Ctx& c, double rr, const FluidCoefBa
     vb[P_XA2] += re(qab * c.lno);
 }
 
+// module_int.f90:261-304 rad_amat:
+//   t = (1 - 2 F' C'^-1) / r, k = C'^-1, s = -omega^2 rho + 4 (gamma - rho g r) / r^2,
+//   gamma = A' - N' - F'^2 C'^-1, with X' = X (1 + q_X lno)
+__device__ inline void rad_amat_adj(const Ctx& c, double rr, const RadCoefBar& s, double* vb)
+{
+    const Seg& g = c.sg[c.il];
+    const double u = rr - g.r0;
+    const double rrho = seg(g, u, P_RHO), racon = seg(g, u, P_ACON), rccon = seg(g, u, P_CCON);
+    const double rfcon = seg(g, u, P_FCON), rncon = seg(g, u, P_NCON), gg = seg(g, u, P_GRAV);
+    const double rqmu = seg(g, u, P_QMU), rxlam = seg(g, u, P_XLAM), rxa2 = seg(g, u, P_XA2);
+    const cd qaa = 1.0 + rxa2 * c.lno, qff = 1.0 + rxlam * c.lno, qll = 1.0 + rqmu * c.lno;
+    const cd cfcon = rfcon * qff;
+    const cd k = 1.0 / (rccon * qaa);
+    const double ri = 1.0 / rr, ri2 = ri * ri;
+    vb[P_RHO] += re(s.s * (-c.omega2)) + re(s.s) * (-4.0 * gg * rr * ri2);
+    vb[P_GRAV] += re(s.s) * (-4.0 * rrho * rr * ri2);
+    const cd gb = s.s * (4.0 * ri2);
+    // gamma = cacon - cncon - cfcon^2 k
+    const cd cab = gb, cnb = -gb;
+    cd cfb = gb * (-2.0 * (cfcon * k));
+    cd kb = gb * (-(cfcon * cfcon)) + s.k;
+    // t = (1 - 2 cfcon k) ri
+    const cd fcb = s.t * (-2.0 * ri);
+    cfb += fcb * k;
+    kb += fcb * cfcon;
+    vb[P_CCON] += re(kb * (-k / rccon));
+    cd qab = kb * (-k / qaa);
+    vb[P_ACON] += re(cab * qaa);
+    qab += cab * racon;
+    vb[P_FCON] += re(cfb * qff);
+    const cd qfb = cfb * rfcon;
+    vb[P_NCON] += re(cnb * qll);
+    const cd qlb = cnb * rncon;
+    vb[P_XA2] += re(qab * c.lno);
+    vb[P_XLAM] += re(qfb * c.lno);
+    vb[P_QMU] += re(qlb * c.lno);
+}
+
 // The systems the reverse sweep supports, with their coefficient matrices.
 struct TorT {
     using Sys = TorSys;
     using A = TorSysAdj;
     __device__ static TorCoef amat(const Ctx& c, double r) { return tor_amat(c, r); }
     __device__ static void amat_adj(const Ctx& c, double r, const TorCoefBar& s, double* vb) { tor_amat_adj(c, r, s, vb); }
+};
+struct RadT {
+    using Sys = RadSys;
+    using A = RadSysAdj;
+    __device__ static RadCoef amat(const Ctx& c, double r) { return rad_amat(c, r); }
+    __device__ static void amat_adj(const Ctx& c, double r, const RadCoefBar& s, double* vb) { rad_amat_adj(c, r, s, vb); }
 };
 struct MinorSolidGT {
     using Sys = MinorSolidG;
@@ -288,7 +332,9 @@ __device__ void rk_step_adj(const Ctx& c, const cd* y, double x, double h, cd* y
 }
 
 // Work space of one yint sweep: the state before every step, the step's
-// radius, size, interval and rescaling factor.
+// radius, size, interval and rescaling factor.  Entry e of an array sits at
+// e * st, so the logs of the threads of a launch can be interleaved (st =
+// the number of logs, each base pointer offset by its thread's index).
 struct StepLog {
     cd* y;            // nmax x N
     double* x;        // nmax
@@ -296,6 +342,7 @@ struct StepLog {
     int* il;          // nmax
     double* f;        // nmax: factor applied after the step (1, 1e20 or 1e-20)
     int nmax;
+    int st;
 };
 
 // The forward yint of ysg_ode.cuh (same intervals, step counts and
@@ -332,10 +379,11 @@ __device__ bool yint_adj(Ctx& c, int i1, int i2, double r1, double r2, const cd*
         for (int j = 1; j <= n - 1; j++) {
             if (ns >= L.nmax) return false;
             double rr = __dadd_rn(rr1, __dmul_rn((double)(j - 1), drr));
-            for (int k = 0; k < N; k++) L.y[(size_t)ns * N + k] = y[k];
-            L.x[ns] = rr;
-            L.h[ns] = drr;
-            L.il[ns] = i;
+            const size_t e = (size_t)ns * L.st;
+            for (int k = 0; k < N; k++) L.y[((size_t)ns * N + k) * L.st] = y[k];
+            L.x[e] = rr;
+            L.h[e] = drr;
+            L.il[e] = i;
             rkck_step<typename T::Sys>(c, y, rr, drr);
             double f = 1.0;
             if (scaled) {
@@ -343,16 +391,19 @@ __device__ bool yint_adj(Ctx& c, int i1, int i2, double r1, double r2, const cd*
                 rescale<N>(y, &sc);
                 f = sc > 0 ? SC_HUGE : (sc < 0 ? SC_TINY : 1.0);
             }
-            L.f[ns] = f;
+            L.f[e] = f;
             ns++;
         }
     }
     for (int q = ns - 1; q >= 0; q--) {
-        c.il = L.il[q];
-        const double f = L.f[q];
+        const size_t e = (size_t)q * L.st;
+        c.il = L.il[e];
+        const double f = L.f[e];
         if (f != 1.0)
             for (int k = 0; k < N; k++) yb[k] = f * yb[k];
-        rk_step_adj<T>(c, L.y + (size_t)q * N, L.x[q], L.h[q], yb, G);
+        cd ys[N];
+        for (int k = 0; k < N; k++) ys[k] = L.y[((size_t)q * N + k) * L.st];
+        rk_step_adj<T>(c, ys, L.x[e], L.h[e], yb, G);
     }
     return true;
 }

@@ -81,4 +81,53 @@ cudaError_t launch_ifft(const TraceDev& td, const cd* ur, const cd* ut, const cd
                         const double* filt, const cd* tw, const double* expt,
                         const double* cs_azep, cd* scratch, double* out, cudaStream_t s);
 
+// Reverse mode (k_solve_adjoint.cu).  Work space of the reverse sweeps,
+// interleaved over threads: thread t's step log (nmax steps) and grid log
+// (gmax points of the l = 0 gravity solve), entry e of an array at
+// e * nthreads + t.
+constexpr int ADJ_THREADS = 128;
+struct AdjLogs {
+    cd* ly;            // nmax x 14 states
+    double* lx;        // nmax radii
+    double* lh;        // nmax step sizes
+    int* lil;          // nmax intervals
+    double* lf;        // nmax rescaling factors
+    int nmax;
+    cd* gy;            // gmax x 4 states
+    double* gr;        // gmax radii
+    int* gi;           // gmax intervals
+    int gmax;
+    int nthreads;      // a multiple of ADJ_THREADS
+};
+inline size_t adj_log_bytes(int nmax, int gmax)
+{
+    return (size_t)nmax * (14 * sizeof(cd) + 3 * sizeof(double) + sizeof(int)) +
+           (size_t)gmax * (4 * sizeof(cd) + sizeof(double) + sizeof(int));
+}
+// resident blocks of k_solve_adjoint over the device (0 on failure)
+int solve_adjoint_blocks();
+// Time stage on the 2 nw basis spectra (k_basis) with azimuth 0: bout
+// (nout, 4, 2 nw); basis holds 2 nw * nw complex, scratch
+// ifft_scratch_bytes(nt, 2 nw) bytes, cs0 2 nw (cos, sin) = (1, 0) pairs.
+cudaError_t launch_time_basis(const TraceDev& td, cd* basis, const double* filt, const cd* tw,
+                              const double* expt, const double* cs0, cd* scratch, double* bout, cudaStream_t st);
+// Trace adjoint gout (nout, 4, nr) -> spectrum adjoints sbar (3 x (nw, nr)).
+cudaError_t launch_spec_adjoint(int nw, int nr, int nout, const double* bout, const double* gout, const double* cs,
+                                cd* sbar, cudaStream_t st);
+// Spectrum adjoints -> coefficient adjoints coefb ((nw, 15, L) complex).
+cudaError_t launch_lsum_adjoint(int nw, int nr, int lmin, int lmax, const double* T, const cd* E, const cd* sbar,
+                                cd* coefb, cudaStream_t st);
+// Reverse sweeps of the l >= 1 entries of `pairs` (one event,
+// launch_pair_schedule's list; w needs no grid log): grad ((nknot + 1) x
+// NPARAM x 4 doubles, zeroed by the caller) receives dL/dc[i][p][k]; status
+// bit 0 is set if a sweep failed.  launch_radial_adjoint: the l = 0 pairs,
+// one thread per frequency (w with grid logs).
+cudaError_t launch_radial_adjoint(const Knot* kn, const Seg* sg, const ModelHdr* mh, const EventDev* ev,
+                                  const UnitDirs& u, const cd* coefb, const AdjLogs& w, double* grad, int* status,
+                                  cudaStream_t st);
+cudaError_t launch_solve_adjoint(const Knot* kn, const Seg* sg, const ModelHdr* mh, const EventDev* ev,
+                                 const UnitDirs& u, const cd* coefb, const unsigned long long* pairs,
+                                 long long nentries, const AdjLogs& w, double* grad,
+                                 unsigned long long* counter, int* status, cudaStream_t st);
+
 }  // namespace ysg

@@ -92,6 +92,14 @@ struct __align__(16) Seg {
 };
 static_assert(sizeof(Seg) == 432, "segment record size");
 
+// Unit model directions of the reverse sweep, one per parameter: knot
+// records with v[p][0] = 1 for parameter p and zero elsewhere, and the
+// segments of the same (c[p][0] = 1).
+struct UnitDirs {
+    const Knot* kn[NPARAM];
+    const Seg* sg[NPARAM];
+};
+
 __device__ __forceinline__ double seg(const Seg& s, double t, int p)
 {
     // two 128-bit loads through the read-only path (the table never changes

@@ -37,13 +37,6 @@
 namespace ysg {
 inline namespace v_local {
 
-// Unit model directions, one per parameter: knot records with v[p][0] = 1
-// for parameter p and zero elsewhere (and the segments of the same).
-struct UnitDirs {
-    const Knot* kn[NPARAM];
-    const Seg* sg[NPARAM];
-};
-
 __device__ inline void tangent_ctx(const Ctx& c, const UnitDirs& u, int p, v_tangent::Ctx& t)
 {
     t.kn = c.kn;
@@ -73,11 +66,11 @@ __device__ inline void tangent_ctx(const Ctx& c, const UnitDirs& u, int p, v_tan
 
 // vb_p += Re(sum_k yb_k dy_k / dv_p) for the start vectors at (i1, rt) and
 // the moments of the result go to G.  WHICH: 0 toroidal (2), 1 solid minor
-// (14), 2 fluid minor (5).
+// (14), 2 fluid minor (5), 3 radial with gravity (2).
 template <int WHICH>
 __device__ inline void start_adj(const Ctx& c, const UnitDirs& u, int i1, double rt, const cd* yb, SegGrad& G)
 {
-    constexpr int N = WHICH == 0 ? 2 : (WHICH == 1 ? 14 : 5);
+    constexpr int N = (WHICH == 0 || WHICH == 3) ? 2 : (WHICH == 1 ? 14 : 5);
     double vb[NPARAM];
     for (int p = 0; p < NPARAM; p++) {
         v_tangent::Ctx t;
@@ -85,7 +78,8 @@ __device__ inline void start_adj(const Ctx& c, const UnitDirs& u, int i1, double
         v_tangent::mcplx y[N];
         if (WHICH == 0) v_tangent::tor_ystart(t, i1, rt, y);
         else if (WHICH == 1) v_tangent::sph_minor_solid_start(t, i1, rt, y);
-        else v_tangent::sph_minor_fluid_start(t, i1, rt, y);
+        else if (WHICH == 2) v_tangent::sph_minor_fluid_start(t, i1, rt, y);
+        else v_tangent::rad_ystart<true>(t, i1, rt, y);
         double s = 0.0;
         for (int k = 0; k < N; k++) s += re(yb[k] * y[k].d);
         vb[p] = s;
@@ -117,6 +111,22 @@ __device__ inline void source_adj(const Ctx& c, const UnitDirs& u, int is, doubl
                 for (int b = 0; b < 6; b++) s += re(svsb[q][b] * svs[q][b].d);
         }
         vb[p] = s;
+    }
+    G.add(is, rs - c.kn[is].r, vb);
+}
+
+// Radial source vector at (is, rs) (module_solver.f90:566-627): s0b holds
+// the adjoints of its two components.
+__device__ inline void source_rad_adj(const Ctx& c, const UnitDirs& u, int is, double rs, const double* mm,
+                                      const cd* s0b, SegGrad& G)
+{
+    double vb[NPARAM];
+    for (int p = 0; p < NPARAM; p++) {
+        v_tangent::Ctx t;
+        tangent_ctx(c, u, p, t);
+        v_tangent::mcplx s0[2];
+        v_tangent::source_vector_rad(t, is, rs, mm, s0);
+        vb[p] = re(s0b[0] * s0[0].d) + re(s0b[1] * s0[1].d);
     }
     G.add(is, rs - c.kn[is].r, vb);
 }
@@ -372,6 +382,185 @@ __device__ inline bool sph_solver_g_adj(Ctx& c, const UnitDirs& u, double rr, do
 // ---------------------------------------------------------------------------
 // The class of events the reverse sweep covers: self-gravitation, a solid
 // inner core, no ocean, the receiver at or above the source.
+// Grid of the l = 0 gravity solve (rad_solver_wg): per grid point k its
+// radius, interval and the upward and downward solutions there.  Entry e
+// of an array sits at e * st, as in StepLog.
+struct GridLog {
+    cd* y;            // nmax x 4: upward y1[0], y1[1], downward y2[0], y2[1]
+    double* r;        // nmax
+    int* i;           // nmax
+    int nmax;
+    int st;
+};
+
+// rad_solver_wg (ysg_solvers.cuh, module_solver.f90:446-561) run forward
+// with every grid point stored, its result in yout, then reversed: yb holds
+// the adjoints of yout.  The grid walk is the forward one, point for point;
+// each piece between grid points is replayed from its stored start by
+// yint_adj.  Returns false if the grid or a piece exceeds the logs, or the
+// receiver is not on the grid.
+__device__ inline bool rad_solver_wg_adj(Ctx& c, const UnitDirs& u, double rr, double rs, const cd yb[2][2],
+                                         cd yout[2][2], StepLog& L, GridLog& GL, SegGrad& G)
+{
+    const ModelHdr* mh = c.mh;
+    const Knot* kn = c.kn;
+    const double drr = c.dr;
+    int ngrid = 0, iss = 0, irr = 0;
+    for (int i = 1; i <= mh->nknot - 1; i++) {
+        double r1 = kn[i].r, r2 = kn[i + 1].r;
+        if (r1 == r2) continue;
+        GridSeg sg[3];
+        int sa, ra;
+        int ns = grid_segs(r1, r2, rs, rr, sg, &sa, &ra);
+        for (int q = 0; q < ns; q++) {
+            ngrid += seg_npts(sg[q], drr) - (sg[q].first - 1);
+            if (q == sa) iss = ngrid;
+            if (q == ra) irr = ngrid;
+        }
+    }
+    if (ngrid + 1 > GL.nmax || iss < 2 || irr < 2) return false;
+    const int st = GL.st;
+    auto gy = [&](int k, int s) -> cd& { return GL.y[((size_t)k * 4 + s) * st]; };
+    // upward through grid points 2..iss
+    cd y1[2], ys[2];
+    double rt = 0.0;
+    {
+        int k = 0, iprev = 0;
+        double rprev = 0.0;
+        for (int i = 1; i <= mh->nknot - 1 && k < iss; i++) {
+            double r1 = kn[i].r, r2 = kn[i + 1].r;
+            if (r1 == r2) continue;
+            GridSeg sg[3];
+            int sa, ra;
+            int ns = grid_segs(r1, r2, rs, rr, sg, &sa, &ra);
+            for (int q = 0; q < ns && k < iss; q++) {
+                int np = seg_npts(sg[q], drr);
+                double drt = (sg[q].b - sg[q].a) / (double)(np - 1);
+                for (int jj = sg[q].first; jj <= np && k < iss; jj++) {
+                    k++;
+                    double rk = __dadd_rn(sg[q].a, __dmul_rn((double)(jj - 1), drt));
+                    GL.r[(size_t)k * st] = rk;
+                    GL.i[(size_t)k * st] = i;
+                    if (k == 2) {
+                        rt = fmin(0.1 * drr, 0.1 * rk);
+                        rad_ystart<true>(c, 1, rt, ys);
+                        y1[0] = ys[0]; y1[1] = ys[1];
+                        yint<RadSys>(c, 1, i, rt, rk, y1, nullptr);
+                    } else if (k > 2) {
+                        yint<RadSys>(c, iprev, i, rprev, rk, y1, nullptr);
+                    }
+                    if (k >= 2) { gy(k, 0) = y1[0]; gy(k, 1) = y1[1]; }
+                    iprev = i;
+                    rprev = rk;
+                }
+            }
+        }
+    }
+    // downward from grid point ngrid to iss
+    cd y2[2] = {mk(1.0), mk(0.0)};
+    {
+        int k = ngrid + 1, iprev = 0;
+        double rprev = 0.0;
+        for (int i = mh->nknot - 1; i >= 1 && k > iss; i--) {
+            double r1 = kn[i].r, r2 = kn[i + 1].r;
+            if (r1 == r2) continue;
+            GridSeg sg[3];
+            int sa, ra;
+            int ns = grid_segs(r1, r2, rs, rr, sg, &sa, &ra);
+            for (int q = ns - 1; q >= 0 && k > iss; q--) {
+                int np = seg_npts(sg[q], drr);
+                double drt = (sg[q].b - sg[q].a) / (double)(np - 1);
+                for (int jj = np; jj >= sg[q].first && k > iss; jj--) {
+                    k--;
+                    double rk = __dadd_rn(sg[q].a, __dmul_rn((double)(jj - 1), drt));
+                    GL.r[(size_t)k * st] = rk;
+                    GL.i[(size_t)k * st] = i;
+                    if (k < ngrid) yint<RadSys>(c, iprev, i, rprev, rk, y2, nullptr);
+                    gy(k, 2) = y2[0];
+                    gy(k, 3) = y2[1];
+                    iprev = i;
+                    rprev = rk;
+                }
+            }
+        }
+    }
+    const bool rec_up = irr <= iss;               // receiver on the upward walk
+    const cd yrec[2] = {gy(irr, rec_up ? 0 : 2), gy(irr, rec_up ? 1 : 3)};
+    const cd D = y2[1] * y1[0] - y2[0] * y1[1];
+    const cd delta = 1.0 / D;
+    const cd* Y = rec_up ? y2 : y1;
+    const cd bv[2] = {Y[1], -Y[0]};
+    const cd dy[2] = {delta * yrec[0], delta * yrec[1]};
+    for (int a = 0; a < 2; a++)
+        for (int b = 0; b < 2; b++) yout[a][b] = -(dy[a] * bv[b]);
+    // reverse: yout[a][b] = -delta yrec[a] bv[b]
+    cd dyb[2] = {mk(0.0), mk(0.0)}, bvb[2] = {mk(0.0), mk(0.0)};
+    for (int a = 0; a < 2; a++)
+        for (int b = 0; b < 2; b++) {
+            dyb[a] = dyb[a] - yb[a][b] * bv[b];
+            bvb[b] = bvb[b] - yb[a][b] * dy[a];
+        }
+    const cd deltab = dyb[0] * yrec[0] + dyb[1] * yrec[1];
+    const cd yrecb[2] = {dyb[0] * delta, dyb[1] * delta};
+    const cd Db = -(deltab * (delta * delta));
+    cd y1b[2] = {Db * y2[1], -(Db * y2[0])};
+    cd y2b[2] = {-(Db * y1[1]), Db * y1[0]};
+    cd* Yb = rec_up ? y2b : y1b;
+    Yb[1] = Yb[1] + bvb[0];
+    Yb[0] = Yb[0] - bvb[1];
+    // downward walk, reversed: y2(k) = piece(k+1 -> k) y2(k+1)
+    for (int k = iss; k < ngrid; k++) {
+        if (!rec_up && k == irr) {
+            y2b[0] = y2b[0] + yrecb[0];
+            y2b[1] = y2b[1] + yrecb[1];
+        }
+        const cd yin[2] = {gy(k + 1, 2), gy(k + 1, 3)};
+        if (!yint_adj<RadT>(c, GL.i[(size_t)(k + 1) * st], GL.i[(size_t)k * st], GL.r[(size_t)(k + 1) * st],
+                            GL.r[(size_t)k * st], yin, y2b, false, L, G))
+            return false;
+    }
+    // upward walk, reversed: y1(k) = piece(k-1 -> k) y1(k-1), y1(2) from the start
+    for (int k = iss; k >= 2; k--) {
+        if (rec_up && k == irr) {
+            y1b[0] = y1b[0] + yrecb[0];
+            y1b[1] = y1b[1] + yrecb[1];
+        }
+        if (k > 2) {
+            const cd yin[2] = {gy(k - 1, 0), gy(k - 1, 1)};
+            if (!yint_adj<RadT>(c, GL.i[(size_t)(k - 1) * st], GL.i[(size_t)k * st], GL.r[(size_t)(k - 1) * st],
+                                GL.r[(size_t)k * st], yin, y1b, false, L, G))
+                return false;
+        } else {
+            if (!yint_adj<RadT>(c, 1, GL.i[(size_t)k * st], rt, GL.r[(size_t)k * st], ys, y1b, false, L, G))
+                return false;
+            start_adj<3>(c, u, 1, rt, y1b, G);
+        }
+    }
+    return true;
+}
+
+// coefb: adjoints of the 15 coefficients of pair (l = 0, j); only uu(3)
+// is formed by the radial solve (yspec.f90:263-293).
+__device__ inline bool pair_radial_adj(Ctx& c, const UnitDirs& u, const EventDev& ev, int j, const cd* coefb,
+                                       StepLog& L, GridLog& GL, SegGrad& G)
+{
+    const cd w = omega_of(ev, j);
+    set_l(c, 0);
+    set_omega(c, w);
+    cd sr0[2], yrad[2][2];
+    source_vector_rad(c, ev.is, ev.rs, ev.mm, sr0);
+    alpha_steps(c);
+    // u3 = f (sr0[0] yrad[0][0] + sr0[1] yrad[0][1]) / rr
+    cd g = coefb[2];
+    if (ev.out != 0) g = out_factor(ev.out, w) * g;
+    g = g / ev.rr;
+    const cd yb[2][2] = {{g * sr0[0], g * sr0[1]}, {mk(0.0), mk(0.0)}};
+    if (!rad_solver_wg_adj(c, u, ev.rr, ev.rs, yb, yrad, L, GL, G)) return false;
+    const cd s0b[2] = {g * yrad[0][0], g * yrad[0][1]};
+    source_rad_adj(c, u, ev.is, ev.rs, ev.mm, s0b, G);
+    return true;
+}
+
 __device__ __forceinline__ bool pair_adj_supported(const ModelHdr* mh, const EventDev& ev)
 {
     return ev.grav == 2 && mh->fic == 0 && mh->ocean == 0 && ev.rr >= ev.rs;
