@@ -60,3 +60,23 @@ def test_jacobian_columns_are_tangents():
             np.testing.assert_allclose(jac[name][:, col].numpy(), dm.val[i], rtol=1e-12, atol=1e-300)
             np.testing.assert_allclose(jac[name + "_cs"][:, col].numpy(), dm.cs[i], rtol=1e-12,
                                        atol=1e-12 * np.abs(dm.cs[i]).max() + 1e-300)
+
+
+@pytest.mark.parametrize("deck", ["model200.deck", "model400.deck"])
+def test_chain_transpose_by_autograd(deck):
+    """The reverse-mode gradient's last step (adjoint.ModelSynthetics with
+    method "adjoint"): dL/d(rho, Vp, Vs) from dL/d(knot arrays) by autograd
+    through the chain equals the transpose of the complex-step Jacobian."""
+    km = KnotModel(GOLDEN / deck)
+    rng = np.random.default_rng(5)
+    gval = rng.standard_normal((13, km.nknot))
+    gcs = rng.standard_normal((13, km.nknot))
+    pp = tuple(x.clone().requires_grad_() for x in km.params())
+    arrs = km.arrays(*pp)
+    s = sum((torch.from_numpy(gval[i]) * arrs[n]).sum() + (torch.from_numpy(gcs[i]) * arrs[n + "_cs"]).sum()
+            for i, n in enumerate(PARAMS))
+    gr = torch.autograd.grad(s, pp, allow_unused=True)
+    got = torch.cat([g if g is not None else torch.zeros(km.nknot, dtype=torch.float64) for g in gr]).numpy()
+    jac = km.jacobian()
+    ref = sum(gval[i] @ jac[n].numpy() + gcs[i] @ jac[n + "_cs"].numpy() for i, n in enumerate(PARAMS))
+    assert np.abs(got - ref).max() <= 1e-12 * np.abs(ref).max()

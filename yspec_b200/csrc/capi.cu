@@ -873,10 +873,14 @@ int ensure_units(ysg_handle* h)
 // 2 + floor(length / drr) - 1 steps on each interval it crosses, with
 // drr = max(alpha_i, alpha_i+1) / (4 Re omega) (module_int.f90:2121-2138),
 // never more than on the whole interval at the band's largest frequency;
-// one more per interval covers rounding.  Grid points of the l = 0 gravity
-// solve: floor(length / dr) + 2 per piece, at most three pieces per interval
-// (split at the source and the receiver), dr = alpha_min / (4 Re omega) or
-// 1/4 at omega = 0 (module_model.f90:578-787 with module_int.f90:1145-1166).
+// one more per interval covers rounding.  The supported solves integrate
+// within one region at a time (inner core, outer core, mantle: the start
+// levels, the solid / fluid hand-overs at nic and noc, source and receiver
+// in the mantle), so the longest region bounds a yint.  Grid points of the
+// l = 0 gravity solve: floor(length / dr) + 2 per piece, at most three
+// pieces per interval (split at the source and the receiver),
+// dr = alpha_min / (4 Re omega) or 1/4 at omega = 0 (module_model.f90:578-787
+// with module_int.f90:1145-1166).
 void adj_bounds(const ysg_handle* h, const EventDev& d, int* nmax, int* gmax)
 {
     const int n = h->hdr.nknot;
@@ -885,15 +889,17 @@ void adj_bounds(const ysg_handle* h, const EventDev& d, int* nmax, int* gmax)
     const double w = d.wmin + (double)(d.jofs + (d.nw - 1) * d.jstride) * d.dw;
     const double amin = al[h->hdr.imin_alpha - 1];
     const double dr = w > 0.0 ? std::min(0.25, amin / (4.0 * w)) : 0.25;
-    double steps = 0.0, pts = 0.0;
+    double steps[3] = {0.0, 0.0, 0.0}, pts = 0.0;
     for (int i = 1; i <= n - 1; i++) {
         const double hh = r[i] - r[i - 1];
         if (hh == 0.0) continue;
         const double drr = std::max(al[i - 1], al[i]) / (4.0 * w);
-        steps += 2.0 + std::floor(hh / drr);
+        const int reg = i < h->hdr.nic ? 0 : (i < h->hdr.noc ? 1 : 2);
+        steps[reg] += 2.0 + std::floor(hh / drr);
         pts += 8.0 + std::floor(hh / dr);
     }
-    *nmax = (int)std::min(steps + 2.0, 1.0e8);
+    const double smax = std::max(steps[0], std::max(steps[1], steps[2]));
+    *nmax = (int)std::min(smax + 2.0, 1.0e8);
     *gmax = (int)std::min(pts + 4.0, 1.0e8);
 }
 
@@ -1139,7 +1145,10 @@ int ysg_event_gradient(ysg_handle* h, const ysg_event* ev, const ysg_time* tm, c
     int rc = check_event(h, ev);
     if (rc) return rc;
     if (!tm || !gval || !gcs || tm->nr != ev->nr || (ev->nr > 0 && !gout)) return YSG_ERR_ARG;
-    if (ev->grav != 2 || h->hdr.fic != 0 || h->hdr.ocean != 0 || ev->rr < ev->rs) return YSG_ERR_UNSUPPORTED;
+    // self-gravitation, solid inner core, no ocean, source in the mantle,
+    // receivers at or above it
+    if (ev->grav != 2 || h->hdr.fic != 0 || h->hdr.ocean != 0 || ev->rr < ev->rs || ev->is <= h->hdr.noc)
+        return YSG_ERR_UNSUPPORTED;
     const int L = ev->lmax - ev->lmin + 1;
     if (L >= (1 << 23) || L > 65535 || ev->nw >= (1 << 24) || ev->nr > 65535) return YSG_ERR_LIMIT;
     cudaSetDevice(h->device);
@@ -1168,6 +1177,8 @@ int ysg_event_gradient(ysg_handle* h, const ysg_event* ev, const ysg_time* tm, c
     const size_t per = adj_log_bytes(nmax, 0), per_r = adj_log_bytes(nmax, gmax);
     const size_t Tr = ev->lmin == 0 ? (size_t)(nw + ADJ_THREADS - 1) / ADJ_THREADS * ADJ_THREADS : 0;
     const size_t budget = (free_b + h->alogs.cap) / 4;
+    // no more threads than entries
+    nblk = (int)std::min<long long>(nblk, (2 * h->npairs + ADJ_THREADS - 1) / ADJ_THREADS);
     while (nblk > 1 && (size_t)nblk * ADJ_THREADS * per + Tr * per_r > budget) nblk--;
     if ((size_t)nblk * ADJ_THREADS * per + Tr * per_r > budget) return YSG_ERR_LIMIT;
     const size_t T = (size_t)nblk * ADJ_THREADS;

@@ -23,6 +23,10 @@
 // Complex adjoints follow one convention throughout: for a real L and a
 // complex z, zb = dL/dRe z - i dL/dIm z, so dL = Re(sum zb dz) and a
 // complex-linear map is transposed without conjugation.
+// The primal solves of the sweep take the looped Cash-Karp step: the kernel
+// holds every system's replay, reverse step and tangent start / source
+// evaluations, and its instruction footprint, not its registers, limits it.
+#define YSG_LOOPED_STEP 1
 #include "ysg_kernels.h"
 #include "ysg_pair_adjoint.cuh"
 
@@ -112,7 +116,7 @@ __global__ void k_lsum_adjoint(int nw, int nr, int lmin, const double* __restric
     for (int q = 0; q < NCOEF; q++) coefb[((size_t)li * NCOEF + q) * nw + j] = acc[q];
 }
 
-__device__ __forceinline__ void adj_ctx(v_local::Ctx& c, const Knot* kn, const Seg* sg, const ModelHdr* mh,
+__device__ __forceinline__ void adj_ctx(primal::Ctx& c, const Knot* kn, const Seg* sg, const ModelHdr* mh,
                                         const EventDev& ev)
 {
     c.kn = kn;
@@ -121,7 +125,7 @@ __device__ __forceinline__ void adj_ctx(v_local::Ctx& c, const Knot* kn, const S
     c.pib = mh->pibigg;
     c.ats = (double)ev.ats;
     c.kb = nullptr;
-    for (int q = 0; q < v_local::NSYS; q++) c.nst[q] = 0;
+    for (int q = 0; q < primal::NSYS; q++) c.nst[q] = 0;
 }
 
 // Reverse sweeps of the l >= 1 entries (the l = 0 pairs go to
@@ -139,7 +143,7 @@ __global__ void __launch_bounds__(ADJ_THREADS) k_solve_adjoint(
     const EventDev ev = *evp;
     SegGrad G;
     G.init(grad);
-    v_local::Ctx c;                               // the plain form of the solver code
+    primal::Ctx c;                               // the plain form of the solver code
     adj_ctx(c, kn, sg, mh, ev);
     const int lane = threadIdx.x & 31;
     for (;;) {
@@ -185,7 +189,7 @@ __global__ void __launch_bounds__(ADJ_THREADS) k_radial_adjoint(
     GridLog GL{w.gy + tid, w.gr + tid, w.gi + tid, w.gmax, w.nthreads};
     SegGrad G;
     G.init(grad);
-    v_local::Ctx c;
+    primal::Ctx c;
     adj_ctx(c, kn, sg, mh, ev);
     for (int j = tid + 1; j <= ev.nw; j += w.nthreads) {
         cd wb[NCOEF];

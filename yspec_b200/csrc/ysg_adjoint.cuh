@@ -299,34 +299,40 @@ template <class T>
 __device__ void rk_step_adj(const Ctx& c, const cd* y, double x, double h, cd* yb, SegGrad& G)
 {
     constexpr int N = T::A::N;
-    cd Y[6][N], k[6][N];
+    // K holds the stage derivatives k_s while the stage inputs Y_s are
+    // formed, then their adjoints; the stage loops stay rolled (one copy of
+    // each right-hand side and of its transposes in the code)
+    cd Y[6][N], K[6][N];
+#pragma unroll 1
     for (int s = 0; s < 6; s++) {
         for (int i = 0; i < N; i++) {
             cd v = y[i];
-            for (int t = 0; t < s; t++) v = v + (h * ck_b(s, t)) * k[t][i];
+            for (int t = 0; t < s; t++) v = v + (h * ck_b(s, t)) * K[t][i];
             Y[s][i] = v;
         }
-        T::Sys::f(c, x + ck_x(s) * h, Y[s], k[s]);
+        T::Sys::f(c, x + ck_x(s) * h, Y[s], K[s]);
     }
-    cd kb[6][N];
+#pragma unroll 1
     for (int s = 0; s < 6; s++)
-        for (int i = 0; i < N; i++) kb[s][i] = (h * ck_c(s)) * yb[i];
+        for (int i = 0; i < N; i++) K[s][i] = (h * ck_c(s)) * yb[i];
+#pragma unroll 1
     for (int s = 5; s >= 0; s--) {
         const double r = x + ck_x(s) * h;
         const auto a = T::amat(c, r);
         cd Yb[N];
-        T::A::tr(a, kb[s], Yb);
+        T::A::tr(a, K[s], Yb);
         typename T::A::Bar sb;
         sb.zero();
-        T::A::cgrad(kb[s], Y[s], sb);
+        T::A::cgrad(K[s], Y[s], sb);
         double vb[NPARAM];
         for (int p = 0; p < NPARAM; p++) vb[p] = 0.0;
         T::amat_adj(c, r, sb, vb);
         G.add(c.il, r - c.sg[c.il].r0, vb);
         for (int i = 0; i < N; i++) yb[i] = yb[i] + Yb[i];
+#pragma unroll 1
         for (int t = 0; t < s; t++) {
             const double w = h * ck_b(s, t);
-            for (int i = 0; i < N; i++) kb[t][i] = kb[t][i] + w * Yb[i];
+            for (int i = 0; i < N; i++) K[t][i] = K[t][i] + w * Yb[i];
         }
     }
 }
@@ -348,10 +354,11 @@ struct StepLog {
 // The forward yint of ysg_ode.cuh (same intervals, step counts and
 // rescaling) logging every step, then its adjoint: yb holds the adjoint of
 // the result on entry and that of the starting state y0 on exit.  Returns
-// false if the steps exceed the log.
+// false if the steps exceed the log.  One copy per system in the code (the
+// drivers call it from several places).
 template <class T>
-__device__ bool yint_adj(Ctx& c, int i1, int i2, double r1, double r2, const cd* y0, cd* yb, bool scaled,
-                         StepLog& L, SegGrad& G)
+__device__ __noinline__ bool yint_adj(Ctx& c, int i1, int i2, double r1, double r2, const cd* y0, cd* yb,
+                                      bool scaled, StepLog& L, SegGrad& G)
 {
     constexpr int N = T::A::N;
     if (r2 == r1) return true;
@@ -384,7 +391,7 @@ __device__ bool yint_adj(Ctx& c, int i1, int i2, double r1, double r2, const cd*
             L.x[e] = rr;
             L.h[e] = drr;
             L.il[e] = i;
-            rkck_step<typename T::Sys>(c, y, rr, drr);
+            yint_step<typename T::Sys>(c, y, rr, drr);
             double f = 1.0;
             if (scaled) {
                 int sc = 0;

@@ -15,7 +15,7 @@
 #include "ysg_dual.cuh"
 #include "ysg_model.cuh"
 
-// Four builds of the solver code exist: the plain form keeps the Cash-Karp
+// Five builds of the solver code exist: the plain form keeps the Cash-Karp
 // stage vectors in per-thread arrays (the compiler places them in local
 // memory); with YSG_SMEM_STAGES the stage vectors live in a per-thread slab
 // of shared memory and only y and the stage input stay in registers; with
@@ -24,7 +24,11 @@
 // layers, step counts -- is made as in a real solve, no state is stepped);
 // with YSG_TANGENT every quantity that depends on the earth model is a dual
 // number (ysg_dual.cuh) and the solve returns, beside its value, the
-// derivative along one direction of the model (the tangent-linear solver).
+// derivative along one direction of the model (the tangent-linear solver);
+// with YSG_LOOPED_STEP the plain solve takes the looped Cash-Karp step of
+// the tangent build (one right-hand side in the code instead of six), for
+// kernels whose instruction footprint matters more than the step's
+// registers (the reverse sweep).
 // Each form gets its own inline namespace so the translation units never
 // share a definition, and a translation unit may include this header once
 // per form (the reverse sweep uses the plain and the tangent form): the
@@ -37,6 +41,9 @@
 #endif
 #ifndef YSG_TANGENT
 #define YSG_TANGENT 0
+#endif
+#ifndef YSG_LOOPED_STEP
+#define YSG_LOOPED_STEP 0
 #endif
 #undef YSG_VARIANT
 #undef YSG_ODE_BODY
@@ -56,6 +63,12 @@
 #define YSG_VARIANT v_smem
 #ifndef YSG_ODE_DONE_v_smem
 #define YSG_ODE_DONE_v_smem
+#define YSG_ODE_BODY
+#endif
+#elif YSG_LOOPED_STEP
+#define YSG_VARIANT v_loop
+#ifndef YSG_ODE_DONE_v_loop
+#define YSG_ODE_DONE_v_loop
 #define YSG_ODE_BODY
 #endif
 #else
@@ -756,8 +769,22 @@ __device__ __forceinline__ void rescale(mcplx* y, int* scale)
     }
 }
 
+// One Cash-Karp step of yint in this build form (the reverse sweep replays
+// yint's steps through it, so the replayed states are yint's).
+template <class Sys>
+__device__ __forceinline__ void yint_step(const Ctx& c, mcplx* y, double x, double h)
+{
+#if YSG_SMEM_STAGES
+    rkck_step_loop<Sys>(c, y, x, h);
+#elif YSG_TANGENT || YSG_LOOPED_STEP
+    rkck_step_loop_local<Sys>(c, y, x, h);
+#else
+    rkck_step<Sys>(c, y, x, h);
+#endif
+}
+
 // module_int.f90:1847-1968 yint
-#if YSG_SMEM_STAGES || YSG_TANGENT
+#if YSG_SMEM_STAGES || YSG_TANGENT || YSG_LOOPED_STEP
 #undef YSG_YINT_ATTR
 #define YSG_YINT_ATTR __noinline__
 #else
@@ -802,13 +829,7 @@ __device__ YSG_YINT_ATTR void yint(Ctx& cio, int i1, int i2, double r1, double r
         if (YSG_COUNT_ONLY) continue;
         for (int j = 1; j <= n - 1; j++) {
             double rr = __dadd_rn(rr1, __dmul_rn((double)(j - 1), drr));
-#if YSG_SMEM_STAGES
-            rkck_step_loop<Sys>(c, y, rr, drr);
-#elif YSG_TANGENT
-            rkck_step_loop_local<Sys>(c, y, rr, drr);
-#else
-            rkck_step<Sys>(c, y, rr, drr);
-#endif
+            yint_step<Sys>(c, y, rr, drr);
             if (scale) rescale<Sys::N>(y, scale);
         }
     }

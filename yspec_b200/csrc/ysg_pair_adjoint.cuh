@@ -27,15 +27,20 @@
 #include "ysg_adjoint.cuh"
 #include "ysg_solvers.cuh"
 
-// the tangent-linear form of the same headers (namespace ysg::v_tangent)
+// the tangent-linear form of the same headers (namespace ysg::v_tangent);
+// this file's own code goes to the form included first (v_local, or v_loop
+// with YSG_LOOPED_STEP), named ysg::primal
+#pragma push_macro("YSG_VARIANT")
 #pragma push_macro("YSG_TANGENT")
 #undef YSG_TANGENT
 #define YSG_TANGENT 1
 #include "ysg_solvers.cuh"
 #pragma pop_macro("YSG_TANGENT")
+#pragma pop_macro("YSG_VARIANT")
 
 namespace ysg {
-inline namespace v_local {
+namespace primal = YSG_VARIANT;
+inline namespace YSG_VARIANT {
 
 __device__ inline void tangent_ctx(const Ctx& c, const UnitDirs& u, int p, v_tangent::Ctx& t)
 {
@@ -68,7 +73,7 @@ __device__ inline void tangent_ctx(const Ctx& c, const UnitDirs& u, int p, v_tan
 // the moments of the result go to G.  WHICH: 0 toroidal (2), 1 solid minor
 // (14), 2 fluid minor (5), 3 radial with gravity (2).
 template <int WHICH>
-__device__ inline void start_adj(const Ctx& c, const UnitDirs& u, int i1, double rt, const cd* yb, SegGrad& G)
+__device__ __noinline__ void start_adj(const Ctx& c, const UnitDirs& u, int i1, double rt, const cd* yb, SegGrad& G)
 {
     constexpr int N = (WHICH == 0 || WHICH == 3) ? 2 : (WHICH == 1 ? 14 : 5);
     double vb[NPARAM];
@@ -90,7 +95,7 @@ __device__ inline void start_adj(const Ctx& c, const UnitDirs& u, int i1, double
 // Source vectors at (is, rs): svtb (5 x 2) and svsb (5 x 6) are the
 // adjoints of the toroidal and spheroidal source vectors (either may be
 // null).
-__device__ inline void source_adj(const Ctx& c, const UnitDirs& u, int is, double rs, const double* mm,
+__device__ __noinline__ void source_adj(const Ctx& c, const UnitDirs& u, int is, double rs, const double* mm,
                                   const cd (*svtb)[2], const cd (*svsb)[6], SegGrad& G)
 {
     double vb[NPARAM];
@@ -117,7 +122,7 @@ __device__ inline void source_adj(const Ctx& c, const UnitDirs& u, int is, doubl
 
 // Radial source vector at (is, rs) (module_solver.f90:566-627): s0b holds
 // the adjoints of its two components.
-__device__ inline void source_rad_adj(const Ctx& c, const UnitDirs& u, int is, double rs, const double* mm,
+__device__ __noinline__ void source_rad_adj(const Ctx& c, const UnitDirs& u, int is, double rs, const double* mm,
                                       const cd* s0b, SegGrad& G)
 {
     double vb[NPARAM];
@@ -212,7 +217,7 @@ __device__ inline void f2s_adj(const cd* msb, cd* mfb)
 // The forward solve again, keeping what the reverse sweep needs; yb is the
 // adjoint of yout.  Returns false if a step log overflowed.
 __device__ inline bool tor_solver_adj(Ctx& c, const UnitDirs& u, double rr, double rs, int ir, int is,
-                                      const cd yb_out[2][2], StepLog& L, SegGrad& G)
+                                      const cd yb_out[2][2], cd yout[2][2], StepLog& L, SegGrad& G)
 {
     const ModelHdr* mh = c.mh;
     const Knot* kn = c.kn;
@@ -239,8 +244,12 @@ __device__ inline bool tor_solver_adj(Ctx& c, const UnitDirs& u, double rr, doub
     const cd delta = 1.0 / D;
     const cd b0 = y1[1], b1 = -y1[0];
     const cd dy0 = delta * y2[0], dy1 = delta * y2[1];
-    // reverse: yout[a][0] = -(dy_a b0), yout[a][1] = -(dy_a b1), times huge^scale3
+    // yout[a][0] = -(dy_a b0), yout[a][1] = -(dy_a b1), times huge^scale3
     const double F = huge_pow(scale3);
+    yout[0][0] = F * (-(dy0 * b0));
+    yout[1][0] = F * (-(dy1 * b0));
+    yout[0][1] = F * (-(dy0 * b1));
+    yout[1][1] = F * (-(dy1 * b1));
     cd yb[2][2];
     for (int a = 0; a < 2; a++)
         for (int b = 0; b < 2; b++) yb[a][b] = F * yb_out[a][b];
@@ -270,7 +279,7 @@ __device__ inline bool tor_solver_adj(Ctx& c, const UnitDirs& u, double rr, doub
 // (module_solver.f90:640-823): yb_out (6 x 4) is the adjoint of yout.
 // ---------------------------------------------------------------------------
 __device__ inline bool sph_solver_g_adj(Ctx& c, const UnitDirs& u, double rr, double rs, int ir, int is,
-                                        const cd yb_out[6][4], StepLog& L, SegGrad& G)
+                                        const cd yb_out[6][4], cd yout[6][4], StepLog& L, SegGrad& G)
 {
     const ModelHdr* mh = c.mh;
     const Knot* kn = c.kn;
@@ -335,6 +344,7 @@ __device__ inline bool sph_solver_g_adj(Ctx& c, const UnitDirs& u, double rr, do
         const double F = huge_pow(scale3 - scale4);
         cd ysb[6];
         for (int k = 0; k < 6; k++) {
+            yout[k][i] = F * (-(ys[k] / delta));
             const cd yk = F * yb_out[k][i];
             ysb[k] = -(yk / delta);
             deltab = deltab + yk * (ys[k] / (delta * delta));
@@ -566,7 +576,10 @@ __device__ __forceinline__ bool pair_adj_supported(const ModelHdr* mh, const Eve
     return ev.grav == 2 && mh->fic == 0 && mh->ocean == 0 && ev.rr >= ev.rs;
 }
 
-// wwb: adjoints of ww(1:5) of pair (l >= 2, j)
+// wwb: adjoints of ww(1:5) of pair (l >= 2, j).  The adjoints of the
+// solver's output need only the source vectors, so the solver's reverse
+// sweep runs first and its own forward pass supplies the output that the
+// source vectors' adjoints need.
 __device__ inline bool pair_toroidal_adj(Ctx& c, const UnitDirs& u, const EventDev& ev, int l, int j,
                                          const cd* wwb, StepLog& L, SegGrad& G)
 {
@@ -575,32 +588,35 @@ __device__ inline bool pair_toroidal_adj(Ctx& c, const UnitDirs& u, const EventD
     set_omega(c, w);
     cd svt[5][2], ytor[2][2];
     source_vector_tor(c, ev.is, ev.rs, ev.mm, svt);
-    tor_solver(c, ev.rr, ev.rs, ev.ir, ev.is, ytor);
     const cd f = out_factor(ev.out, w);
-    if (ev.out != 0)
-        for (int a = 0; a < 2; a++)
-            for (int b = 0; b < 2; b++) ytor[a][b] = f * ytor[a][b];
     const double zeta = (double)sqrtf((float)(l * (l + 1)));
     const double zr = zeta * ev.rr;
-    // ww[q] = (svt[q][0] ytor[0][0] + svt[q][1] ytor[0][1]) / zr
-    cd svtb[5][2], yb[2][2] = {{mk(0.0), mk(0.0)}, {mk(0.0), mk(0.0)}};
+    // ww[q] = (svt[q][0] ytor'[0][0] + svt[q][1] ytor'[0][1]) / zr, ytor' = f ytor
+    cd yb[2][2] = {{mk(0.0), mk(0.0)}, {mk(0.0), mk(0.0)}};
     for (int q = 0; q < 5; q++) {
         const cd g = wwb[q] / zr;
-        svtb[q][0] = g * ytor[0][0];
-        svtb[q][1] = g * ytor[0][1];
         yb[0][0] = yb[0][0] + g * svt[q][0];
         yb[0][1] = yb[0][1] + g * svt[q][1];
     }
     if (ev.out != 0)
         for (int a = 0; a < 2; a++)
             for (int b = 0; b < 2; b++) yb[a][b] = f * yb[a][b];
+    if (!tor_solver_adj(c, u, ev.rr, ev.rs, ev.ir, ev.is, yb, ytor, L, G)) return false;
+    if (ev.out != 0)
+        for (int a = 0; a < 2; a++)
+            for (int b = 0; b < 2; b++) ytor[a][b] = f * ytor[a][b];
+    cd svtb[5][2];
+    for (int q = 0; q < 5; q++) {
+        const cd g = wwb[q] / zr;
+        svtb[q][0] = g * ytor[0][0];
+        svtb[q][1] = g * ytor[0][1];
+    }
     source_adj(c, u, ev.is, ev.rs, ev.mm, svtb, nullptr, G);
-    set_l(c, l);
-    set_omega(c, w);
-    return tor_solver_adj(c, u, ev.rr, ev.rs, ev.ir, ev.is, yb, L, G);
+    return true;
 }
 
-// uub, vvb: adjoints of uu(1:5), vv(1:5) of pair (l >= 1, j)
+// uub, vvb: adjoints of uu(1:5), vv(1:5) of pair (l >= 1, j); the same
+// order as the toroidal part.
 __device__ inline bool pair_spheroidal_adj(Ctx& c, const UnitDirs& u, const EventDev& ev, int l, int j,
                                            const cd* uub, const cd* vvb, StepLog& L, SegGrad& G)
 {
@@ -608,14 +624,59 @@ __device__ inline bool pair_spheroidal_adj(Ctx& c, const UnitDirs& u, const Even
     set_l(c, l);
     set_omega(c, w);
     alpha_steps(c);
-    cd svs[5][6], ysph[6][4], y0[6][4];
+    cd svs[5][6], ysph[6][4];
     source_vector_sph(c, ev.is, ev.rs, ev.mm, svs);
-    sph_solver_g(c, ev.rr, ev.rs, ev.ir, ev.is, ysph);
-    for (int a = 0; a < 6; a++)
-        for (int b = 0; b < 4; b++) y0[a][b] = ysph[a][b];
     const double zeta = (double)sqrtf((float)(l * (l + 1)));
     const cd mw2 = -(w * w);
     const double gr = ev.grav_ir;
+    const double zr = zeta * ev.rr;
+    const int col[4] = {0, 1, 3, 4};
+    // uu[q] = sum_b ysph'[0][b] svs[q][col b] / rr;  vv[q] = sum_b ysph'[1][b] svs[q][col b] / zr,
+    // ysph' the solver output after the output scaling and corrections
+    cd yb[6][4], ybo[2][4];
+    for (int a = 0; a < 6; a++)
+        for (int b = 0; b < 4; b++) yb[a][b] = mk(0.0);
+    for (int q = 0; q < 5; q++) {
+        const cd gu = uub[q] / ev.rr, gv = vvb[q] / zr;
+        for (int b = 0; b < 4; b++) {
+            yb[0][b] = yb[0][b] + gu * svs[q][col[b]];
+            yb[1][b] = yb[1][b] + gv * svs[q][col[b]];
+        }
+    }
+    for (int b = 0; b < 4; b++) {
+        ybo[0][b] = yb[0][b];
+        ybo[1][b] = yb[1][b];
+    }
+    // output scaling and the potential / tilt correction (yspec.f90:376-391)
+    if (ev.out == 1) {
+        const cd f = imul(w);
+        for (int b = 0; b < 4; b++)
+            for (int a = 0; a < 3; a++) yb[a][b] = f * yb[a][b];
+    } else if (ev.out == 2) {
+        if (ev.cor == 0) {
+            for (int b = 0; b < 4; b++)
+                for (int a = 0; a < 3; a++) yb[a][b] = mw2 * yb[a][b];
+        } else {
+            for (int b = 0; b < 4; b++) {
+                const cd a0 = yb[0][b], a1 = yb[1][b];
+                // y0' = mw2 y0 - ((l+1) y2 + 2 g y0) / rr;  y1' = mw2 y1 + zeta (y2 + g y0) / rr
+                yb[0][b] = a0 * (mw2 - (2.0 * gr) / ev.rr) + a1 * (zeta * gr / ev.rr);
+                yb[1][b] = a1 * mw2;
+                yb[2][b] = yb[2][b] + a0 * (-(double)(l + 1) / ev.rr) + a1 * (zeta / ev.rr);
+            }
+        }
+    }
+    if (!sph_solver_g_adj(c, u, ev.rr, ev.rs, ev.ir, ev.is, yb, ysph, L, G)) return false;
+    // grav(ir), the c0 coefficient of segment ir, through the correction
+    if (ev.out == 2 && ev.cor != 0) {
+        double gb = 0.0;
+        for (int b = 0; b < 4; b++)
+            gb += re(ybo[0][b] * (-2.0 * ysph[0][b] / ev.rr)) + re(ybo[1][b] * (zeta * ysph[0][b] / ev.rr));
+        double vb[NPARAM];
+        for (int p = 0; p < NPARAM; p++) vb[p] = 0.0;
+        vb[P_GRAV] = gb;
+        G.add(ev.ir, 0.0, vb);
+    }
     if (ev.out == 1) {
         const cd f = imul(w);
         for (int b = 0; b < 4; b++)
@@ -633,54 +694,16 @@ __device__ inline bool pair_spheroidal_adj(Ctx& c, const UnitDirs& u, const Even
             }
         }
     }
-    const double zr = zeta * ev.rr;
-    const int col[4] = {0, 1, 3, 4};
-    // uu[q] = sum_b ysph[0][b] svs[q][col b] / rr;  vv[q] = sum_b ysph[1][b] svs[q][col b] / zr
-    cd svsb[5][6], yb[6][4];
+    cd svsb[5][6];
     for (int q = 0; q < 5; q++)
         for (int b = 0; b < 6; b++) svsb[q][b] = mk(0.0);
-    for (int a = 0; a < 6; a++)
-        for (int b = 0; b < 4; b++) yb[a][b] = mk(0.0);
     for (int q = 0; q < 5; q++) {
         const cd gu = uub[q] / ev.rr, gv = vvb[q] / zr;
-        for (int b = 0; b < 4; b++) {
-            svsb[q][col[b]] = svsb[q][col[b]] + gu * ysph[0][b] + gv * ysph[1][b];
-            yb[0][b] = yb[0][b] + gu * svs[q][col[b]];
-            yb[1][b] = yb[1][b] + gv * svs[q][col[b]];
-        }
-    }
-    // output scaling and the potential / tilt correction (yspec.f90:376-391)
-    if (ev.out == 1) {
-        const cd f = imul(w);
-        for (int b = 0; b < 4; b++)
-            for (int a = 0; a < 3; a++) yb[a][b] = f * yb[a][b];
-    } else if (ev.out == 2) {
-        if (ev.cor == 0) {
-            for (int b = 0; b < 4; b++)
-                for (int a = 0; a < 3; a++) yb[a][b] = mw2 * yb[a][b];
-        } else {
-            double gb = 0.0;
-            for (int b = 0; b < 4; b++) {
-                const cd a0 = yb[0][b], a1 = yb[1][b];
-                // y0' = mw2 y0 - ((l+1) y2 + 2 g y0) / rr;  y1' = mw2 y1 + zeta (y2 + g y0) / rr
-                yb[0][b] = a0 * (mw2 - (2.0 * gr) / ev.rr) + a1 * (zeta * gr / ev.rr);
-                yb[1][b] = a1 * mw2;
-                yb[2][b] = yb[2][b] + a0 * (-(double)(l + 1) / ev.rr) + a1 * (zeta / ev.rr);
-                gb += re(a0 * (-2.0 * y0[0][b] / ev.rr)) + re(a1 * (zeta * y0[0][b] / ev.rr));
-            }
-            // grav(ir) is the c0 coefficient of segment ir
-            double vb[NPARAM];
-            for (int p = 0; p < NPARAM; p++) vb[p] = 0.0;
-            vb[P_GRAV] = gb;
-            G.add(ev.ir, 0.0, vb);
-        }
+        for (int b = 0; b < 4; b++) svsb[q][col[b]] = svsb[q][col[b]] + gu * ysph[0][b] + gv * ysph[1][b];
     }
     source_adj(c, u, ev.is, ev.rs, ev.mm, nullptr, svsb, G);
-    set_l(c, l);
-    set_omega(c, w);
-    alpha_steps(c);
-    return sph_solver_g_adj(c, u, ev.rr, ev.rs, ev.ir, ev.is, yb, L, G);
+    return true;
 }
 
-}  // namespace v_local
+}  // namespace YSG_VARIANT
 }  // namespace ysg

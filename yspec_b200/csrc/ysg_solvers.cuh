@@ -23,6 +23,11 @@
 #define YSG_SOLVERS_DONE_v_smem
 #define YSG_SOLVERS_BODY
 #endif
+#elif YSG_LOOPED_STEP
+#ifndef YSG_SOLVERS_DONE_v_loop
+#define YSG_SOLVERS_DONE_v_loop
+#define YSG_SOLVERS_BODY
+#endif
 #else
 #ifndef YSG_SOLVERS_DONE_v_local
 #define YSG_SOLVERS_DONE_v_local

@@ -3,14 +3,18 @@
     python -m yspec_b200.stages c2 [--solver batched|plain] [--schedule 0|1|2] [--reps 3]
                                    [--seed 0] [--set lmax=300 --set fmax=20.0] [--batch]
     python -m yspec_b200.stages c5 --batch --reuse-output --schedule 2 --reps 2
+    python -m yspec_b200.stages c4 --gradient --reps 2
 
 Runs the configuration's first event through `Engine.run` (or, with
 --batch, all its events through one `Engine.batch_run`) `reps` times and
 prints, per run, the device time of each stage (Legendre table, solves,
 l-sum, filter + inverse FFT) measured with CUDA events on the engine's
 stream, the number of (omega,l) solves and the counted FP64 work of the
-solve stage.  It is also the small, self-contained command used for ncu
-captures of one kernel.
+solve stage.  With --gradient it runs the reverse mode instead
+(Engine.gradient of a seeded random trace adjoint) and prints its stages
+(Legendre table, reverse sweeps, l-sum transpose, time-stage transpose).
+It is also the small, self-contained command used for ncu captures of one
+kernel.
 """
 from __future__ import annotations
 
@@ -44,6 +48,8 @@ def main(argv=None) -> None:
     ap.add_argument("--batch", action="store_true", help="run every event of the configuration as one batch")
     ap.add_argument("--reuse-output", action="store_true",
                     help="with --batch: one host trace buffer for every event (c5's traces exceed host memory)")
+    ap.add_argument("--gradient", action="store_true",
+                    help="time the reverse-mode gradient of the event (Engine.gradient) instead")
     ap.add_argument("--set", action="append", default=[], metavar="KEY=VALUE",
                     help="override a parameter of the configuration")
     a = ap.parse_args(argv)
@@ -56,6 +62,19 @@ def main(argv=None) -> None:
         m = Model(ps[0].model_file)
         eng.upload(m)
         evs = [Event(m, Params(p.write(Path(tmp) / f"{a.config}_{i}.in"))) for i, p in enumerate(ps)]
+        if a.gradient:
+            ev = evs[0]
+            gout = np.random.default_rng(a.seed).standard_normal((ev.nr, 4, ev.nout()))
+            gout[:, 0, :] = 0.0
+            for rep in range(a.reps):
+                t = time.perf_counter()
+                gval, _ = eng.gradient(ev, gout)
+                wall = time.perf_counter() - t
+                ms = eng.timings()
+                print(f"{a.config} gradient rep{rep}: wall {wall:.3f} s  stages (ms) legendre {ms[0]:.3f} "
+                      f"sweeps {ms[1]:.3f} lsum-T {ms[2]:.3f} time-T {ms[3]:.3f}  pairs {ev.L * ev.nw}  "
+                      f"|dL/dval|_1 {float(np.abs(gval).sum()):.6e}", flush=True)
+            return
         outs = None
         if a.batch and a.reuse_output:
             if any((e.nr, e.nout()) != (evs[0].nr, evs[0].nout()) for e in evs):
