@@ -6,7 +6,7 @@ compares <dL/d(knot arrays), d> from the reverse sweep with the directional
 derivative of the same pair solve in dual numbers, for radial, toroidal and
 spheroidal pairs from l = 0 to lmax, to 1e-9 relative.  The GPU form of the
 same comparison, through the whole gradient pipeline, is
-tests/test_gpu_adjoint.py."""
+tests/test_gpu_reverse.py."""
 from __future__ import annotations
 
 import shutil
