@@ -5,7 +5,8 @@ forward mode: for a random trace adjoint gout and random model directions d,
 Covered: the c1 and c4 configurations, displacement / velocity /
 acceleration with the potential and tilt corrections, receivers at the
 surface and at depth, and the whole ModelSynthetics backward pass against
-its forward-mode counterpart."""
+its forward-mode counterpart and, at the c4 size, against central
+differences of the misfit along 20 directions."""
 from __future__ import annotations
 
 import numpy as np
@@ -97,3 +98,46 @@ def test_unsupported_path_falls_back(tmp_path):
     (syn(rho, vp, vs, mm) ** 2).sum().backward()
     assert syn.last_method == "tangent"
     assert torch.count_nonzero(rho.grad) <= 2
+
+
+def test_c4_misfit_gradient_against_differences(tmp_path):
+    """The c4 workload at size (lmax 300, 20 mHz, 50 receivers, 200 knots):
+    the reverse-mode gradient of an L2 waveform misfit with respect to the
+    600 knot parameters and the moment tensor, along 20 random directions,
+    against central differences of the misfit (step 1e-3, start levels and
+    step counts of the deck's model), to 1e-6 relative."""
+    import torch
+
+    from yspec_b200 import adjoint
+
+    from yspec_b200 import workloads as W
+
+    eng, ev, km = _setup(tmp_path, "c4", {})
+    p = W.config("c4", seed=0)[0]
+    syn = adjoint.ModelSynthetics(eng, ev, km)
+    P0 = km.params()
+    mm0 = torch.tensor(p.mm, dtype=torch.float64)
+    rng = np.random.default_rng(11)
+    kern = np.exp(-0.5 * (np.arange(-9, 10) / 3.0) ** 2)
+    kern /= kern.sum()
+    Pobs = tuple(x * (1.0 + torch.from_numpy(np.convolve(rng.standard_normal(km.nknot), kern, mode="same")) * 1e-2)
+                 for x in P0)
+    obs = syn(*Pobs, mm0).detach()
+    rho, vp, vs = (x.clone().requires_grad_() for x in P0)
+    mm = mm0.clone().requires_grad_()
+    loss = 0.5 * ((syn(rho, vp, vs, mm) - obs) ** 2).sum()
+    loss.backward()
+    assert syn.last_method == "adjoint"
+    grad = (rho.grad, vp.grad, vs.grad, mm.grad)
+    worst = 0.0
+    for k in range(20):
+        r = np.random.default_rng(100 + k)
+        dk = tuple(torch.from_numpy(r.standard_normal(km.nknot)) * x * 1e-2 for x in P0)
+        dm = torch.from_numpy(r.standard_normal(6)) * 1e18
+        with torch.no_grad():
+            lp = float(0.5 * ((syn(*(x + 1e-3 * y for x, y in zip(P0, dk)), mm0 + 1e-3 * dm) - obs) ** 2).sum())
+            lm = float(0.5 * ((syn(*(x - 1e-3 * y for x, y in zip(P0, dk)), mm0 - 1e-3 * dm) - obs) ** 2).sum())
+        fd = (lp - lm) / 2e-3
+        ad = sum(float((g * y).sum()) for g, y in zip(grad, dk + (dm,)))
+        worst = max(worst, abs(ad - fd) / abs(fd))
+    assert worst <= 1e-6, worst
