@@ -100,8 +100,17 @@ __global__ void __launch_bounds__(LS_J* LS_K) k_lsum(int nw, int nr, int L, cons
 // each warp issues 44 MMAs: the signs s = (-1)^m for m < 0 and the factors
 // +-m of the i m terms scale the Legendre fragments, never the
 // accumulators, and the phase factors e^{i m phi_k} are applied once, in
-// the epilogue.  Receivers run fastest in the grid, so the CTAs in flight
-// share one frequency tile's coefficients through L2.
+// the epilogue.
+//
+// Every CTA reads its frequency tile's coefficient rows and its receiver
+// tile's Legendre rows for all degrees, so which tiles are in flight
+// together decides the DRAM traffic: neither array fits L2 at c5 sizes.
+// The 1-D grid is rasterised in groups of F frequency tiles: consecutive
+// CTAs take the F frequency tiles of one receiver tile, then those of the
+// next, so the CTAs in flight share F tiles of coefficients and about
+// (CTAs in flight / F) tiles of Legendre rows through L2.  The launcher
+// picks F to minimise the modelled re-reads with that working set within
+// half of L2.
 // ---------------------------------------------------------------------------
 constexpr int LM_J = 16;                  // frequencies per CTA
 constexpr int LM_K = 32;                  // receivers per CTA
@@ -159,7 +168,7 @@ __device__ __forceinline__ void lm_stage(unsigned char* buf, int l0, int j0, int
     }
 }
 
-__global__ void __launch_bounds__(LM_THREADS, 1) k_lsum_mma(int nw, int nr, int L, int lmin,
+__global__ void __launch_bounds__(LM_THREADS, 1) k_lsum_mma(int nw, int nr, int L, int lmin, int group,
                                                            const cd* __restrict__ coef,
                                                            const double* __restrict__ T,
                                                            const cd* __restrict__ E,
@@ -168,7 +177,15 @@ __global__ void __launch_bounds__(LM_THREADS, 1) k_lsum_mma(int nw, int nr, int 
 {
     extern __shared__ __align__(16) unsigned char lm_smem[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int k0 = blockIdx.x * LM_K, j0 = blockIdx.y * LM_J;
+    // grouped rasterisation (above): group g holds frequency tiles
+    // g F .. g F + Fg - 1 of every receiver tile, frequency tile fastest
+    const int nft = (nw + LM_J - 1) / LM_J, nrt = (nr + LM_K - 1) / LM_K;
+    const long long b = blockIdx.x;
+    const int grp = (int)(b / ((long long)group * nrt));
+    const int f0 = grp * group;
+    const int fg = min(group, nft - f0);
+    const int idx = (int)(b - (long long)grp * group * nrt);
+    const int k0 = (idx / fg) * LM_K, j0 = (f0 + idx % fg) * LM_J;
     const int jsub = warp & 1, ksub = warp >> 1;
     const int fr = lane >> 2, fc = lane & 3;      // fragment row / column of this lane
     // acc[slot][0..5]: ar re, ar im, at re, at im, ap re, ap im
@@ -259,19 +276,55 @@ __global__ void __launch_bounds__(LM_THREADS, 1) k_lsum_mma(int nw, int nr, int 
 
 bool lsum_uses_mma(int nr) { return nr >= 8; }
 
+// Group width F of the rasterisation: the modelled DRAM reads are the
+// coefficients once per group of receiver tiles in flight together plus
+// the Legendre rows once per group of frequency tiles; the working set (F
+// coefficient tiles, inflight / F Legendre tiles) should stay within half
+// of L2, else the smallest working set is taken.
+int lsum_group_width(int nft, int nrt, int L, int inflight, double l2_bytes)
+{
+    const double coef_tile = (double)LM_J * NCOEF * L * 16.0, leg_tile = (double)LM_K * L * 64.0;
+    const double coef_tot = nft * coef_tile, leg_tot = nrt * leg_tile;
+    int best = 1;
+    double best_reads = 0.0, best_ws = 0.0;
+    bool best_fits = false;
+    for (int F = 1; F <= nft; F++) {
+        const int R = std::max(1, inflight / F);
+        const double ws = F * coef_tile + std::min(R, nrt) * leg_tile;
+        const double reads = coef_tot * (double)((nrt + R - 1) / R) + leg_tot * (double)((nft + F - 1) / F);
+        const bool fits = ws <= 0.5 * l2_bytes;
+        const bool better = F == 1 || (fits && (!best_fits || reads < best_reads)) ||
+                            (!fits && !best_fits && ws < best_ws);
+        if (better) {
+            best = F;
+            best_reads = reads;
+            best_ws = ws;
+            best_fits = fits;
+        }
+    }
+    return best;
+}
+
 cudaError_t launch_lsum(int nw, int nr, int lmin, int lmax, const cd* coef, const double* T,
                         const cd* E, cd* ur, cd* ut, cd* up, cudaStream_t s)
 {
     if (nw <= 0 || nr <= 0) return cudaSuccess;
     const int L = lmax - lmin + 1;
     if (lsum_uses_mma(nr)) {
-        dim3 grid((nr + LM_K - 1) / LM_K, (nw + LM_J - 1) / LM_J);
-        if (grid.y > 65535) return cudaErrorInvalidValue;
+        const long long nft = (nw + LM_J - 1) / LM_J, nrt = (nr + LM_K - 1) / LM_K;
+        if (nft * nrt > 0x7fffffffLL) return cudaErrorInvalidValue;
         const size_t smem = 2 * LM_STAGE_BYTES;
         cudaError_t e = cudaFuncSetAttribute(k_lsum_mma, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)smem);
         if (e != cudaSuccess) return e;
-        k_lsum_mma<<<grid, LM_THREADS, smem, s>>>(nw, nr, L, lmin, coef, T, E, ur, ut, up);
+        int dev = 0, nsm = 0, l2 = 0, per = 0;
+        if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+        if ((e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+        if ((e = cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, dev)) != cudaSuccess) return e;
+        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_lsum_mma, LM_THREADS, smem)) != cudaSuccess)
+            return e;
+        const int group = lsum_group_width((int)nft, (int)nrt, L, nsm * std::max(per, 1), (double)l2);
+        k_lsum_mma<<<(unsigned)(nft * nrt), LM_THREADS, smem, s>>>(nw, nr, L, lmin, group, coef, T, E, ur, ut, up);
         return cudaGetLastError();
     }
     dim3 block(LS_J, LS_K);
