@@ -217,6 +217,10 @@ int main(int argc, char** argv)
     std::vector<double> lx(nmax), lh(nmax), lf(nmax), gr(gmax);
     std::vector<int> lil(nmax), gi(gmax);
     StepLog L{ly.data(), lx.data(), lh.data(), lil.data(), lf.data(), nmax, 1};
+    std::vector<cd> cy((size_t)nmax * N);
+    std::vector<double> cx(nmax), ch(nmax), cf(nmax);
+    std::vector<int> cil(nmax);
+    StepLog CL{cy.data(), cx.data(), ch.data(), cil.data(), cf.data(), nmax, 1};
     GridLog GL{gy.data(), gr.data(), gi.data(), gmax, 1};
     const int pairs[][2] = {{0, 3},      {0, ev.nw / 2}, {0, ev.nw},     {1, ev.nw},      {2, ev.nw},
                             {1, 3},      {2, 10},        {5, 40},        {20, ev.nw / 2}, {60, ev.nw},
@@ -243,8 +247,8 @@ int main(int argc, char** argv)
         if (l == 0) {
             ok = pair_radial_adj(c, U, ev, j, w, L, GL, G);
         } else {
-            if (l > 1) ok = pair_toroidal_adj(c, U, ev, l, j, w + 10, L, G);
-            ok = ok && pair_spheroidal_adj(c, U, ev, l, j, w, w + 5, L, G);
+            if (l > 1) ok = pair_toroidal_adj(c, U, ev, l, j, w + 10, L, CL, G);
+            ok = ok && pair_spheroidal_adj(c, U, ev, l, j, w, w + 5, L, CL, G);
         }
         G.flush();
         std::vector<double> yb, ysb;

@@ -881,7 +881,7 @@ int ensure_units(ysg_handle* h)
 // pieces per interval (split at the source and the receiver),
 // dr = alpha_min / (4 Re omega) or 1/4 at omega = 0 (module_model.f90:578-787
 // with module_int.f90:1145-1166).
-void adj_bounds(const ysg_handle* h, const EventDev& d, int* nmax, int* gmax)
+void adj_bounds(const ysg_handle* h, const EventDev& d, int* nmax, int* ncmax, int* gmax)
 {
     const int n = h->hdr.nknot;
     const double* r = h->r_host.data();
@@ -900,6 +900,8 @@ void adj_bounds(const ysg_handle* h, const EventDev& d, int* nmax, int* gmax)
     }
     const double smax = std::max(steps[0], std::max(steps[1], steps[2]));
     *nmax = (int)std::min(smax + 2.0, 1.0e8);
+    // the chain from the start level to the source crosses at most all three
+    *ncmax = (int)std::min(steps[0] + steps[1] + steps[2] + 2.0, 1.0e8);
     *gmax = (int)std::min(pts + 4.0, 1.0e8);
 }
 
@@ -1165,8 +1167,8 @@ int ysg_event_gradient(ysg_handle* h, const ysg_event* ev, const ysg_time* tm, c
     const int n = h->hdr.nknot, nw = ev->nw, nr = ev->nr;
     const TraceDev& td = s.ptd;
     const int nout = td.nout;
-    int nmax = 0, gmax = 0;
-    adj_bounds(h, s.pev, &nmax, &gmax);
+    int nmax = 0, ncmax = 0, gmax = 0;
+    adj_bounds(h, s.pev, &nmax, &ncmax, &gmax);
     // sweep work space: every resident thread of the l >= 1 sweeps (step
     // logs only) and one thread per frequency of the l = 0 sweeps (step and
     // grid logs), within a quarter of the free memory
@@ -1174,7 +1176,7 @@ int ysg_event_gradient(ysg_handle* h, const ysg_event* ev, const ysg_time* tm, c
     if (nblk <= 0) return YSG_ERR_CUDA;
     size_t free_b = 0, total_b = 0;
     CK(cudaMemGetInfo(&free_b, &total_b));
-    const size_t per = adj_log_bytes(nmax, 0), per_r = adj_log_bytes(nmax, gmax);
+    const size_t per = adj_log_bytes(nmax, ncmax, 0), per_r = adj_log_bytes(nmax, 0, gmax);
     const size_t Tr = ev->lmin == 0 ? (size_t)(nw + ADJ_THREADS - 1) / ADJ_THREADS * ADJ_THREADS : 0;
     const size_t budget = (free_b + h->alogs.cap) / 4;
     // no more threads than entries
@@ -1202,30 +1204,37 @@ int ysg_event_gradient(ysg_handle* h, const ysg_event* ev, const ysg_time* tm, c
     if (nr > 0)
         CK(cudaMemcpyAsync(h->agout.p, gout, (size_t)nout * 4 * nr * sizeof(double), cudaMemcpyHostToDevice, h->st));
     h->h2d += (double)(cs0.size() * sizeof(double) + (size_t)nout * 4 * nr * sizeof(double));
-    // work space layout per launch: complex arrays, then doubles, then ints
+    // work space: each log's arrays in turn (every size a multiple of 512
+    // bytes, as the thread counts are multiples of 128)
     unsigned char* base = h->alogs.as<unsigned char>();
     auto take = [&](size_t bytes) {
         unsigned char* q = base;
         base += bytes;
         return q;
     };
-    auto carve = [&](size_t nt, int ng) {
+    auto steps_of = [&](size_t nt, int n) {
+        AdjStepArrays a{};
+        a.n = n;
+        a.y = reinterpret_cast<cd*>(take((size_t)n * 14 * nt * sizeof(cd)));
+        a.x = reinterpret_cast<double*>(take((size_t)n * nt * sizeof(double)));
+        a.h = reinterpret_cast<double*>(take((size_t)n * nt * sizeof(double)));
+        a.f = reinterpret_cast<double*>(take((size_t)n * nt * sizeof(double)));
+        a.il = reinterpret_cast<int*>(take((size_t)n * nt * sizeof(int)));
+        return a;
+    };
+    auto carve = [&](size_t nt, int nc, int ng) {
         AdjLogs w{};
         w.nthreads = (int)nt;
-        w.nmax = nmax;
+        w.s = steps_of(nt, nmax);
+        w.c = steps_of(nt, nc);
         w.gmax = ng;
-        w.ly = reinterpret_cast<cd*>(take((size_t)nmax * 14 * nt * sizeof(cd)));
         w.gy = reinterpret_cast<cd*>(take((size_t)ng * 4 * nt * sizeof(cd)));
-        w.lx = reinterpret_cast<double*>(take((size_t)nmax * nt * sizeof(double)));
-        w.lh = reinterpret_cast<double*>(take((size_t)nmax * nt * sizeof(double)));
-        w.lf = reinterpret_cast<double*>(take((size_t)nmax * nt * sizeof(double)));
         w.gr = reinterpret_cast<double*>(take((size_t)ng * nt * sizeof(double)));
-        w.lil = reinterpret_cast<int*>(take((size_t)nmax * nt * sizeof(int)));
         w.gi = reinterpret_cast<int*>(take((size_t)ng * nt * sizeof(int)));
         return w;
     };
-    const AdjLogs w = carve(T, 0);
-    const AdjLogs wr = Tr ? carve(Tr, gmax) : AdjLogs{};
+    const AdjLogs w = carve(T, ncmax, 0);
+    const AdjLogs wr = Tr ? carve(Tr, 0, gmax) : AdjLogs{};
     UnitDirs u;
     for (int p = 0; p < NPARAM; p++) {
         u.kn[p] = h->ukn.as<Knot>() + (size_t)p * (n + 2);

@@ -116,6 +116,12 @@ __global__ void k_lsum_adjoint(int nw, int nr, int lmin, const double* __restric
     for (int q = 0; q < NCOEF; q++) coefb[((size_t)li * NCOEF + q) * nw + j] = acc[q];
 }
 
+// Thread tid's view of an interleaved step log.
+__device__ __forceinline__ StepLog step_log(const AdjStepArrays& a, int tid, int nthreads)
+{
+    return StepLog{a.y + tid, a.x + tid, a.h + tid, a.il + tid, a.f + tid, a.n, nthreads};
+}
+
 __device__ __forceinline__ void adj_ctx(primal::Ctx& c, const Knot* kn, const Seg* sg, const ModelHdr* mh,
                                         const EventDev& ev)
 {
@@ -129,9 +135,9 @@ __device__ __forceinline__ void adj_ctx(primal::Ctx& c, const Knot* kn, const Se
 }
 
 // Reverse sweeps of the l >= 1 entries (the l = 0 pairs go to
-// k_radial_adjoint).  Thread tid owns step log tid of the interleaved work
-// space; the grid holds exactly w.nthreads threads.  status bit 0: a sweep
-// exceeded its log.
+// k_radial_adjoint).  Thread tid owns scratch and chain step logs tid of
+// the interleaved work space; the grid holds exactly w.nthreads threads.
+// status bit 0: a sweep exceeded its logs.
 __global__ void __launch_bounds__(ADJ_THREADS) k_solve_adjoint(
     const Knot* __restrict__ kn, const Seg* __restrict__ sg, const ModelHdr* __restrict__ mh,
     const EventDev* __restrict__ evp, UnitDirs u, const cd* __restrict__ coefb,
@@ -139,7 +145,7 @@ __global__ void __launch_bounds__(ADJ_THREADS) k_solve_adjoint(
     unsigned long long* __restrict__ counter, int* __restrict__ status)
 {
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
-    StepLog L{w.ly + tid, w.lx + tid, w.lh + tid, w.lil + tid, w.lf + tid, w.nmax, w.nthreads};
+    StepLog L = step_log(w.s, tid, w.nthreads), CL = step_log(w.c, tid, w.nthreads);
     const EventDev ev = *evp;
     SegGrad G;
     G.init(grad);
@@ -168,8 +174,8 @@ __global__ void __launch_bounds__(ADJ_THREADS) k_solve_adjoint(
             any = any || wb[q].x != 0.0 || wb[q].y != 0.0;
         }
         if (!any) continue;                       // the pair does not reach L
-        const bool ok = part == 1 ? pair_toroidal_adj(c, u, ev, l, j, wb + 10, L, G)
-                                  : pair_spheroidal_adj(c, u, ev, l, j, wb, wb + 5, L, G);
+        const bool ok = part == 1 ? pair_toroidal_adj(c, u, ev, l, j, wb + 10, L, CL, G)
+                                  : pair_spheroidal_adj(c, u, ev, l, j, wb, wb + 5, L, CL, G);
         if (!ok) atomicOr(status, 1);
     }
     G.flush();
@@ -185,7 +191,7 @@ __global__ void __launch_bounds__(ADJ_THREADS) k_radial_adjoint(
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
     const EventDev ev = *evp;
     if (ev.lmin != 0) return;
-    StepLog L{w.ly + tid, w.lx + tid, w.lh + tid, w.lil + tid, w.lf + tid, w.nmax, w.nthreads};
+    StepLog L = step_log(w.s, tid, w.nthreads);
     GridLog GL{w.gy + tid, w.gr + tid, w.gi + tid, w.gmax, w.nthreads};
     SegGrad G;
     G.init(grad);

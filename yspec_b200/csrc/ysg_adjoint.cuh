@@ -342,7 +342,7 @@ __device__ void rk_step_adj(const Ctx& c, const cd* y, double x, double h, cd* y
 // e * st, so the logs of the threads of a launch can be interleaved (st =
 // the number of logs, each base pointer offset by its thread's index).
 struct StepLog {
-    cd* y;            // nmax x N
+    cd* y;            // nmax x LOG_N states
     double* x;        // nmax
     double* h;        // nmax
     int* il;          // nmax
@@ -351,23 +351,26 @@ struct StepLog {
     int st;
 };
 
+// Entry e of a step log holds its state at (e LOG_N + k) st: every system
+// takes LOG_N slots, so legs of different systems can share one log.
+constexpr int LOG_N = 14;
+
 // The forward yint of ysg_ode.cuh (same intervals, step counts and
-// rescaling) logging every step, then its adjoint: yb holds the adjoint of
-// the result on entry and that of the starting state y0 on exit.  Returns
-// false if the steps exceed the log.  One copy per system in the code (the
-// drivers call it from several places).
+// rescaling: scale counts the rescalings when non-null, as in yint) on y in
+// place, every step logged from entry `at` of L on; *ns receives the number
+// of steps.  Returns false if they exceed the log.
 template <class T>
-__device__ __noinline__ bool yint_adj(Ctx& c, int i1, int i2, double r1, double r2, const cd* y0, cd* yb,
-                                      bool scaled, StepLog& L, SegGrad& G)
+__device__ __noinline__ bool yint_log(Ctx& c, int i1, int i2, double r1, double r2, cd* y, int* scale,
+                                      StepLog& L, int at, int* ns)
 {
     constexpr int N = T::A::N;
+    static_assert(N <= LOG_N, "log slot too small");
+    *ns = 0;
     if (r2 == r1) return true;
-    cd y[N];
-    for (int k = 0; k < N; k++) y[k] = y0[k];
     const bool up = r2 > r1;
     const Knot* kn = c.kn;
     const int di = up ? 1 : -1;
-    int ns = 0;
+    int q = at;
     for (int i = i1; up ? (i <= i2) : (i >= i2); i += di) {
         double rr1, rr2;
         if (up) {
@@ -384,34 +387,61 @@ __device__ __noinline__ bool yint_adj(Ctx& c, int i1, int i2, double r1, double 
         int n = 2 + (int)fmin(nf, 4194304.0);
         drr = (rr2 - rr1) / (double)(n - 1);
         for (int j = 1; j <= n - 1; j++) {
-            if (ns >= L.nmax) return false;
+            if (q >= L.nmax) return false;
             double rr = __dadd_rn(rr1, __dmul_rn((double)(j - 1), drr));
-            const size_t e = (size_t)ns * L.st;
-            for (int k = 0; k < N; k++) L.y[((size_t)ns * N + k) * L.st] = y[k];
+            const size_t e = (size_t)q * L.st;
+            for (int k = 0; k < N; k++) L.y[((size_t)q * LOG_N + k) * L.st] = y[k];
             L.x[e] = rr;
             L.h[e] = drr;
             L.il[e] = i;
             yint_step<typename T::Sys>(c, y, rr, drr);
             double f = 1.0;
-            if (scaled) {
+            if (scale) {
                 int sc = 0;
                 rescale<N>(y, &sc);
+                *scale += sc;
                 f = sc > 0 ? SC_HUGE : (sc < 0 ? SC_TINY : 1.0);
             }
             L.f[e] = f;
-            ns++;
+            q++;
         }
     }
-    for (int q = ns - 1; q >= 0; q--) {
+    *ns = q - at;
+    return true;
+}
+
+// The adjoint of the ns steps logged from entry `at` of L on: yb holds the
+// adjoint of their result on entry and that of their starting state on exit.
+template <class T>
+__device__ __noinline__ void yint_rev(Ctx& c, const StepLog& L, int at, int ns, cd* yb, SegGrad& G)
+{
+    constexpr int N = T::A::N;
+    for (int q = at + ns - 1; q >= at; q--) {
         const size_t e = (size_t)q * L.st;
         c.il = L.il[e];
         const double f = L.f[e];
         if (f != 1.0)
             for (int k = 0; k < N; k++) yb[k] = f * yb[k];
         cd ys[N];
-        for (int k = 0; k < N; k++) ys[k] = L.y[((size_t)q * N + k) * L.st];
+        for (int k = 0; k < N; k++) ys[k] = L.y[((size_t)q * LOG_N + k) * L.st];
         rk_step_adj<T>(c, ys, L.x[e], L.h[e], yb, G);
     }
+}
+
+// A yint replayed from its starting state y0 into the log, then reversed:
+// yb holds the adjoint of the result on entry and that of y0 on exit.
+// Returns false if the steps exceed the log.
+template <class T>
+__device__ __forceinline__ bool yint_adj(Ctx& c, int i1, int i2, double r1, double r2, const cd* y0, cd* yb,
+                                         bool scaled, StepLog& L, SegGrad& G)
+{
+    constexpr int N = T::A::N;
+    if (r2 == r1) return true;
+    cd y[N];
+    for (int k = 0; k < N; k++) y[k] = y0[k];
+    int sc = 0, ns = 0;
+    if (!yint_log<T>(c, i1, i2, r1, r2, y, scaled ? &sc : nullptr, L, 0, &ns)) return false;
+    yint_rev<T>(c, L, 0, ns, yb, G);
     return true;
 }
 

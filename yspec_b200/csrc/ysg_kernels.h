@@ -82,27 +82,32 @@ cudaError_t launch_ifft(const TraceDev& td, const cd* ur, const cd* ut, const cd
                         const double* cs_azep, cd* scratch, double* out, cudaStream_t s);
 
 // Reverse mode (k_solve_adjoint.cu).  Work space of the reverse sweeps,
-// interleaved over threads: thread t's step log (nmax steps) and grid log
+// interleaved over threads: thread t's scratch step log (nmax steps: the
+// replayed integrations), chain step log (ncmax steps: the minor chain from
+// the start level to the source, logged in the forward pass) and grid log
 // (gmax points of the l = 0 gravity solve), entry e of an array at
 // e * nthreads + t.
 constexpr int ADJ_THREADS = 128;
+struct AdjStepArrays {
+    cd* y;             // n x 14 states
+    double* x;         // n radii
+    double* h;         // n step sizes
+    int* il;           // n intervals
+    double* f;         // n rescaling factors
+    int n;
+};
 struct AdjLogs {
-    cd* ly;            // nmax x 14 states
-    double* lx;        // nmax radii
-    double* lh;        // nmax step sizes
-    int* lil;          // nmax intervals
-    double* lf;        // nmax rescaling factors
-    int nmax;
+    AdjStepArrays s, c;  // scratch and chain step logs
     cd* gy;            // gmax x 4 states
     double* gr;        // gmax radii
     int* gi;           // gmax intervals
     int gmax;
     int nthreads;      // a multiple of ADJ_THREADS
 };
-inline size_t adj_log_bytes(int nmax, int gmax)
+inline size_t adj_step_bytes(int n) { return (size_t)n * (14 * sizeof(cd) + 3 * sizeof(double) + sizeof(int)); }
+inline size_t adj_log_bytes(int nmax, int ncmax, int gmax)
 {
-    return (size_t)nmax * (14 * sizeof(cd) + 3 * sizeof(double) + sizeof(int)) +
-           (size_t)gmax * (4 * sizeof(cd) + sizeof(double) + sizeof(int));
+    return adj_step_bytes(nmax) + adj_step_bytes(ncmax) + (size_t)gmax * (4 * sizeof(cd) + sizeof(double) + sizeof(int));
 }
 // resident blocks of k_solve_adjoint over the device (0 on failure)
 int solve_adjoint_blocks();

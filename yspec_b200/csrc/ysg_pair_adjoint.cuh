@@ -217,12 +217,12 @@ __device__ inline void f2s_adj(const cd* msb, cd* mfb)
 // The forward solve again, keeping what the reverse sweep needs; yb is the
 // adjoint of yout.  Returns false if a step log overflowed.
 __device__ inline bool tor_solver_adj(Ctx& c, const UnitDirs& u, double rr, double rs, int ir, int is,
-                                      const cd yb_out[2][2], cd yout[2][2], StepLog& L, SegGrad& G)
+                                      const cd yb_out[2][2], cd yout[2][2], StepLog& L, StepLog& CL, SegGrad& G)
 {
     const ModelHdr* mh = c.mh;
     const Knot* kn = c.kn;
     int scale1 = 0, scale2 = 0, scale3 = 0;
-    cd y1[2], y2[2], y3[2], y1s[2];
+    cd y1[2], y2[2], y3[2];
     const int it = is;
     int i1 = tor_start_level(c, c.ll, c.omega.x, it);
     if (i1 == it && i1 > mh->noc + 1) i1 = i1 - 1;
@@ -230,9 +230,10 @@ __device__ inline bool tor_solver_adj(Ctx& c, const UnitDirs& u, double rr, doub
     const bool cmb_start = i1 == mh->noc + 1;
     if (cmb_start) { y1[0] = mk(1.0); y1[1] = mk(0.0); }
     else tor_ystart(c, i1, rt, y1);
-    y1s[0] = y1[0];
-    y1s[1] = y1[1];
-    yint<TorSys>(c, i1, is, rt, rs, y1, &scale1);
+    // the leg from the start level to the source is logged as it runs (the
+    // chain log) and reversed last; the others are replayed when reversed
+    int n1 = 0;
+    if (!yint_log<TorT>(c, i1, is, rt, rs, y1, &scale1, CL, 0, &n1)) return false;
     y3[0] = y1[0];
     y3[1] = y1[1];
     if (rr != rs) yint<TorSys>(c, is, ir, rs, rr, y3, &scale3);
@@ -269,7 +270,7 @@ __device__ inline bool tor_solver_adj(Ctx& c, const UnitDirs& u, double rr, doub
     if (rr != rs && !yint_adj<TorT>(c, is, ir, rs, rr, y1, y3b, true, L, G)) return false;
     y1b[0] = y1b[0] + y3b[0];
     y1b[1] = y1b[1] + y3b[1];
-    if (!yint_adj<TorT>(c, i1, is, rt, rs, y1s, y1b, true, L, G)) return false;
+    yint_rev<TorT>(c, CL, 0, n1, y1b, G);
     if (!cmb_start) start_adj<0>(c, u, i1, rt, y1b, G);
     return true;
 }
@@ -279,7 +280,8 @@ __device__ inline bool tor_solver_adj(Ctx& c, const UnitDirs& u, double rr, doub
 // (module_solver.f90:640-823): yb_out (6 x 4) is the adjoint of yout.
 // ---------------------------------------------------------------------------
 __device__ inline bool sph_solver_g_adj(Ctx& c, const UnitDirs& u, double rr, double rs, int ir, int is,
-                                        const cd yb_out[6][4], cd yout[6][4], StepLog& L, SegGrad& G)
+                                        const cd yb_out[6][4], cd yout[6][4], StepLog& L, StepLog& CL,
+                                        SegGrad& G)
 {
     const ModelHdr* mh = c.mh;
     const Knot* kn = c.kn;
@@ -293,32 +295,33 @@ __device__ inline bool sph_solver_g_adj(Ctx& c, const UnitDirs& u, double rr, do
     // the chain from the start level to the source; branch 0: solid inner
     // core start, 1: fluid outer core start, 2: mantle start
     const int branch = i1 <= mh->nic ? 0 : (i1 <= mh->noc ? 1 : 2);
-    cd st[14], ms1[14], mf[5], mfs[5], ms_a[14], mf_a[5];
+    // The chain's legs (inner core, outer core, mantle to the source) are
+    // logged as they run, one after the other in the chain log, and reversed
+    // in the opposite order at the end; the other integrations are replayed
+    // in the scratch log when reversed.
+    cd st[14], ms1[14], mf[5];
+    int nic_s = 0, noc_s = 0, nm_s = 0;                          // steps of the three legs
     if (branch == 0) {
         sph_minor_solid_start(c, i1, rt, st);
         for (int k = 0; k < 14; k++) ms1[k] = st[k];
-        yint<MinorSolidG>(c, i1, mh->nic, rt, kn[mh->nic].r, ms1, &scale1);
-        for (int k = 0; k < 14; k++) ms_a[k] = ms1[k];           // before s2f
+        if (!yint_log<MinorSolidGT>(c, i1, mh->nic, rt, kn[mh->nic].r, ms1, &scale1, CL, 0, &nic_s)) return false;
         s2f(ms1, mf);
-        for (int k = 0; k < 5; k++) mfs[k] = mf[k];
-        yint<MinorFluidG>(c, mh->nic + 1, mh->noc, kn[mh->nic].r, kn[mh->noc].r, mf, &scale1);
-        for (int k = 0; k < 5; k++) mf_a[k] = mf[k];             // before f2s
+        if (!yint_log<MinorFluidGT>(c, mh->nic + 1, mh->noc, kn[mh->nic].r, kn[mh->noc].r, mf, &scale1, CL, nic_s,
+                                    &noc_s))
+            return false;
         f2s(mf, ms1);
     } else if (branch == 1) {
         sph_minor_fluid_start(c, i1, rt, mf);
-        for (int k = 0; k < 5; k++) mfs[k] = mf[k];
-        yint<MinorFluidG>(c, i1, mh->noc, rt, kn[mh->noc].r, mf, &scale1);
-        for (int k = 0; k < 5; k++) mf_a[k] = mf[k];
+        if (!yint_log<MinorFluidGT>(c, i1, mh->noc, rt, kn[mh->noc].r, mf, &scale1, CL, 0, &noc_s)) return false;
         f2s(mf, ms1);
     } else {
         sph_minor_solid_start(c, i1, rt, st);
         for (int k = 0; k < 14; k++) ms1[k] = st[k];
     }
-    cd msm[14];                                                  // solid state entering the last leg
-    for (int k = 0; k < 14; k++) msm[k] = ms1[k];
     const int mi1 = branch == 2 ? i1 : mh->noc + 1;
     const double mr1 = branch == 2 ? rt : kn[mh->noc + 1].r;
-    yint<MinorSolidG>(c, mi1, it, mr1, rtop, ms1, &scale1);
+    const int moff = nic_s + noc_s;
+    if (!yint_log<MinorSolidGT>(c, mi1, it, mr1, rtop, ms1, &scale1, CL, moff, &nm_s)) return false;
     cd ms3[14], ms2[14];
     for (int k = 0; k < 14; k++) ms3[k] = ms1[k];
     if (rr > rs) yint<MinorSolidG>(c, is, ir, rs, rr, ms3, &scale3);
@@ -335,10 +338,10 @@ __device__ inline bool sph_solver_g_adj(Ctx& c, const UnitDirs& u, double rr, do
         cd s[6];
         unit(s, 6, jump[i]);
         int scale4 = 0;
-        cd b0[14], b[14], ys[6];
-        b_solid_start(ms1, s, b0);
-        for (int k = 0; k < 14; k++) b[k] = b0[k];
-        yint<BvecSolidG>(c, is, ir, rs, rr, b, &scale4);
+        cd b[14], ys[6];
+        b_solid_start(ms1, s, b);
+        int nb = 0;
+        if (!yint_log<BvecSolidGT>(c, is, ir, rs, rr, b, &scale4, L, 0, &nb)) return false;
         sph_ysol(ms2, b, ys);
         // yout[k][i] = (-ys[k] / delta) huge^(scale3 - scale4)
         const double F = huge_pow(scale3 - scale4);
@@ -352,7 +355,7 @@ __device__ inline bool sph_solver_g_adj(Ctx& c, const UnitDirs& u, double rr, do
         cd bb[14];
         for (int k = 0; k < 14; k++) bb[k] = mk(0.0);
         ysol_adj(ms2, b, ysb, ms2b, bb);
-        if (!yint_adj<BvecSolidGT>(c, is, ir, rs, rr, b0, bb, true, L, G)) return false;
+        yint_rev<BvecSolidGT>(c, L, 0, nb, bb, G);
         bstart_adj(s, bb, ms1b);
     }
     delta_adj(ms3, ms2, deltab, ms3b, ms2b);
@@ -362,7 +365,7 @@ __device__ inline bool sph_solver_g_adj(Ctx& c, const UnitDirs& u, double rr, do
     }
     for (int k = 0; k < 14; k++) ms1b[k] = ms1b[k] + ms3b[k];
     // back along the chain to the start level
-    if (!yint_adj<MinorSolidGT>(c, mi1, it, mr1, rtop, msm, ms1b, true, L, G)) return false;
+    yint_rev<MinorSolidGT>(c, CL, moff, nm_s, ms1b, G);
     if (branch == 2) {
         start_adj<1>(c, u, i1, rt, ms1b, G);
         return true;
@@ -370,20 +373,16 @@ __device__ inline bool sph_solver_g_adj(Ctx& c, const UnitDirs& u, double rr, do
     cd mfb[5];
     for (int k = 0; k < 5; k++) mfb[k] = mk(0.0);
     f2s_adj(ms1b, mfb);
+    yint_rev<MinorFluidGT>(c, CL, nic_s, noc_s, mfb, G);
     if (branch == 1) {
-        if (!yint_adj<MinorFluidGT>(c, i1, mh->noc, rt, kn[mh->noc].r, mfs, mfb, true, L, G)) return false;
         start_adj<2>(c, u, i1, rt, mfb, G);
         return true;
     }
-    if (!yint_adj<MinorFluidGT>(c, mh->nic + 1, mh->noc, kn[mh->nic].r, kn[mh->noc].r, mfs, mfb, true, L, G))
-        return false;
     cd msb[14];
     for (int k = 0; k < 14; k++) msb[k] = mk(0.0);
     s2f_adj(mfb, msb);
-    if (!yint_adj<MinorSolidGT>(c, i1, mh->nic, rt, kn[mh->nic].r, st, msb, true, L, G)) return false;
+    yint_rev<MinorSolidGT>(c, CL, 0, nic_s, msb, G);
     start_adj<1>(c, u, i1, rt, msb, G);
-    (void)ms_a;
-    (void)mf_a;
     return true;
 }
 
@@ -581,7 +580,7 @@ __device__ __forceinline__ bool pair_adj_supported(const ModelHdr* mh, const Eve
 // sweep runs first and its own forward pass supplies the output that the
 // source vectors' adjoints need.
 __device__ inline bool pair_toroidal_adj(Ctx& c, const UnitDirs& u, const EventDev& ev, int l, int j,
-                                         const cd* wwb, StepLog& L, SegGrad& G)
+                                         const cd* wwb, StepLog& L, StepLog& CL, SegGrad& G)
 {
     const cd w = omega_of(ev, j);
     set_l(c, l);
@@ -601,7 +600,7 @@ __device__ inline bool pair_toroidal_adj(Ctx& c, const UnitDirs& u, const EventD
     if (ev.out != 0)
         for (int a = 0; a < 2; a++)
             for (int b = 0; b < 2; b++) yb[a][b] = f * yb[a][b];
-    if (!tor_solver_adj(c, u, ev.rr, ev.rs, ev.ir, ev.is, yb, ytor, L, G)) return false;
+    if (!tor_solver_adj(c, u, ev.rr, ev.rs, ev.ir, ev.is, yb, ytor, L, CL, G)) return false;
     if (ev.out != 0)
         for (int a = 0; a < 2; a++)
             for (int b = 0; b < 2; b++) ytor[a][b] = f * ytor[a][b];
@@ -618,7 +617,7 @@ __device__ inline bool pair_toroidal_adj(Ctx& c, const UnitDirs& u, const EventD
 // uub, vvb: adjoints of uu(1:5), vv(1:5) of pair (l >= 1, j); the same
 // order as the toroidal part.
 __device__ inline bool pair_spheroidal_adj(Ctx& c, const UnitDirs& u, const EventDev& ev, int l, int j,
-                                           const cd* uub, const cd* vvb, StepLog& L, SegGrad& G)
+                                           const cd* uub, const cd* vvb, StepLog& L, StepLog& CL, SegGrad& G)
 {
     const cd w = omega_of(ev, j);
     set_l(c, l);
@@ -666,7 +665,7 @@ __device__ inline bool pair_spheroidal_adj(Ctx& c, const UnitDirs& u, const Even
             }
         }
     }
-    if (!sph_solver_g_adj(c, u, ev.rr, ev.rs, ev.ir, ev.is, yb, ysph, L, G)) return false;
+    if (!sph_solver_g_adj(c, u, ev.rr, ev.rs, ev.ir, ev.is, yb, ysph, L, CL, G)) return false;
     // grav(ir), the c0 coefficient of segment ir, through the correction
     if (ev.out == 2 && ev.cor != 0) {
         double gb = 0.0;
