@@ -105,6 +105,18 @@ module yspec_gpu
        integer(c_int), intent(out) :: nouts(*)
      end function ysg_batch_run
 
+     ! potential traces: out(nout, 2, nr) = t, potential; tm%amp_norm the
+     ! potential's normalisation for the output type
+     integer(c_int) function ysg_event_potential(h, ev, tm, out, nout) &
+          bind(C, name="ysg_event_potential")
+       import :: c_int, c_ptr, c_double, ysg_event, ysg_time
+       type(c_ptr), value :: h
+       type(ysg_event), intent(in) :: ev
+       type(ysg_time), intent(in) :: tm
+       real(c_double), intent(out) :: out(*)
+       integer(c_int), intent(out) :: nout
+     end function ysg_event_potential
+
      ! dL/dval(p, i), dL/dcs(p, i) of L = sum gout * traces (reverse mode):
      ! gout(nout, 4, nr) as ysg_event_run's out; gval, gcs (nknot, 13)
      integer(c_int) function ysg_event_gradient(h, ev, tm, gout, gval, gcs) &

@@ -114,6 +114,23 @@ int ysg_model_tangent_upload(ysg_handle *h, const ysg_model *dm);
  * YSG_ERR_LIMIT. */
 int ysg_model_tangents_upload(ysg_handle *h, int ndir, const ysg_model *dms);
 
+/* Potential traces of one event: the perturbation of the gravitational
+ * potential at every receiver, in the event's output type (potential, its
+ * first or second time derivative).  Each pair contributes its potential
+ * coefficients in place of uu: the spheroidal solution's third component
+ * (ysph(3,:), the potential; zero without self-gravitation) combined with
+ * the source vectors as uu is in yspec.f90:396-398, and for l = 0 the
+ * potential that rad_solver_wg forms and the main program discards
+ * (module_solver.f90:534-554); toroidal pairs contribute nothing.  The
+ * l-sum and the time stage (module_fourier.f90 ifft4 applied to the
+ * potential row, then yspec.f90:432-473) are those of the displacement.
+ * out is (nout, 2, nr) column-major: time in seconds, then the potential;
+ * tm->amp_norm must be the potential's normalisation for the output type
+ * (pot_norm, pot_norm / t_norm or pot_norm / t_norm^2, module_model.f90:489).
+ * No reference counterpart as a whole: the reference computes these pieces
+ * but never writes potential traces. */
+int ysg_event_potential(ysg_handle *h, const ysg_event *ev, const ysg_time *tm, double *out, int *nout);
+
 /* Gradient of the misfit functional L = sum gout * traces of one event
  * with respect to the uploaded model (reverse mode: the discrete adjoint of
  * every (omega, l) solve, after the transposes of the time stage and of the

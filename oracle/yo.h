@@ -145,6 +145,17 @@ int yo_green(const yo_model *m, const yo_norms *n, int kind, int l, double wr,
  * the reference's rule, module_int.f90:1903-1905).  Process-wide. */
 void yo_set_step_refine(int refine);
 
+/* Potential mode: yo_solve_pair and everything built on it (spectra,
+ * traces) return the perturbation of the gravitational potential at the
+ * receivers in place of the displacement: per pair the spheroidal
+ * solution's third component (ysph(3,:)) combined with the source vectors
+ * as uu, for l = 0 the potential of rad_solver_wg (module_solver.f90:
+ * 534-554), no toroidal part; ur carries the potential, ut and up are zero.
+ * The time stage's amplitude factor stays that of the output type (the
+ * caller rescales to the potential's normalisation).  Process-wide;
+ * 0 restores the reference's outputs. */
+void yo_set_potential(int on);
+
 /* Legendre/geometry table used by the l-sum (yspec.f90:144-174):
  * xa/xpa/xca are (lmax+1, 3, nr) column-major; delta/azst/azep are nr. */
 void yo_geometry(const yo_params *p, double *delta, double *azep,

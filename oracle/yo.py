@@ -92,6 +92,7 @@ def lib() -> C.CDLL:
                                C.c_double, C.c_int, C.c_double, C.c_double, C.c_int, C.c_int, _dp]
         L.yo_find_radius_index.argtypes = [C.POINTER(Model), C.c_double]
         L.yo_set_step_refine.argtypes = [C.c_int]
+        L.yo_set_potential.argtypes = [C.c_int]
         L.yo_geometry.argtypes = [C.POINTER(Params), _dp, _dp, _dp]
         L.yo_legendre_table.argtypes = [_dp, C.c_int, C.c_int, _dp, _dp, _dp]
         L.yo_traces.argtypes = [C.POINTER(Norms), C.POINTER(Params), C.POINTER(Grid), _dp, _dp, _dp,
@@ -242,6 +243,34 @@ class Problem:
 
     def run(self, nthreads: int = 0) -> np.ndarray:
         return self.traces(*self.spectra(nthreads=nthreads))
+
+    def potential_traces(self, nthreads: int = 0) -> np.ndarray:
+        """Potential traces (nr, 2, nout): time and the perturbation of the
+        gravitational potential at each receiver in SI units, in the
+        output type (see yo_set_potential)."""
+        with potential():
+            ur, ut, up = self.spectra(nthreads=nthreads)
+        out = self.traces(ur, ut, up)
+        n = self.norms
+        o = self.params.out
+        amp = n.r_norm if o == 0 else (n.vel_norm if o == 1 else n.acl_norm)
+        res = np.empty((out.shape[0], 2, out.shape[2]))
+        res[:, 0] = out[:, 0]
+        res[:, 1] = out[:, 1] / amp * (n.pot_norm / n.t_norm ** o)
+        return res
+
+
+class potential:
+    """Context manager: the oracle's solves return potential coefficients
+    (yo_set_potential)."""
+
+    def __enter__(self):
+        lib().yo_set_potential(1)
+        return self
+
+    def __exit__(self, *exc):
+        lib().yo_set_potential(0)
+        return False
 
 
 class step_refine:

@@ -51,6 +51,12 @@ int yo_event_setup(const yo_model *m, const yo_norms *n, const yo_params *p,
     return 0;
 }
 
+/* Potential mode (yo_set_potential): each pair's uu carries its potential */
+/* coefficients, vv and ww are zero.  Process-wide.                         */
+static int g_potential = 0;
+
+void yo_set_potential(int on) { g_potential = on != 0; }
+
 /* yspec.f90:259-400 for one (omega_j, l) */
 void yo_solve_pair(const yo_model *m, const yo_norms *n, const yo_params *p,
                    const yo_grid *g, int l, int j, yo_cd coef[15], yo_counts *cnt)
@@ -73,14 +79,21 @@ void yo_solve_pair(const yo_model *m, const yo_norms *n, const yo_params *p,
     if (l == 0) {
         yo_cd sr0[2], yrad[2][2];
         yo_source_vector_rad(&c, w, is, rs, g->mm, sr0);
-        if (p->grav == 0) yo_rad_solver_ng(&c, w, rr, rs, ir, is, yrad);
-        else yo_rad_solver_wg(&c, w, rr, rs, ir, is, yrad);
-        uu[2] = (sr0[0] * yrad[0][0] + sr0[1] * yrad[0][1]) / rr;
+        if (g_potential) {
+            /* the potential of rad_solver_wg (module_solver.f90:534-554) */
+            yo_cd ph[2] = {0.0, 0.0};
+            if (p->grav != 0) yo_rad_solver_wg(&c, w, rr, rs, ir, is, yrad, ph);
+            uu[2] = (sr0[0] * ph[0] + sr0[1] * ph[1]) / rr;
+        } else {
+            if (p->grav == 0) yo_rad_solver_ng(&c, w, rr, rs, ir, is, yrad);
+            else yo_rad_solver_wg(&c, w, rr, rs, ir, is, yrad, NULL);
+            uu[2] = (sr0[0] * yrad[0][0] + sr0[1] * yrad[0][1]) / rr;
+        }
         if (p->out == 1) uu[2] = I_ * w * uu[2];
         else if (p->out == 2) uu[2] = -(w * w * uu[2]);
         return;
     }
-    if (l > 1) {
+    if (l > 1 && !g_potential) {
         yo_cd svt[5][2], ytor[2][2];
         yo_source_vector_tor(&c, l, w, is, rs, g->mm, svt);
         yo_tor_solver(&c, l, w, rr, rs, ir, is, ytor);
@@ -107,6 +120,18 @@ void yo_solve_pair(const yo_model *m, const yo_norms *n, const yo_params *p,
             ysph[4][b] = yng[3][b];
             ysph[5][b] = 0.0;
         }
+    }
+    if (g_potential) {
+        /* the potential (third solution component) in the output type,     */
+        /* combined with the source vectors as uu (yspec.f90:396-398)        */
+        for (int b = 0; b < 4; b++) {
+            if (p->out == 1) ysph[2][b] = I_ * w * ysph[2][b];
+            else if (p->out == 2) ysph[2][b] = -(w * w * ysph[2][b]);
+        }
+        for (int q = 0; q < 5; q++)
+            uu[q] = (ysph[2][0] * svs[q][0] + ysph[2][1] * svs[q][1] +
+                     ysph[2][2] * svs[q][3] + ysph[2][3] * svs[q][4]) / rr;
+        return;
     }
     if (p->out == 1) {
         for (int a = 0; a < 3; a++)
@@ -409,7 +434,7 @@ int yo_green(const yo_model *m, const yo_norms *n, int kind, int l, double wr, d
     } else if (kind == 1 || kind == 2) {
         yo_cd y[2][2];
         if (kind == 1) yo_rad_solver_ng(&c, w, rr, rs, ir, is, y);
-        else yo_rad_solver_wg(&c, w, rr, rs, ir, is, y);
+        else yo_rad_solver_wg(&c, w, rr, rs, ir, is, y, NULL);
         for (int a = 0; a < 2; a++) for (int b = 0; b < 2; b++) out[2 * a + b] = y[a][b];
     } else if (kind == 3) {
         yo_cd y[6][4];

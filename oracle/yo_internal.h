@@ -29,7 +29,7 @@ void yo_tor_solver(yo_ctx *c, int l, yo_cd w, double rr, double rs, int ir, int 
 void yo_rad_solver_ng(yo_ctx *c, yo_cd w, double rr, double rs, int ir, int is,
                       yo_cd yout[2][2]);
 void yo_rad_solver_wg(yo_ctx *c, yo_cd w, double rr, double rs, int ir, int is,
-                      yo_cd yout[2][2]);
+                      yo_cd yout[2][2], yo_cd *pout1);
 void yo_sph_solver_g(yo_ctx *c, int l, yo_cd w, double rr, double rs, int ir, int is,
                      int fic, yo_cd yout[6][4]);
 void yo_sph_solver_ngcow(yo_ctx *c, int l, yo_cd w, double rr, double rs, int ir,

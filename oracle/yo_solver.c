@@ -1014,10 +1014,11 @@ static void make_grid(const yo_model *m, double drr, double rs, double rr, int *
     }
 }
 
-/* module_solver.f90:446-561 rad_solver_wg.  Only yout is returned: the    */
-/* potential pout is not used by the main program (yspec.f90:277-281).      */
+/* module_solver.f90:446-561 rad_solver_wg.  The main program does not use */
+/* the potential pout (yspec.f90:277-281); with pout1 non-NULL, pout(1, i)  */
+/* of the two unit sources i is formed as at :534-554.                      */
 void yo_rad_solver_wg(yo_ctx *c, yo_cd w, double rr, double rs, int ir, int is,
-                      yo_cd yout[2][2])
+                      yo_cd yout[2][2], yo_cd *pout1)
 {
     const yo_model *m = c->M;
     (void)ir; (void)is;
@@ -1059,6 +1060,21 @@ void yo_rad_solver_wg(yo_ctx *c, yo_cd w, double rr, double rs, int ir, int is,
             b = y1[1] * s1 - y1[0] * s2;
             yout[0][i] = -(delta * y2s[2 * irr] * b);
             yout[1][i] = -(delta * y2s[2 * irr + 1] * b);
+        }
+        if (pout1) {
+            /* ys(1, ig): below the source from y1s, above from y2s (:517-527); */
+            /* phi = rr * trapezoid sum of -4 pibigg ys(1) / r, zero at ig = 1  */
+            yo_cd bb = y2[1] * s1 - y2[0] * s2, ba = y1[1] * s1 - y1[0] * s2;
+            yo_cd sum = 0.0, ctmp1, ctmp2;
+            for (int ig = 1; ig <= irr - 1; ig++) {
+                yo_cd ys1 = ig <= iss ? -(delta * y1s[2 * ig] * bb) : -(delta * y2s[2 * ig] * ba);
+                yo_cd ys2 = ig + 1 <= iss ? -(delta * y1s[2 * (ig + 1)] * bb)
+                                          : -(delta * y2s[2 * (ig + 1)] * ba);
+                ctmp1 = ig == 1 ? 0.0 : -4.0 * c->N->pibigg * ys1 / rgrid[ig];
+                ctmp2 = -4.0 * c->N->pibigg * ys2 / rgrid[ig + 1];
+                sum = sum + 0.5 * (ctmp1 + ctmp2) * (rgrid[ig + 1] - rgrid[ig]);
+            }
+            pout1[i] = rr * sum;
         }
     }
     free(igrid); free(rgrid); free(y1s); free(y2s);

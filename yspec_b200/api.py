@@ -241,6 +241,21 @@ class Engine:
         N.check(N.lib().ysg_batch_run(self.h, nev, evs, tms, ptrs, nouts), "batch_run")
         return outs
 
+    def potential(self, event: Event) -> np.ndarray:
+        """Potential traces (nr, 2, nout): time in seconds and the perturbation
+        of the gravitational potential at each receiver in SI units, in the
+        event's output type (potential, or its first or second time
+        derivative)."""
+        nrm = norms()
+        out_type = event.raw.ev.out
+        tm = N.YsgTime.from_buffer_copy(event.raw.tm)
+        tm.amp_norm = nrm["pot_norm"] / nrm["t_norm"] ** out_type
+        out = np.zeros((event.nr, 2, event.nout()))
+        n = C.c_int()
+        N.check(N.lib().ysg_event_potential(self.h, C.byref(event.raw.ev), C.byref(tm), N.dptr(out), C.byref(n)),
+                "event_potential")
+        return out
+
     def gradient(self, event: Event, gout: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
         """Reverse mode: the gradient of L = sum(gout * traces) with respect to
         the uploaded model's knot arrays.  gout is (nr, 4, nout) like run()'s

@@ -96,6 +96,7 @@ struct ysg_handle {
     cudaEvent_t ev[6] = {};          // stage boundaries 0..4; 5 = end of an overlapped K2
     bool leg_overlap = false;        // K2 of the last single event ran beside K1
     int solver = 1;
+    int pot_mode = 0;                // events uploaded in potential mode (ysg_event_potential)
     // model
     DevBuf kn, sg, hdr_dev;
     ModelHdr hdr{};
@@ -206,6 +207,7 @@ EventDev make_event(const ysg_handle* h, const ysg_event* ev)
     d.wmin = ev->wmin;
     d.dw = ev->dw;
     d.grav_ir = h->grav_host[(size_t)ev->ir - 1];
+    d.pot = h->pot_mode;
     for (int i = 0; i < 6; i++) d.mm[i] = ev->mm[i];
     return d;
 }
@@ -1138,6 +1140,37 @@ int ysg_event_coef(ysg_handle* h, const ysg_event* ev, double* coef)
     if (coef) CK(cudaMemcpyAsync(coef, slot0(h).coef.p, n * sizeof(cd), cudaMemcpyDeviceToHost, h->st));
     rc = finish(h, 1, true, false);
     h->has_spectra = false;
+    return rc;
+}
+
+int ysg_event_potential(ysg_handle* h, const ysg_event* ev, const ysg_time* tm, double* out, int* nout)
+{
+    int rc = check_event(h, ev);
+    if (rc) return rc;
+    if (!tm || tm->nr != ev->nr) return YSG_ERR_ARG;
+    cudaSetDevice(h->device);
+    h->has_spectra = false;
+    h->h2d = h->d2h = 0.0;
+    h->pot_mode = 1;
+    rc = prepare_single(h, ev);
+    h->launches = 0;          // count this call's kernels only (not autotuning)
+    if (!rc) rc = upload_time(h, slot0(h), tm, ev->nw);
+    h->pot_mode = 0;
+    if (rc) return rc;
+    rc = enqueue_spectra(h, 1);
+    if (!rc) rc = enqueue_traces(h, 1, 0);
+    if (rc) return rc;
+    const Slot& s = slot0(h);
+    const TraceDev& td = s.ptd;
+    if (nout) *nout = td.nout;
+    if (out && td.nr > 0) {
+        // columns 0 (time) and 1 (the potential, in the Z position) of each receiver
+        CK(cudaMemcpy2DAsync(out, (size_t)2 * td.nout * sizeof(double), s.out.p, (size_t)4 * td.nout * sizeof(double),
+                             (size_t)2 * td.nout * sizeof(double), (size_t)td.nr, cudaMemcpyDeviceToHost, h->st));
+        h->d2h += (double)td.nout * 2 * td.nr * sizeof(double);
+    }
+    rc = finish(h, 1, true, true);
+    h->has_spectra = false;            // the device spectra hold the potential, not displacements
     return rc;
 }
 

@@ -38,6 +38,7 @@ struct ModelHdr {
 struct EventDev {
     int lmin, lmax, nw, is, ir, ats, grav, out, cor, nr;
     int jofs, jstride;   // frequency shard: local j -> full-band index jofs + (j-1) jstride
+    int pot;             // 1: potential coefficients in place of the displacement ones
     double rs, rr, ep, wmin, dw, grav_ir;
     double mm[6];
 };

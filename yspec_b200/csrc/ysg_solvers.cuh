@@ -198,10 +198,17 @@ __device__ __forceinline__ int seg_npts(const GridSeg& s, double drr)
     return (int)floor((s.b - s.a) / drr) + 2;
 }
 
-// module_solver.f90:446-561 rad_solver_wg.  The potential pout is not used
-// by the main program (yspec.f90:277-281) and is not formed.
-__device__ inline void rad_solver_wg(Ctx& c, double rr, double rs, mcplx yout[2][2])
+// module_solver.f90:446-561 rad_solver_wg.  The main program does not use
+// the potential (yspec.f90:277-281); with pot non-null it is formed as
+// there (:534-554, pout(1, i) for the two unit sources i): rr times the
+// trapezoid sum over grid points 1 .. irr of -4 pibigg ys(1) / r, the
+// value at the first point taken as zero.  ys is -delta y1s b_below at
+// points up to the source and -delta y2s b_above beyond it, so the sum is
+// collected on the two walks as S1 (over y1s) and S2 (over y2s) and
+// combined at the end.
+__device__ inline void rad_solver_wg(Ctx& c, double rr, double rs, mcplx yout[2][2], mcplx* pot = nullptr)
 {
+    if (YSG_COUNT_ONLY) pot = nullptr;              // the cost model counts steps only
     const ModelHdr* mh = c.mh;
     const Knot* kn = c.kn;
     const double drr = c.dr;
@@ -221,10 +228,13 @@ __device__ inline void rad_solver_wg(Ctx& c, double rr, double rs, mcplx yout[2]
     }
     // pass 2: upward from rt through grid points 2..iss
     mcplx y1[2], yrec[2] = {mk(0.0), mk(0.0)};
+    mcplx s1 = mk(0.0), s2 = mk(0.0), g1_iss = mk(0.0), g2_next = mk(0.0);
+    double r_iss = 0.0, r_next = 0.0;
     bool have_rec = false;
     {
         int k = 0, iprev = 0;
         double rprev = 0.0;
+        mcplx gprev = mk(0.0);                       // y1s(1) / r at the previous point
         bool started = false;
         for (int i = 1; i <= mh->nknot - 1 && k < iss; i++) {
             double r1 = kn[i].r, r2 = kn[i + 1].r;
@@ -247,6 +257,12 @@ __device__ inline void rad_solver_wg(Ctx& c, double rr, double rs, mcplx yout[2]
                         yint<RadSys>(c, iprev, i, rprev, rk, y1, nullptr);
                     }
                     if (started && k == irr) { yrec[0] = y1[0]; yrec[1] = y1[1]; have_rec = true; }
+                    if (pot && k >= 2) {
+                        const mcplx g = y1[0] / rk;
+                        if (k <= irr) s1 = s1 + (0.5 * (rk - rprev)) * (gprev + g);
+                        if (k == iss) { g1_iss = g; r_iss = rk; }
+                        gprev = g;
+                    }
                     iprev = i;
                     rprev = rk;
                 }
@@ -272,6 +288,13 @@ __device__ inline void rad_solver_wg(Ctx& c, double rr, double rs, mcplx yout[2]
                     double rk = __dadd_rn(sg[q].a, __dmul_rn((double)(jj - 1), drt));
                     if (k < ngrid) yint<RadSys>(c, iprev, i, rprev, rk, y2, nullptr);
                     if (k == irr && irr > iss) { yrec[0] = y2[0]; yrec[1] = y2[1]; have_rec = true; }
+                    if (pot && k > iss) {
+                        const mcplx g = y2[0] / rk;
+                        // segment [k, k + 1] within [1, irr], above the source
+                        if (k < ngrid && k + 1 <= irr) s2 = s2 + (0.5 * (rprev - rk)) * (g + g2_next);
+                        g2_next = g;
+                        r_next = rk;
+                    }
                     iprev = i;
                     rprev = rk;
                 }
@@ -286,6 +309,17 @@ __device__ inline void rad_solver_wg(Ctx& c, double rr, double rs, mcplx yout[2]
     mcplx dy0 = delta * yrec[0], dy1 = delta * yrec[1];
     yout[0][0] = -(dy0 * b0); yout[1][0] = -(dy1 * b0);
     yout[0][1] = -(dy0 * b1); yout[1][1] = -(dy1 * b1);
+    if (pot) {
+        // the segment across the source, [iss, iss + 1]
+        if (iss + 1 <= irr && iss + 1 <= ngrid) {
+            s1 = s1 + (0.5 * (r_next - r_iss)) * g1_iss;
+            s2 = s2 + (0.5 * (r_next - r_iss)) * g2_next;
+        }
+        // pout(1, i) = rr (-4 pibigg) (-delta) (b_below_i S1 + b_above_i S2)
+        const mcplx f = (rr * (4.0 * c.mh->pibigg)) * delta;
+        pot[0] = f * (y2[1] * s1 + y1[1] * s2);
+        pot[1] = f * (-(y2[0] * s1) - y1[0] * s2);
+    }
 }
 
 // Spheroidal solve with self-gravitation: sph_solver (:640-823) and
@@ -548,9 +582,18 @@ __device__ inline void pair_radial(Ctx& c, const EventDev& ev, int j, mcplx* coe
     mcplx sr0[2], yrad[2][2];
     source_vector_rad(c, ev.is, ev.rs, ev.mm, sr0);
     alpha_steps(c);
-    if (ev.grav == 0) rad_solver_ng(c, ev.rr, ev.rs, ev.ir, ev.is, yrad);
-    else rad_solver_wg(c, ev.rr, ev.rs, yrad);
-    mcplx u3 = (sr0[0] * yrad[0][0] + sr0[1] * yrad[0][1]) / ev.rr;
+    mcplx u3;
+    if (ev.pot) {
+        // the potential at the receiver (module_solver.f90:534-554); no
+        // gravity, no potential
+        mcplx ph[2] = {mk(0.0), mk(0.0)};
+        if (ev.grav != 0) rad_solver_wg(c, ev.rr, ev.rs, yrad, ph);
+        u3 = (sr0[0] * ph[0] + sr0[1] * ph[1]) / ev.rr;
+    } else {
+        if (ev.grav == 0) rad_solver_ng(c, ev.rr, ev.rs, ev.ir, ev.is, yrad);
+        else rad_solver_wg(c, ev.rr, ev.rs, yrad);
+        u3 = (sr0[0] * yrad[0][0] + sr0[1] * yrad[0][1]) / ev.rr;
+    }
     if (ev.out != 0) u3 = out_factor(ev.out, w) * u3;
     for (int q = 0; q < NCOEF; q++) coef[q] = mk(0.0);
     coef[2] = u3;
@@ -559,6 +602,10 @@ __device__ inline void pair_radial(Ctx& c, const EventDev& ev, int j, mcplx* coe
 // l >= 2: toroidal part, yspec.f90:301-316 -> ww(1:5)
 __device__ inline void pair_toroidal(Ctx& c, const EventDev& ev, int l, int j, mcplx* ww)
 {
+    if (ev.pot) {                                     // toroidal motion carries no potential
+        for (int q = 0; q < 5; q++) ww[q] = mk(0.0);
+        return;
+    }
     cd w = omega_of(ev, j);
     set_l(c, l);
     set_omega(c, w);
@@ -597,6 +644,21 @@ __device__ inline void pair_spheroidal(Ctx& c, const EventDev& ev, int l, int j,
         }
     }
     double zeta = (double)sqrtf((float)(l * (l + 1)));   // yspec.f90:255 (FP32)
+    if (ev.pot) {
+        // the potential perturbation at the receiver (the third solution
+        // component, zero without self-gravitation) in the output type of
+        // the event, combined with the source vectors as uu
+        if (ev.out != 0) {
+            const cd f = out_factor(ev.out, w);
+            for (int b = 0; b < 4; b++) ysph[2][b] = f * ysph[2][b];
+        }
+        for (int q = 0; q < 5; q++) {
+            uu[q] = (ysph[2][0] * svs[q][0] + ysph[2][1] * svs[q][1] + ysph[2][2] * svs[q][3] +
+                     ysph[2][3] * svs[q][4]) / ev.rr;
+            vv[q] = mk(0.0);
+        }
+        return;
+    }
     if (ev.out == 1) {
         cd f = imul(w);
         for (int b = 0; b < 4; b++)

@@ -79,7 +79,7 @@ EXPORTS = [
     "ysg_create", "ysg_model_upload", "ysg_model_tangent_upload", "ysg_model_tangents_upload", "ysg_event_spectra", "ysg_event_spectra_device",
     "ysg_event_traces", "ysg_trace_rows",
     "ysg_event_run", "ysg_event_prepare", "ysg_event_execute", "ysg_event_fetch", "ysg_get_stream",
-    "ysg_batch_run", "ysg_event_coef", "ysg_event_gradient", "ysg_legendre_table", "ysg_set_solver", "ysg_set_schedule", "ysg_last_schedule",
+    "ysg_batch_run", "ysg_event_coef", "ysg_event_gradient", "ysg_event_potential", "ysg_legendre_table", "ysg_set_solver", "ysg_set_schedule", "ysg_last_schedule",
     "ysg_last_timings", "ysg_last_work", "ysg_last_bytes", "ysg_last_launches", "ysg_fp64_peak", "ysg_status_string",
     "ysg_last_cuda_error", "ysg_destroy", "ysg_traces_noalloc",
     "ysh_norms_get", "ysh_read_params", "ysh_free_params", "ysh_read_model", "ysh_model_view",
@@ -126,6 +126,7 @@ def lib() -> C.CDLL:
                                 C.POINTER(_dp), C.POINTER(C.c_int)]
     L.ysg_event_coef.argtypes = [vp, C.POINTER(YsgEvent), _dp]
     L.ysg_event_gradient.argtypes = [vp, C.POINTER(YsgEvent), C.POINTER(YsgTime), _dp, _dp, _dp]
+    L.ysg_event_potential.argtypes = [vp, C.POINTER(YsgEvent), C.POINTER(YsgTime), _dp, C.POINTER(C.c_int)]
     L.ysg_legendre_table.argtypes = [vp, C.c_int, C.c_int, _dp, _dp, _dp, _dp]
     L.ysg_set_solver.argtypes = [vp, C.c_int]
     L.ysg_set_schedule.argtypes = [vp, C.c_int]
