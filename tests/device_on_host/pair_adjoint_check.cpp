@@ -50,6 +50,7 @@ void build(const ysg_model* m, Tables& T)
             k.v[p][0] = m->val[p][i];
             k.v[p][1] = m->cs[p][i];
         }
+        knot_derive(k);
     }
     T.sg.assign((size_t)n + 1, Seg{});
     std::memset(T.sg.data(), 0, T.sg.size() * sizeof(Seg));

@@ -1,6 +1,6 @@
 """The reverse sweep of single (omega, l) pairs (ysg_pair_adjoint.cuh, the
 code of k_solve_adjoint.cu) against the tangent-linear pair solve, on the
-CPU: tests/adjoint_host/pair_adjoint_check.cpp compiles the device solver
+CPU: tests/device_on_host/pair_adjoint_check.cpp compiles the device solver
 headers as host C++ (the looped-step form the sweep kernel uses) and
 compares <dL/d(knot arrays), d> from the reverse sweep with the directional
 derivative of the same pair solve in dual numbers, for radial, toroidal and
@@ -16,7 +16,7 @@ from pathlib import Path
 import pytest
 
 ROOT = Path(__file__).resolve().parent.parent
-SRC = Path(__file__).resolve().parent / "adjoint_host"
+SRC = Path(__file__).resolve().parent / "device_on_host"
 LIBDIR = ROOT / "yspec_b200" / "lib"
 CUDA_INC = Path("/usr/local/cuda/include")
 

@@ -127,6 +127,8 @@ struct ysg_handle {
     long long npairs = 0;            // pairs of the active slots
     int nev_items = 0;               // slots the items were built for
     DevBuf offs, keys0, keys1, vals0, vals1, sort_tmp;
+    DevBuf poff, pfx;                // per-frequency step table of the cost model (rows, table)
+    long long nrows = 0;             // frequencies of the active slots
     int sched = -1;                  // batched-solver schedule; -1 = autotuned
     int cur_sched = 0;               // schedule of the next solve launch
     std::map<Signature, int> tuned;  // autotuner choices
@@ -285,6 +287,13 @@ int upload_items(ysg_handle* h, std::vector<Item>& items, const std::vector<Even
     const long long np = off.back();
     CK(h->offs.ensure(off.size() * sizeof(long long)));
     CK(cudaMemcpyAsync(h->offs.p, off.data(), off.size() * sizeof(long long), cudaMemcpyHostToDevice, h->st));
+    // rows of the cost model's per-frequency step table
+    std::vector<long long> poff(evs.size() + 1, 0);
+    for (size_t e = 0; e < evs.size(); e++) poff[e + 1] = poff[e] + evs[e].nw;
+    CK(h->poff.ensure(poff.size() * sizeof(long long)));
+    CK(cudaMemcpyAsync(h->poff.p, poff.data(), poff.size() * sizeof(long long), cudaMemcpyHostToDevice, h->st));
+    CK(h->pfx.ensure(std::max<size_t>((size_t)poff.back() * ((size_t)h->hdr.nknot + 1) * sizeof(int), 16)));
+    h->nrows = poff.back();
     const size_t pb = (size_t)std::max<long long>(2 * np, 1) * sizeof(unsigned long long);
     CK(h->keys0.ensure(pb));
     CK(h->keys1.ensure(pb));
@@ -293,7 +302,7 @@ int upload_items(ysg_handle* h, std::vector<Item>& items, const std::vector<Even
     CK(h->sort_tmp.ensure(std::max<size_t>(pair_sort_tmp_bytes(np), 16)));
     CK(cudaStreamSynchronize(h->st));
     h->h2d += (double)(packed.size() * sizeof(int4) + evs.size() * sizeof(EventDev) +
-                       coefs.size() * sizeof(cd*) + off.size() * sizeof(long long));
+                       coefs.size() * sizeof(cd*) + (off.size() + poff.size()) * sizeof(long long));
     h->nitems = (int)packed.size();
     h->npairs = np;
     h->nev_items = (int)evs.size();
@@ -456,10 +465,11 @@ int enqueue_solve(ysg_handle* h, int nev)
         unsigned long long* keys[2] = {h->keys0.as<unsigned long long>(), h->keys1.as<unsigned long long>()};
         unsigned long long* vals[2] = {h->vals0.as<unsigned long long>(), h->vals1.as<unsigned long long>()};
         unsigned long long* sorted = nullptr;
-        h->launches += 2;            // k_pair_cost and the tangent solve (the radix sort is CUB's)
+        h->launches += 3;            // k_step_prefix, k_pair_cost and the tangent solve (the radix sort is CUB's)
         CK(launch_pair_schedule(h->kn.as<Knot>(), h->sg.as<Seg>(), h->hdr_dev.as<ModelHdr>(),
-                                h->evdev.as<EventDev>(), h->offs.as<long long>(), nev, h->npairs, sc, keys,
-                                vals, h->sort_tmp.p, h->sort_tmp.cap, &sorted, h->st));
+                                h->evdev.as<EventDev>(), h->offs.as<long long>(), nev, h->npairs,
+                                h->poff.as<long long>(), h->nrows, h->pfx.as<int>(), sc, keys, vals,
+                                h->sort_tmp.p, h->sort_tmp.cap, &sorted, h->st));
         CK(launch_solve_tangent(h->kn.as<Knot>(), h->sg.as<Seg>(), h->dkn.as<Knot>(), h->dsg.as<Seg>(),
                                 h->ndir, h->hdr_dev.as<ModelHdr>(), h->evdev.as<EventDev>(),
                                 h->coefptr.as<cd*>(), sorted, 2 * h->npairs,
@@ -474,11 +484,11 @@ int enqueue_solve(ysg_handle* h, int nev)
             unsigned long long* keys[2] = {h->keys0.as<unsigned long long>(), h->keys1.as<unsigned long long>()};
             unsigned long long* vals[2] = {h->vals0.as<unsigned long long>(), h->vals1.as<unsigned long long>()};
             unsigned long long* sorted = nullptr;
-            h->launches += 1;        // k_pair_cost (the radix sort is CUB's)
+            h->launches += 2;        // k_step_prefix and k_pair_cost (the radix sort is CUB's)
             CK(launch_pair_schedule(h->kn.as<Knot>(), h->sg.as<Seg>(), h->hdr_dev.as<ModelHdr>(),
                                     h->evdev.as<EventDev>(), h->offs.as<long long>(), h->nev_items,
-                                    h->npairs, sc, keys, vals, h->sort_tmp.p, h->sort_tmp.cap, &sorted,
-                                    h->st));
+                                    h->npairs, h->poff.as<long long>(), h->nrows, h->pfx.as<int>(), sc, keys,
+                                    vals, h->sort_tmp.p, h->sort_tmp.cap, &sorted, h->st));
             pairs = sorted;
         }
         const long long np = h->npairs;
@@ -819,6 +829,7 @@ void build_tables(int n, const double* r, const double* const* val, const double
             k.v[p][0] = val[p][i];
             k.v[p][1] = cs[p][i];
         }
+        knot_derive(k);
     }
     seg.assign((size_t)n + 1, Seg{});
     std::memset(seg.data(), 0, seg.size() * sizeof(Seg));
@@ -965,7 +976,7 @@ void ysg_destroy(ysg_handle* h)
     if (h->gexec) cudaGraphExecDestroy(h->gexec);
     for (Slot& s : h->slots) s.release();
     for (DevBuf* b : {&h->kn, &h->sg, &h->hdr_dev, &h->offs, &h->keys0, &h->keys1, &h->vals0,
-                      &h->vals1, &h->sort_tmp, &h->work, &h->status, &h->items, &h->counter,
+                      &h->vals1, &h->sort_tmp, &h->poff, &h->pfx, &h->work, &h->status, &h->items, &h->counter,
                       &h->evdev, &h->coefptr, &h->dkn, &h->dsg, &h->ukn, &h->usg, &h->abasis,
                       &h->about, &h->ascr, &h->acs0, &h->agout, &h->asbar, &h->acoefb, &h->agrad, &h->alogs})
         b->release();
@@ -1303,10 +1314,10 @@ int ysg_event_gradient(ysg_handle* h, const ysg_event* ev, const ysg_time* tm, c
     unsigned long long* keys[2] = {h->keys0.as<unsigned long long>(), h->keys1.as<unsigned long long>()};
     unsigned long long* vals[2] = {h->vals0.as<unsigned long long>(), h->vals1.as<unsigned long long>()};
     unsigned long long* sorted = nullptr;
-    h->launches += 2;                // k_pair_cost and the sweeps (the radix sort is CUB's)
+    h->launches += 3;                // k_step_prefix, k_pair_cost and the sweeps (the radix sort is CUB's)
     CK(launch_pair_schedule(h->kn.as<Knot>(), h->sg.as<Seg>(), h->hdr_dev.as<ModelHdr>(), h->evdev.as<EventDev>(),
-                            h->offs.as<long long>(), 1, h->npairs, sc, keys, vals, h->sort_tmp.p, h->sort_tmp.cap,
-                            &sorted, h->st));
+                            h->offs.as<long long>(), 1, h->npairs, h->poff.as<long long>(), h->nrows,
+                            h->pfx.as<int>(), sc, keys, vals, h->sort_tmp.p, h->sort_tmp.cap, &sorted, h->st));
     CK(cudaMemsetAsync(h->agrad.p, 0, ngrad * sizeof(double), h->st));
     CK(cudaMemsetAsync(h->status.p, 0, sizeof(int), h->st));
     // the l = 0 sweeps (few, long) beside the others on a side stream

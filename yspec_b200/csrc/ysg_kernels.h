@@ -56,8 +56,12 @@ struct StepCost {
     double base;                 // per-pair work outside the stepping
 };
 size_t pair_sort_tmp_bytes(long long npairs);
+// poff[e] is the first row of event e in the per-frequency step table pfx
+// (poff[nev] = nrows = sum of the events' nw; pfx holds nrows x (nknot + 1)
+// ints, filled here).
 cudaError_t launch_pair_schedule(const Knot* kn, const Seg* sg, const ModelHdr* mh,
                                  const EventDev* evs, const long long* off, int nev, long long npairs,
+                                 const long long* poff, long long nrows, int* pfx,
                                  const StepCost& sc, unsigned long long* keys[2],
                                  unsigned long long* vals[2], void* tmp, size_t tmp_bytes,
                                  unsigned long long** sorted, cudaStream_t st);

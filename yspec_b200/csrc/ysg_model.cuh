@@ -17,11 +17,25 @@ enum Param {
 };
 
 struct Knot {
-    double r, alpha, beta, pad0;
+    double r, alpha, beta;
+    double inv_a2;             // 1 / (alpha alpha), rounded as the start-level search forms it
     double v[NPARAM][2];       // value, spline second derivative
-    double pad1[2];
+    double inv_b2;             // 1 / (beta beta), the same
+    double r2;                 // r r, the same
 };
 static_assert(sizeof(Knot) == 256, "knot record must be 256 bytes");
+
+// The derived fields of a knot record: the start-level search
+// (module_start.f90:14-178) forms 1/v^2 and r^2 of every knot it visits for
+// every solve; each is one correctly rounded operation of the knot's own
+// values, formed here once per model instead.  A zero speed (a fluid's
+// beta) gives +inf, as the search's own quotient does.
+inline __host__ __device__ void knot_derive(Knot& k)
+{
+    k.inv_a2 = 1.0 / (k.alpha * k.alpha);
+    k.inv_b2 = 1.0 / (k.beta * k.beta);
+    k.r2 = k.r * k.r;
+}
 
 // Scalar part of the model.  Indices are 1-based as in the reference.
 struct ModelHdr {

@@ -175,6 +175,9 @@ struct Ctx {
     unsigned nst[NSYS];
     const Seg* sg;   // power-form spline segments (right-hand sides)
     cd* kb;          // shared-memory stage slab of this thread (smem form)
+#if YSG_COUNT_ONLY
+    const int* pfx;  // steps of the whole knot intervals below k, summed, at this omega (or null)
+#endif
 #if YSG_TANGENT
     const Knot* dkn; // derivative of the knot values along the model direction
     const Seg* dsg;  // derivative of the power-form segments
@@ -809,6 +812,26 @@ __device__ YSG_YINT_ATTR void yint(Ctx& cio, int i1, int i2, double r1, double r
     const bool up = r2 > r1;
     const Knot* kn = c.kn;
     const int di = up ? 1 : -1;
+#if YSG_COUNT_ONLY
+    if (c.pfx) {
+        // the two end intervals as below, the whole ones between them from
+        // the per-omega prefix sums of the same counts
+        auto part = [&](int i, double a, double b) -> unsigned {
+            if (a == b) return 0u;
+            const double nf = floor(fabs(b - a) / steps(c, i));
+            return (unsigned)(1 + (int)fmin(nf, 4194304.0));
+        };
+        unsigned cnt = 0u;
+        if (i1 == i2) cnt = part(i1, r1, r2);
+        else if (up && i1 < i2)
+            cnt = part(i1, r1, kn[i1 + 1].r) + (unsigned)(c.pfx[i2] - c.pfx[i1 + 1]) + part(i2, kn[i2].r, r2);
+        else if (!up && i1 > i2)
+            cnt = part(i1, r1, kn[i1].r) + (unsigned)(c.pfx[i1] - c.pfx[i2 + 1]) + part(i2, kn[i2 + 1].r, r2);
+        c.nst[Sys::CLS] += cnt;
+        c.il = i2;
+        return;
+    }
+#endif
     for (int i = i1; up ? (i <= i2) : (i >= i2); i += di) {
         double rr1, rr2;
         if (up) {
@@ -849,10 +872,12 @@ __device__ inline int start_level(const Ctx& c, int l, double w, int i1, int i2,
     const Knot* kn = c.kn;
     int isign = (i2 >= i1) ? 1 : -1;
     double pp = (double)(float)(l * (l + 1)) / __dmul_rn(w, w);
+    // q(i) = 1 / v_i^2 - pp / r_i^2, with 1 / v^2 and r^2 formed once per
+    // model (knot_derive) by the same rounded operations
+    auto q = [&](int i) { return (wt == 1 ? kn[i].inv_b2 : kn[i].inv_a2) - pp / kn[i].r2; };
     int j = i2;
     for (int i = i1; isign == 1 ? i <= i2 : i >= i2; i += isign) {
-        double v = wt == 1 ? kn[i].beta : kn[i].alpha;
-        double q1 = 1.0 / __dmul_rn(v, v) - pp / __dmul_rn(kn[i].r, kn[i].r);
+        double q1 = q(i);
         if (isign == 1) {
             if (q1 > 0.0) { j = max(i1, i - 1); break; }
         } else {
@@ -865,21 +890,20 @@ __device__ inline int start_level(const Ctx& c, int l, double w, int i1, int i2,
     int j1 = is;
     is = lo;
     double sum = 0.0;
+    // each knot's q enters two consecutive intervals: carried from one to the next
+    double q1 = q(j1);
     for (int i = j1; i >= lo + 1; i--) {
-        double v1 = wt == 1 ? kn[i].beta : kn[i].alpha;
-        double v2 = wt == 1 ? kn[i - 1].beta : kn[i - 1].alpha;
-        double q1 = 1.0 / __dmul_rn(v1, v1) - pp / __dmul_rn(kn[i].r, kn[i].r);
-        double q2 = 1.0 / __dmul_rn(v2, v2) - pp / __dmul_rn(kn[i - 1].r, kn[i - 1].r);
+        const double q2 = q(i - 1);
         if (q1 > 0.0 || q2 > 0.0) {
             sum = 0.0;
         } else {
-            q1 = sqrt(-q1);
-            q2 = sqrt(-q2);
-            double t = __dmul_rn(__dmul_rn(__dmul_rn(0.5, w), __dadd_rn(q1, q2)),
+            const double s1 = sqrt(-q1), s2 = sqrt(-q2);
+            double t = __dmul_rn(__dmul_rn(__dmul_rn(0.5, w), __dadd_rn(s1, s2)),
                                  __dsub_rn(kn[i].r, kn[i - 1].r));
             sum = __dadd_rn(sum, t);
         }
         if (sum > TOL_START) { is = i - 1; break; }
+        q1 = q2;
     }
     return is;
 }
