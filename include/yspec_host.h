@@ -95,6 +95,14 @@ void ysh_format_e15_6(double x, char field[16]);
  * as the reference writes them. */
 int ysh_run(const char *param_file, int device, int write_files, double **out, int *nout,
             int *nr);
+/* The potential traces of the event (ysg_event_potential): out, when
+ * non-NULL, receives a malloc'd (nout, 2, nr) array (time, potential in SI
+ * units of the output type); with write_files, pref_out.pot.1 ..
+ * pref_out.pot.nr, nout lines of two E15.6 fields each.  No reference
+ * counterpart: the reference does not write potential traces. */
+int ysh_run_potential(const char *param_file, int device, int write_files, double **out, int *nout,
+                      int *nr);
+int ysh_write_potential(const char *pref_out, const double *out, int nout, int nr);
 /* Several parameter files in one go: the events that name the same model
  * deck run as one ysg_batch_run (one batched solve launch, one CUDA graph),
  * and each event's files are written under its own output prefix exactly as

@@ -98,3 +98,24 @@ def test_cli_reports_bad_file(workdir):
                          text=True, timeout=600)
     assert res.returncode == 1
     assert "missing.in" in res.stderr and "parameter file" in res.stderr
+
+
+def test_cli_potential_files(workdir):
+    """`yspec --potential input.in` writes prefix.pot.1 .. prefix.pot.nr, two
+    E15.6 fields per line (time, potential), equal to the oracle's potential
+    traces to the text's precision."""
+    import yo
+
+    p = _params(5, out=1)
+    pf = p.write(workdir / "pot.in")
+    res = subprocess.run([str(YSPEC), "--potential", str(pf)], capture_output=True, text=True)
+    assert res.returncode == 0, res.stderr
+    want = yo.Problem(pf).potential_traces(nthreads=8)
+    for k in range(1, len(p.receivers) + 1):
+        lines = open(f"{p.pref_out}.pot.{k}").read().splitlines()
+        assert all(len(line) == 30 for line in lines)
+        got = np.array([[float(line[15 * c:15 * (c + 1)]) for c in range(2)] for line in lines])
+        assert got.shape == (want.shape[2], 2)
+        np.testing.assert_allclose(got[:, 0], want[k - 1, 0], rtol=1e-6, atol=0)
+        scale = np.abs(want[k - 1, 1]).max()
+        assert np.abs(got[:, 1] - want[k - 1, 1]).max() <= 1e-6 * scale

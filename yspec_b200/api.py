@@ -316,14 +316,18 @@ def fp64_peak_tflops(device: int = 0) -> float:
     return t.value
 
 
-def run_file(param_file: str | os.PathLike, device: int = 0, write_files: bool = False) -> np.ndarray:
-    """The whole `yspec input.in` program; returns traces (nr, 4, nout)."""
+def run_file(param_file: str | os.PathLike, device: int = 0, write_files: bool = False,
+             potential: bool = False) -> np.ndarray:
+    """The whole `yspec input.in` program; returns traces (nr, 4, nout).
+    With potential=True, `yspec --potential input.in`: the potential traces
+    (nr, 2, nout), files prefix.pot.k when write_files."""
     out = N._dp()
     nout, nr = C.c_int(), C.c_int()
-    N.check(N.lib().ysh_run(os.fsencode(param_file), device, int(write_files), C.byref(out),
-                            C.byref(nout), C.byref(nr)), "ysh_run")
+    fn = N.lib().ysh_run_potential if potential else N.lib().ysh_run
+    N.check(fn(os.fsencode(param_file), device, int(write_files), C.byref(out), C.byref(nout), C.byref(nr)),
+            "ysh_run_potential" if potential else "ysh_run")
     try:
-        arr = np.ctypeslib.as_array(out, shape=(nr.value, 4, nout.value)).copy()
+        arr = np.ctypeslib.as_array(out, shape=(nr.value, 2 if potential else 4, nout.value)).copy()
     finally:
         N.lib().ysh_free(out)
     return arr

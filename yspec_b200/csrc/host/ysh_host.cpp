@@ -657,20 +657,21 @@ void ysh_free_event(ysh_event* e)
     e->delta = e->azst = e->azep = nullptr;
 }
 
-// One receiver's file (yspec.f90:488-503): nout lines of four E15.6 fields.
-static bool write_one(const char* pref_out, const double* out, int nout, int k)
+// One receiver's file (yspec.f90:488-503): nout lines of ncol E15.6
+// fields, the file name the prefix, a dot and the receiver number.
+static bool write_one(const std::string& pref, const double* out, int nout, int ncol, int k)
 {
     // string_cat_int: digits counted with a single-precision log10
     char num[16];
     std::snprintf(num, sizeof num, "%10d", k);
     int j = (int)std::floor(std::log10((float)k));
-    std::string path = std::string(pref_out) + "." + std::string(num + 9 - j);
+    std::string path = pref + "." + std::string(num + 9 - j);
     std::string text;
-    text.reserve((size_t)nout * 61);
+    text.reserve((size_t)nout * (15 * (size_t)ncol + 1));
     char f[16];
-    const double* base = out + (size_t)nout * 4 * (size_t)(k - 1);
+    const double* base = out + (size_t)nout * ncol * (size_t)(k - 1);
     for (int i = 0; i < nout; i++) {
-        for (int c = 0; c < 4; c++) {
+        for (int c = 0; c < ncol; c++) {
             e15_6_fast(base[(size_t)i + (size_t)nout * c], f);
             text.append(f, 15);
         }
@@ -682,7 +683,8 @@ static bool write_one(const char* pref_out, const double* out, int nout, int k)
     return std::fclose(fp) == 0 && ok;
 }
 
-int ysh_write_traces(const char* pref_out, const double* out, int nout, int nr)
+// The files of nr receivers, (nout, ncol, nr) column-major, on threads.
+static int write_files_of(const std::string& pref, const double* out, int nout, int ncol, int nr)
 {
     // Receivers are independent files: format and write them on several
     // threads (the text conversion dominates at thousands of receivers).
@@ -693,7 +695,7 @@ int ysh_write_traces(const char* pref_out, const double* out, int nout, int nr)
     std::atomic<bool> ok{true};
     auto work = [&]() {
         for (int k = next++; k <= nr; k = next++)
-            if (!write_one(pref_out, out, nout, k)) ok = false;
+            if (!write_one(pref, out, nout, ncol, k)) ok = false;
     };
     if (nth == 1) {
         work();
@@ -703,6 +705,16 @@ int ysh_write_traces(const char* pref_out, const double* out, int nout, int nr)
         for (auto& t : pool) t.join();
     }
     return ok ? YSH_OK : YSH_ERR_IO;
+}
+
+int ysh_write_traces(const char* pref_out, const double* out, int nout, int nr)
+{
+    return write_files_of(pref_out, out, nout, 4, nr);
+}
+
+int ysh_write_potential(const char* pref_out, const double* out, int nout, int nr)
+{
+    return write_files_of(std::string(pref_out) + ".pot", out, nout, 2, nr);
 }
 
 // Wall-clock seconds, for the per-phase report of YSPEC_TIMING.
@@ -758,6 +770,55 @@ int ysh_run(const char* param_file, int device, int write_files, double** out, i
                      "time series %.2f), writer %.3f s (%d files x %d lines)\n",
                      t1 - t0, t2 - t1, ms[0], ms[1], ms[2], ms[3], t3 - t2, write_files ? p.nr : 0, no);
     }
+    if (!rc && out) {
+        *out = buf;
+        buf = nullptr;
+    }
+    if (nout) *nout = no;
+    if (nr) *nr = p.nr;
+    std::free(buf);
+    if (h) ysg_destroy(h);
+    ysh_free_event(&e);
+    ysh_free_model(m);
+    ysh_free_params(&p);
+    return rc;
+}
+
+int ysh_run_potential(const char* param_file, int device, int write_files, double** out, int* nout, int* nr)
+{
+    if (out) *out = nullptr;
+    ysh_params p;
+    int rc = ysh_read_params(param_file, &p);
+    if (rc) return rc;
+    ysh_model* m = nullptr;
+    rc = ysh_read_model(p.model_file, &m);
+    if (rc) {
+        ysh_free_params(&p);
+        return rc;
+    }
+    ysh_event e;
+    rc = ysh_event_setup(m, &p, &e);
+    ysg_handle* h = nullptr;
+    double* buf = nullptr;
+    int no = 0;
+    if (!rc) rc = ysg_create(&h, device);
+    if (!rc) rc = ysg_set_schedule(h, 2);
+    if (!rc) {
+        ysg_model view;
+        ysh_model_view(m, &view);
+        rc = ysg_model_upload(h, &view);
+    }
+    if (!rc) {
+        // the potential's normalisation for the output type (module_model.f90:489)
+        ysh_norms nm;
+        ysh_norms_get(&nm);
+        ysg_time tm = e.tm;
+        tm.amp_norm = nm.pot_norm / std::pow(nm.t_norm, (double)p.out);
+        int rows = ysg_trace_rows(&tm);
+        buf = (double*)std::malloc((size_t)rows * 2 * (size_t)std::max(p.nr, 1) * sizeof(double));
+        rc = ysg_event_potential(h, &e.ev, &tm, buf, &no);
+    }
+    if (!rc && write_files) rc = ysh_write_potential(p.pref_out, buf, no, p.nr);
     if (!rc && out) {
         *out = buf;
         buf = nullptr;

@@ -84,7 +84,8 @@ EXPORTS = [
     "ysg_last_cuda_error", "ysg_destroy", "ysg_traces_noalloc",
     "ysh_norms_get", "ysh_read_params", "ysh_free_params", "ysh_read_model", "ysh_model_view",
     "ysh_model_nknot", "ysh_model_array", "ysh_free_model", "ysh_event_setup", "ysh_free_event",
-    "ysh_write_traces", "ysh_format_e15_6", "ysh_run", "ysh_run_batch", "ysh_free", "ysh_status_string",
+    "ysh_write_traces", "ysh_format_e15_6", "ysh_run", "ysh_run_batch", "ysh_run_potential",
+    "ysh_write_potential", "ysh_free", "ysh_status_string",
 ]
 
 _lib = None
@@ -163,6 +164,8 @@ def lib() -> C.CDLL:
     L.ysh_format_e15_6.restype = None
     L.ysh_run.argtypes = [C.c_char_p, C.c_int, C.c_int, C.POINTER(_dp), C.POINTER(C.c_int),
                           C.POINTER(C.c_int)]
+    L.ysh_run_potential.argtypes = [C.c_char_p, C.c_int, C.c_int, C.POINTER(_dp), C.POINTER(C.c_int),
+                                    C.POINTER(C.c_int)]
     L.ysh_run_batch.argtypes = [C.c_int, C.POINTER(C.c_char_p), C.c_int, C.c_int, C.POINTER(C.c_int)]
     L.ysh_free.argtypes = [vp]
     L.ysh_free.restype = None
