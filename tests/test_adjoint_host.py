@@ -4,7 +4,8 @@ CPU: tests/device_on_host/pair_adjoint_check.cpp compiles the device solver
 headers as host C++ (the looped-step form the sweep kernel uses) and
 compares <dL/d(knot arrays), d> from the reverse sweep with the directional
 derivative of the same pair solve in dual numbers, for radial, toroidal and
-spheroidal pairs from l = 0 to lmax, to 1e-9 relative.  The GPU form of the
+spheroidal pairs from l = 0 to lmax, with a solid or a fluid inner core and
+with or without an ocean, to 1e-9 relative.  The GPU form of the
 same comparison, through the whole gradient pipeline, is
 tests/test_gpu_reverse.py."""
 from __future__ import annotations
@@ -25,6 +26,8 @@ CASES = [
     ("c4", {}),
     ("c4", {"out": 2, "cor": 1}),
     ("c4", {"out": 1, "depth_r": 50.0}),
+    ("c1", {"model_file": "model200_ocean.deck", "depth_r": 3.0, "ats": 1}),
+    ("c1", {"model_file": "model200_fic.deck", "depth_r": 3.0, "ats": 1, "out": 2, "cor": 1}),
 ]
 
 
@@ -49,6 +52,9 @@ def checker(tmp_path_factory):
 def test_pair_adjoint_matches_tangent(checker, tmp_path, cfg, over):
     from yspec_b200 import workloads as W
 
+    over = dict(over)
+    if "model_file" in over:
+        over["model_file"] = str(W.GOLDEN / over["model_file"])
     pf = W.config(cfg, seed=0, **over)[0].write(tmp_path / f"{cfg}.in")
     res = subprocess.run([str(checker), str(pf)], capture_output=True, text=True, timeout=600)
     assert res.returncode == 0, res.stdout[-3000:] + res.stderr[-2000:]

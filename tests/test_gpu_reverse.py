@@ -4,7 +4,7 @@ forward mode: for a random trace adjoint gout and random model directions d,
 <gradient(gout), d> must equal <gout, d traces / dd> to 1e-10 relative.
 Covered: the c1 and c4 configurations, displacement / velocity /
 acceleration with the potential and tilt corrections, receivers at the
-surface and at depth, and the whole ModelSynthetics backward pass against
+surface and at depth, an ocean and a fluid inner core, and the whole ModelSynthetics backward pass against
 its forward-mode counterpart and, at the c4 size, against central
 differences of the misfit along 20 directions."""
 from __future__ import annotations
@@ -19,6 +19,8 @@ CASES = [
     ("c4", {}),
     ("c4", {"out": 2, "cor": 1}),
     ("c4", {"out": 1, "depth_r": 50.0}),
+    ("c4", {"model_file": "model200_ocean.deck", "depth_r": 3.0}),
+    ("c1", {"model_file": "model200_fic.deck", "depth_r": 3.0, "ats": 1, "out": 2, "cor": 1}),
 ]
 
 
@@ -26,6 +28,9 @@ def _setup(tmp_path, cfg, over):
     from yspec_b200 import Engine, Event, Params, workloads as W
     from yspec_b200.model_chain import KnotModel
 
+    over = dict(over)
+    if "model_file" in over:
+        over["model_file"] = str(W.GOLDEN / over["model_file"])
     p = W.config(cfg, seed=0, **over)[0]
     pf = p.write(tmp_path / f"{cfg}.in")
     km = KnotModel(p.model_file)

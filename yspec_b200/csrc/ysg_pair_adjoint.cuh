@@ -1,17 +1,20 @@
 // ysg_pair_adjoint.cuh -- reverse sweep of one (omega, l) solve.
 //
-// The adjoint of pair_toroidal / pair_spheroidal (ysg_solvers.cuh) for the
-// self-gravitating solve with a solid inner core, no ocean and the receiver
-// at or above the source (tor_solver and sph_solver_g on their
-// receiver-above branch, module_solver.f90:25-142 and :640-823): given the
-// adjoints of the pair's uu / vv / ww coefficients, it adds the pair's
-// contribution to dL/dc[i][p][k] (the power-form spline segments, see
-// ysg_adjoint.cuh).  No reference counterpart: the reference has no
-// derivatives.
+// The adjoint of pair_radial / pair_toroidal / pair_spheroidal
+// (ysg_solvers.cuh) for the self-gravitating solve with the source in the
+// mantle and the receiver at or above it, with a solid or a fluid inner core
+// and with or without an ocean (rad_solver_wg, tor_solver and sph_solver_g /
+// sph_solver_fic on their receiver-above branch, module_solver.f90:25-142,
+// :446-561, :640-823, :1203-1382): given the adjoints of the pair's uu / vv /
+// ww coefficients, it adds the pair's contribution to dL/dc[i][p][k] (the
+// power-form spline segments, see ysg_adjoint.cuh).  No reference
+// counterpart: the reference has no derivatives.
 //
 // Pieces:
-//   - the Cash-Karp integrations: yint_adj (ysg_adjoint.cuh), each one
-//     replayed from its stored starting state when its adjoint is needed;
+//   - the Cash-Karp integrations: yint_log / yint_rev / yint_adj
+//     (ysg_adjoint.cuh), every step logged, the minor chain as it runs and
+//     the other legs replayed from their stored starts when their adjoint is
+//     needed;
 //   - the minor algebra (b_solid_start, sph_ysol, the secular determinant,
 //     the solid / fluid transforms) is linear in each argument and free of
 //     the model: its transposes are formed by applying the forward functions
@@ -293,8 +296,10 @@ __device__ inline bool sph_solver_g_adj(Ctx& c, const UnitDirs& u, double rr, do
     if (i1 == 1) rt = fmin(0.1 * c.dr, 0.1 * kn[2].r);
     if (i1 >= it) { i1 = it - 1; rt = kn[i1].r; }
     // the chain from the start level to the source; branch 0: solid inner
-    // core start, 1: fluid outer core start, 2: mantle start
-    const int branch = i1 <= mh->nic ? 0 : (i1 <= mh->noc ? 1 : 2);
+    // core start, 1: fluid start (outer core, or a fluid inner core), 2:
+    // mantle start
+    // a fluid inner core starts from the fluid minor there, as the outer core does
+    const int branch = (i1 <= mh->nic && !mh->fic) ? 0 : (i1 <= mh->noc ? 1 : 2);
     // The chain's legs (inner core, outer core, mantle to the source) are
     // logged as they run, one after the other in the chain log, and reversed
     // in the opposite order at the end; the other integrations are replayed
@@ -325,10 +330,23 @@ __device__ inline bool sph_solver_g_adj(Ctx& c, const UnitDirs& u, double rr, do
     cd ms3[14], ms2[14];
     for (int k = 0; k < 14; k++) ms3[k] = ms1[k];
     if (rr > rs) yint<MinorSolidG>(c, is, ir, rs, rr, ms3, &scale3);
-    cd e1[14];
+    // the solution from the surface down to the receiver: through an ocean
+    // first (a fluid minor from the surface to its floor, then the solid
+    // minor from the floor), else the solid minor from the surface
+    cd e1[14], mo[5], ms2s[14];
     unit(e1, 14, 0);
     for (int k = 0; k < 14; k++) ms2[k] = e1[k];
-    yint<MinorSolidG>(c, mh->nknot - 1, ir, kn[mh->nknot].r, rr, ms2, &scale2);
+    unit(mo, 5, 0);
+    if (mh->ocean) {
+        cd mf2[5];
+        for (int k = 0; k < 5; k++) mf2[k] = mo[k];
+        yint<MinorFluidG>(c, mh->nknot - 1, mh->nsl + 1, kn[mh->nknot].r, kn[mh->nsl + 1].r, mf2, &scale2);
+        f2s(mf2, ms2);
+    }
+    const int s2i1 = mh->ocean ? mh->nsl : mh->nknot - 1;
+    const double s2r1 = mh->ocean ? kn[mh->nsl].r : kn[mh->nknot].r;
+    for (int k = 0; k < 14; k++) ms2s[k] = ms2[k];
+    yint<MinorSolidG>(c, s2i1, ir, s2r1, rr, ms2, &scale2);
     const cd delta = delta_solid(ms3, ms2);
     const int jump[4] = {0, 1, 3, 4};
     cd ms1b[14], ms2b[14], ms3b[14];
@@ -359,7 +377,16 @@ __device__ inline bool sph_solver_g_adj(Ctx& c, const UnitDirs& u, double rr, do
         bstart_adj(s, bb, ms1b);
     }
     delta_adj(ms3, ms2, deltab, ms3b, ms2b);
-    if (!yint_adj<MinorSolidGT>(c, mh->nknot - 1, ir, kn[mh->nknot].r, rr, e1, ms2b, true, L, G)) return false;
+    if (!yint_adj<MinorSolidGT>(c, s2i1, ir, s2r1, rr, ms2s, ms2b, true, L, G)) return false;
+    if (mh->ocean) {
+        // back through the ocean: the fluid minor starts from a fixed vector
+        cd mf2b[5];
+        for (int k = 0; k < 5; k++) mf2b[k] = mk(0.0);
+        f2s_adj(ms2b, mf2b);
+        if (!yint_adj<MinorFluidGT>(c, mh->nknot - 1, mh->nsl + 1, kn[mh->nknot].r, kn[mh->nsl + 1].r, mo, mf2b,
+                                    true, L, G))
+            return false;
+    }
     if (rr > rs) {
         if (!yint_adj<MinorSolidGT>(c, is, ir, rs, rr, ms1, ms3b, true, L, G)) return false;
     }
@@ -572,7 +599,7 @@ __device__ inline bool pair_radial_adj(Ctx& c, const UnitDirs& u, const EventDev
 
 __device__ __forceinline__ bool pair_adj_supported(const ModelHdr* mh, const EventDev& ev)
 {
-    return ev.grav == 2 && mh->fic == 0 && mh->ocean == 0 && ev.rr >= ev.rs;
+    return ev.grav == 2 && ev.rr >= ev.rs && ev.is > mh->noc;
 }
 
 // wwb: adjoints of ww(1:5) of pair (l >= 2, j).  The adjoints of the
