@@ -142,9 +142,9 @@ int ysg_event_potential(ysg_handle *h, const ysg_event *ev, const ysg_time *tm, 
  * (module_model.f90:175-383).  As for the tangent-linear solver, start
  * levels, step counts and rescaling are those of the uploaded model (they
  * are piecewise constant in it) and alpha / beta are not differentiated.
- * Covers self-gravitation (grav 2) with the source in the mantle and the
- * receivers at or above it, solid or fluid inner core, with or without an
- * ocean; other events return
+ * Covers the source in the mantle and the receivers at or above it, for
+ * every gravity setting (self-gravitation, Cowling, none), a solid or a fluid
+ * inner core, with or without an ocean; other events return
  * YSG_ERR_UNSUPPORTED.  No reference counterpart: the reference has no
  * derivatives.  Stage times (ysg_last_timings): Legendre table, reverse
  * sweeps, l-sum transpose, time-stage transpose. */

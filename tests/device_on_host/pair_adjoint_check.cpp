@@ -246,7 +246,7 @@ int main(int argc, char** argv)
         c.ats = ev.ats;
         bool ok = true;
         if (l == 0) {
-            ok = pair_radial_adj(c, U, ev, j, w, L, GL, G);
+            ok = pair_radial_adj(c, U, ev, j, w, L, CL, GL, G);
         } else {
             if (l > 1) ok = pair_toroidal_adj(c, U, ev, l, j, w + 10, L, CL, G);
             ok = ok && pair_spheroidal_adj(c, U, ev, l, j, w, w + 5, L, CL, G);

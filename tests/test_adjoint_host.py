@@ -4,7 +4,8 @@ CPU: tests/device_on_host/pair_adjoint_check.cpp compiles the device solver
 headers as host C++ (the looped-step form the sweep kernel uses) and
 compares <dL/d(knot arrays), d> from the reverse sweep with the directional
 derivative of the same pair solve in dual numbers, for radial, toroidal and
-spheroidal pairs from l = 0 to lmax, with a solid or a fluid inner core and
+spheroidal pairs from l = 0 to lmax, with self-gravitation, in the Cowling
+approximation and without gravity, with a solid or a fluid inner core and
 with or without an ocean, to 1e-9 relative.  The GPU form of the
 same comparison, through the whole gradient pipeline, is
 tests/test_gpu_reverse.py."""
@@ -28,6 +29,10 @@ CASES = [
     ("c4", {"out": 1, "depth_r": 50.0}),
     ("c1", {"model_file": "model200_ocean.deck", "depth_r": 3.0, "ats": 1}),
     ("c1", {"model_file": "model200_fic.deck", "depth_r": 3.0, "ats": 1, "out": 2, "cor": 1}),
+    ("c1", {"grav": 1, "ats": 1}),
+    ("c1", {"grav": 0, "ats": 1, "out": 2, "cor": 1}),
+    ("c1", {"grav": 1, "model_file": "model200_ocean.deck", "depth_r": 3.0}),
+    ("c1", {"grav": 0, "model_file": "model200_fic.deck", "depth_r": 3.0, "ats": 1}),
 ]
 
 

@@ -4,7 +4,8 @@ forward mode: for a random trace adjoint gout and random model directions d,
 <gradient(gout), d> must equal <gout, d traces / dd> to 1e-10 relative.
 Covered: the c1 and c4 configurations, displacement / velocity /
 acceleration with the potential and tilt corrections, receivers at the
-surface and at depth, an ocean and a fluid inner core, and the whole ModelSynthetics backward pass against
+surface and at depth, an ocean and a fluid inner core, Cowling and no
+gravity, and the whole ModelSynthetics backward pass against
 its forward-mode counterpart and, at the c4 size, against central
 differences of the misfit along 20 directions."""
 from __future__ import annotations
@@ -21,6 +22,8 @@ CASES = [
     ("c4", {"out": 1, "depth_r": 50.0}),
     ("c4", {"model_file": "model200_ocean.deck", "depth_r": 3.0}),
     ("c1", {"model_file": "model200_fic.deck", "depth_r": 3.0, "ats": 1, "out": 2, "cor": 1}),
+    ("c4", {"grav": 1}),
+    ("c1", {"grav": 0, "ats": 1, "out": 2, "cor": 1}),
 ]
 
 
@@ -84,15 +87,15 @@ def test_model_synthetics_reverse_equals_forward_mode(tmp_path):
 
 
 def test_unsupported_path_falls_back(tmp_path):
-    """An event the reverse sweep does not cover (Cowling gravity) returns
-    status 8 from Engine.gradient, and ModelSynthetics falls back to the
-    tangent-linear sweep."""
+    """An event the reverse sweep does not cover (receivers below the source)
+    returns status 8 from Engine.gradient, and ModelSynthetics falls back to
+    the tangent-linear sweep."""
     import torch
 
     from yspec_b200 import adjoint
     from yspec_b200.native import YSG_ERR_UNSUPPORTED, YspecError
 
-    eng, ev, km = _setup(tmp_path, "c1", {"grav": 1})
+    eng, ev, km = _setup(tmp_path, "c1", {"depth_s": 20.0, "depth_r": 250.0})
     eng.upload(km.array_model())
     with pytest.raises(YspecError) as ei:
         eng.gradient(ev, np.zeros((ev.nr, 4, ev.nout())))

@@ -1191,8 +1191,8 @@ int ysg_event_gradient(ysg_handle* h, const ysg_event* ev, const ysg_time* tm, c
     int rc = check_event(h, ev);
     if (rc) return rc;
     if (!tm || !gval || !gcs || tm->nr != ev->nr || (ev->nr > 0 && !gout)) return YSG_ERR_ARG;
-    // self-gravitation, source in the mantle, receivers at or above it
-    if (ev->grav != 2 || ev->rr < ev->rs || ev->is <= h->hdr.noc) return YSG_ERR_UNSUPPORTED;
+    // the source in the mantle, receivers at or above it
+    if (ev->rr < ev->rs || ev->is <= h->hdr.noc) return YSG_ERR_UNSUPPORTED;
     const int L = ev->lmax - ev->lmin + 1;
     if (L >= (1 << 23) || L > 65535 || ev->nw >= (1 << 24) || ev->nr > 65535) return YSG_ERR_LIMIT;
     cudaSetDevice(h->device);
@@ -1218,7 +1218,7 @@ int ysg_event_gradient(ysg_handle* h, const ysg_event* ev, const ysg_time* tm, c
     if (nblk <= 0) return YSG_ERR_CUDA;
     size_t free_b = 0, total_b = 0;
     CK(cudaMemGetInfo(&free_b, &total_b));
-    const size_t per = adj_log_bytes(nmax, ncmax, 0), per_r = adj_log_bytes(nmax, 0, gmax);
+    const size_t per = adj_log_bytes(nmax, ncmax, 0), per_r = adj_log_bytes(nmax, ncmax, gmax);
     const size_t Tr = ev->lmin == 0 ? (size_t)(nw + ADJ_THREADS - 1) / ADJ_THREADS * ADJ_THREADS : 0;
     const size_t budget = (free_b + h->alogs.cap) / 4;
     // no more threads than entries
@@ -1276,7 +1276,7 @@ int ysg_event_gradient(ysg_handle* h, const ysg_event* ev, const ysg_time* tm, c
         return w;
     };
     const AdjLogs w = carve(T, ncmax, 0);
-    const AdjLogs wr = Tr ? carve(Tr, 0, gmax) : AdjLogs{};
+    const AdjLogs wr = Tr ? carve(Tr, ncmax, gmax) : AdjLogs{};
     UnitDirs u;
     for (int p = 0; p < NPARAM; p++) {
         u.kn[p] = h->ukn.as<Knot>() + (size_t)p * (n + 2);

@@ -29,7 +29,8 @@ SRC = HERE / "ysg_ode.cuh"
 OUT = HERE / "ysg_rhs_adjoint.cuh"
 
 # system struct -> (coefficient struct, state array name)
-SYSTEMS = ["TorSys", "RadSys", "MinorSolidG", "MinorFluidG", "BvecSolidG"]
+SYSTEMS = ["TorSys", "RadSys", "MinorSolidG", "MinorFluidG", "BvecSolidG",
+           "MinorSolidNC", "MinorFluidNC", "BvecSolidNC"]
 COEF_FIELDS = {
     "TorCoef": ["t", "k", "s"],
     "RadCoef": ["t", "k", "s"],

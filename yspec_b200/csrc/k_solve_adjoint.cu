@@ -181,8 +181,9 @@ __global__ void __launch_bounds__(ADJ_THREADS) k_solve_adjoint(
     G.flush();
 }
 
-// Reverse sweeps of the l = 0 pairs (rad_solver_wg with its grid), one
-// thread per frequency; thread tid owns step and grid logs tid.
+// Reverse sweeps of the l = 0 pairs (rad_solver_wg with its grid, or
+// rad_solver_ng without gravity), one thread per frequency; thread tid owns
+// scratch, chain and grid logs tid.
 __global__ void __launch_bounds__(ADJ_THREADS) k_radial_adjoint(
     const Knot* __restrict__ kn, const Seg* __restrict__ sg, const ModelHdr* __restrict__ mh,
     const EventDev* __restrict__ evp, UnitDirs u, const cd* __restrict__ coefb, AdjLogs w,
@@ -191,7 +192,7 @@ __global__ void __launch_bounds__(ADJ_THREADS) k_radial_adjoint(
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
     const EventDev ev = *evp;
     if (ev.lmin != 0) return;
-    StepLog L = step_log(w.s, tid, w.nthreads);
+    StepLog L = step_log(w.s, tid, w.nthreads), CL = step_log(w.c, tid, w.nthreads);
     GridLog GL{w.gy + tid, w.gr + tid, w.gi + tid, w.gmax, w.nthreads};
     SegGrad G;
     G.init(grad);
@@ -201,7 +202,7 @@ __global__ void __launch_bounds__(ADJ_THREADS) k_radial_adjoint(
         cd wb[NCOEF];
         for (int q = 0; q < NCOEF; q++) wb[q] = coefb[(size_t)q * ev.nw + (j - 1)];
         if (wb[2].x == 0.0 && wb[2].y == 0.0) continue;   // only uu(3) comes from the radial solve
-        if (!pair_radial_adj(c, u, ev, j, wb, L, GL, G)) atomicOr(status, 1);
+        if (!pair_radial_adj(c, u, ev, j, wb, L, CL, GL, G)) atomicOr(status, 1);
     }
     G.flush();
 }

@@ -269,6 +269,28 @@ struct BvecSolidGT {
     __device__ static SolidCoef amat(const Ctx& c, double r) { return solid_amat<2>(c, r); }
     __device__ static void amat_adj(const Ctx& c, double r, const SolidCoefBar& s, double* vb) { solid_amat_adj<2>(c, r, s, vb); }
 };
+// without self-gravitation: KIND 0 no gravity, 1 Cowling (module_int.f90:874-1110)
+template <int KIND>
+struct MinorSolidNCT {
+    using Sys = MinorSolidNC<KIND>;
+    using A = MinorSolidNCAdj;
+    __device__ static SolidCoef amat(const Ctx& c, double r) { return solid_amat<KIND>(c, r); }
+    __device__ static void amat_adj(const Ctx& c, double r, const SolidCoefBar& s, double* vb) { solid_amat_adj<KIND>(c, r, s, vb); }
+};
+template <int KIND>
+struct MinorFluidNCT {
+    using Sys = MinorFluidNC<KIND>;
+    using A = MinorFluidNCAdj;
+    __device__ static FluidCoef amat(const Ctx& c, double r) { return fluid_amat<KIND>(c, r); }
+    __device__ static void amat_adj(const Ctx& c, double r, const FluidCoefBar& s, double* vb) { fluid_amat_adj<KIND>(c, r, s, vb); }
+};
+template <int KIND>
+struct BvecSolidNCT {
+    using Sys = BvecSolidNC<KIND>;
+    using A = BvecSolidNCAdj;
+    __device__ static SolidCoef amat(const Ctx& c, double r) { return solid_amat<KIND>(c, r); }
+    __device__ static void amat_adj(const Ctx& c, double r, const SolidCoefBar& s, double* vb) { solid_amat_adj<KIND>(c, r, s, vb); }
+};
 
 // Cash-Karp tableau (module_int.f90:2039-2049)
 __device__ __forceinline__ double ck_b(int s, int t)

@@ -74,11 +74,13 @@ __device__ inline void tangent_ctx(const Ctx& c, const UnitDirs& u, int p, v_tan
 
 // vb_p += Re(sum_k yb_k dy_k / dv_p) for the start vectors at (i1, rt) and
 // the moments of the result go to G.  WHICH: 0 toroidal (2), 1 solid minor
-// (14), 2 fluid minor (5), 3 radial with gravity (2).
+// (14), 2 fluid minor (5), 3 radial with gravity (2), 4 solid minor without
+// self-gravitation (5), 5 fluid start without it (2), 6 radial without
+// gravity (2).
 template <int WHICH>
 __device__ __noinline__ void start_adj(const Ctx& c, const UnitDirs& u, int i1, double rt, const cd* yb, SegGrad& G)
 {
-    constexpr int N = (WHICH == 0 || WHICH == 3) ? 2 : (WHICH == 1 ? 14 : 5);
+    constexpr int N = WHICH == 1 ? 14 : ((WHICH == 2 || WHICH == 4) ? 5 : 2);
     double vb[NPARAM];
     for (int p = 0; p < NPARAM; p++) {
         v_tangent::Ctx t;
@@ -87,7 +89,10 @@ __device__ __noinline__ void start_adj(const Ctx& c, const UnitDirs& u, int i1, 
         if (WHICH == 0) v_tangent::tor_ystart(t, i1, rt, y);
         else if (WHICH == 1) v_tangent::sph_minor_solid_start(t, i1, rt, y);
         else if (WHICH == 2) v_tangent::sph_minor_fluid_start(t, i1, rt, y);
-        else v_tangent::rad_ystart<true>(t, i1, rt, y);
+        else if (WHICH == 3) v_tangent::rad_ystart<true>(t, i1, rt, y);
+        else if (WHICH == 4) v_tangent::sph_minor_solid_start_ng(t, i1, rt, y);
+        else if (WHICH == 5) v_tangent::sph_fluid_start_ng(t, i1, rt, y);
+        else v_tangent::rad_ystart<false>(t, i1, rt, y);
         double s = 0.0;
         for (int k = 0; k < N; k++) s += re(yb[k] * y[k].d);
         vb[p] = s;
@@ -210,6 +215,67 @@ __device__ inline void f2s_adj(const cd* msb, cd* mfb)
         f2s(e, m);
         cd t = mk(0.0);
         for (int k = 0; k < 14; k++) t = t + msb[k] * m[k];
+        mfb[j] = mfb[j] + t;
+    }
+}
+
+// The same for the minor algebra without self-gravitation (the _ngcow
+// forms: 5 solid minors, 2 fluid minors, 4-component b-vectors).
+__device__ inline void ysol_ngcow_adj(const cd* m, const cd* b, const cd* yb, cd* mb, cd* bb)
+{
+    cd e[5], y[4];
+    for (int j = 0; j < 5; j++) {
+        unit(e, 5, j);
+        sph_ysol_ngcow(e, b, y);
+        cd s = mk(0.0);
+        for (int k = 0; k < 4; k++) s = s + yb[k] * y[k];
+        mb[j] = mb[j] + s;
+    }
+    for (int j = 0; j < 4; j++) {
+        unit(e, 4, j);
+        sph_ysol_ngcow(m, e, y);
+        cd s = mk(0.0);
+        for (int k = 0; k < 4; k++) s = s + yb[k] * y[k];
+        bb[j] = bb[j] + s;
+    }
+}
+__device__ inline void delta_ngcow_adj(const cd* a, const cd* b, cd db, cd* ab, cd* bb)
+{
+    cd e[5];
+    for (int j = 0; j < 5; j++) {
+        unit(e, 5, j);
+        ab[j] = ab[j] + db * delta_solid_ngcow(e, b);
+        bb[j] = bb[j] + db * delta_solid_ngcow(a, e);
+    }
+}
+__device__ inline void bstart_ngcow_adj(const cd* s, const cd* bb, cd* mb)
+{
+    cd e[5], b[4];
+    for (int j = 0; j < 5; j++) {
+        unit(e, 5, j);
+        b_solid_start_ngcow(e, s, b);
+        cd t = mk(0.0);
+        for (int k = 0; k < 4; k++) t = t + bb[k] * b[k];
+        mb[j] = mb[j] + t;
+    }
+}
+__device__ inline void s2f_ngcow_adj(const cd* mfb, cd* msb)
+{
+    cd e[5], f[2];
+    for (int j = 0; j < 5; j++) {
+        unit(e, 5, j);
+        s2f_ngcow(e, f);
+        msb[j] = msb[j] + mfb[0] * f[0] + mfb[1] * f[1];
+    }
+}
+__device__ inline void f2s_ngcow_adj(const cd* msb, cd* mfb)
+{
+    cd e[2], m[5];
+    for (int j = 0; j < 2; j++) {
+        unit(e, 2, j);
+        f2s_ngcow(e, m);
+        cd t = mk(0.0);
+        for (int k = 0; k < 5; k++) t = t + msb[k] * m[k];
         mfb[j] = mfb[j] + t;
     }
 }
@@ -418,6 +484,122 @@ __device__ inline bool sph_solver_g_adj(Ctx& c, const UnitDirs& u, double rr, do
 // ---------------------------------------------------------------------------
 // The class of events the reverse sweep covers: self-gravitation, a solid
 // inner core, no ocean, the receiver at or above the source.
+// ---------------------------------------------------------------------------
+// sph_solver_nc without self-gravitation (KIND 0, module_solver.f90:827-1010)
+// and in the Cowling approximation (KIND 1, :1014-1195), with their fluid
+// inner core forms (:1386-1740), receiver at or above the source: the same
+// sweep as sph_solver_g_adj on the 5-minor / 2-minor / 4-vector systems.
+// ---------------------------------------------------------------------------
+template <int KIND>
+__device__ inline bool sph_solver_nc_adj(Ctx& c, const UnitDirs& u, double rr, double rs, int ir, int is,
+                                         const cd yb_out[4][4], cd yout[4][4], StepLog& L, StepLog& CL,
+                                         SegGrad& G)
+{
+    using SolidT = MinorSolidNCT<KIND>;
+    using FluidT = MinorFluidNCT<KIND>;
+    using BvecT = BvecSolidNCT<KIND>;
+    const ModelHdr* mh = c.mh;
+    const Knot* kn = c.kn;
+    int scale1 = 0, scale2 = 0, scale3 = 0;
+    const int it = is;
+    const double rtop = rs;
+    int i1 = sph_start_level(c, c.ll, c.omega.x, it);
+    double rt = kn[i1].r;
+    if (i1 == 1) rt = fmin(0.1 * c.dr, 0.1 * kn[2].r);
+    if (i1 >= it) { i1 = it - 1; rt = kn[i1].r; }
+    // branch 0: solid inner core start, 1: fluid start (outer core, or a
+    // fluid inner core), 2: mantle start; the chain's legs in the chain log
+    const int branch = (i1 <= mh->nic && !mh->fic) ? 0 : (i1 <= mh->noc ? 1 : 2);
+    cd ms1[5], mf[2];
+    int nic_s = 0, noc_s = 0, nm_s = 0;
+    if (branch == 0) {
+        sph_minor_solid_start_ng(c, i1, rt, ms1);
+        if (!yint_log<SolidT>(c, i1, mh->nic, rt, kn[mh->nic].r, ms1, &scale1, CL, 0, &nic_s)) return false;
+        s2f_ngcow(ms1, mf);
+        if (!yint_log<FluidT>(c, mh->nic + 1, mh->noc, kn[mh->nic].r, kn[mh->noc].r, mf, &scale1, CL, nic_s, &noc_s))
+            return false;
+        f2s_ngcow(mf, ms1);
+    } else if (branch == 1) {
+        sph_fluid_start_ng(c, i1, rt, mf);
+        if (!yint_log<FluidT>(c, i1, mh->noc, rt, kn[mh->noc].r, mf, &scale1, CL, 0, &noc_s)) return false;
+        f2s_ngcow(mf, ms1);
+    } else {
+        sph_minor_solid_start_ng(c, i1, rt, ms1);
+    }
+    const int mi1 = branch == 2 ? i1 : mh->noc + 1;
+    const double mr1 = branch == 2 ? rt : kn[mh->noc + 1].r;
+    const int moff = nic_s + noc_s;
+    if (!yint_log<SolidT>(c, mi1, it, mr1, rtop, ms1, &scale1, CL, moff, &nm_s)) return false;
+    cd ms3[5], ms2[5], ms2s[5], mo[2];
+    for (int k = 0; k < 5; k++) ms3[k] = ms1[k];
+    if (rr > rs) yint<MinorSolidNC<KIND>>(c, is, ir, rs, rr, ms3, &scale3);
+    // from the surface down to the receiver, through an ocean first
+    unit(ms2, 5, 0);
+    unit(mo, 2, 0);
+    if (mh->ocean) {
+        cd mf2[2] = {mo[0], mo[1]};
+        yint<MinorFluidNC<KIND>>(c, mh->nknot - 1, mh->nsl + 1, kn[mh->nknot].r, kn[mh->nsl + 1].r, mf2, &scale2);
+        f2s_ngcow(mf2, ms2);
+    }
+    const int s2i1 = mh->ocean ? mh->nsl : mh->nknot;
+    const double s2r1 = mh->ocean ? kn[mh->nsl].r : kn[mh->nknot].r;
+    for (int k = 0; k < 5; k++) ms2s[k] = ms2[k];
+    yint<MinorSolidNC<KIND>>(c, s2i1, ir, s2r1, rr, ms2, &scale2);
+    const cd delta = delta_solid_ngcow(ms3, ms2);
+    cd ms1b[5], ms2b[5], ms3b[5];
+    for (int k = 0; k < 5; k++) ms1b[k] = ms2b[k] = ms3b[k] = mk(0.0);
+    cd deltab = mk(0.0);
+    for (int i = 0; i < 4; i++) {
+        cd s[4], b[4], ys[4];
+        unit(s, 4, i);
+        b_solid_start_ngcow(ms1, s, b);
+        int scale4 = 0, nb = 0;
+        if (!yint_log<BvecT>(c, is, ir, rs, rr, b, &scale4, L, 0, &nb)) return false;
+        sph_ysol_ngcow(ms2, b, ys);
+        // yout[k][i] = (ys[k] / delta) huge^(scale3 - scale4)
+        const double F = huge_pow(scale3 - scale4);
+        cd ysb[4];
+        for (int k = 0; k < 4; k++) {
+            yout[k][i] = F * (ys[k] / delta);
+            const cd yk = F * yb_out[k][i];
+            ysb[k] = yk / delta;
+            deltab = deltab - yk * (ys[k] / (delta * delta));
+        }
+        cd bb[4] = {mk(0.0), mk(0.0), mk(0.0), mk(0.0)};
+        ysol_ngcow_adj(ms2, b, ysb, ms2b, bb);
+        yint_rev<BvecT>(c, L, 0, nb, bb, G);
+        bstart_ngcow_adj(s, bb, ms1b);
+    }
+    delta_ngcow_adj(ms3, ms2, deltab, ms3b, ms2b);
+    if (!yint_adj<SolidT>(c, s2i1, ir, s2r1, rr, ms2s, ms2b, true, L, G)) return false;
+    if (mh->ocean) {
+        cd mf2b[2] = {mk(0.0), mk(0.0)};
+        f2s_ngcow_adj(ms2b, mf2b);
+        if (!yint_adj<FluidT>(c, mh->nknot - 1, mh->nsl + 1, kn[mh->nknot].r, kn[mh->nsl + 1].r, mo, mf2b, true, L,
+                              G))
+            return false;
+    }
+    if (rr > rs && !yint_adj<SolidT>(c, is, ir, rs, rr, ms1, ms3b, true, L, G)) return false;
+    for (int k = 0; k < 5; k++) ms1b[k] = ms1b[k] + ms3b[k];
+    yint_rev<SolidT>(c, CL, moff, nm_s, ms1b, G);
+    if (branch == 2) {
+        start_adj<4>(c, u, i1, rt, ms1b, G);
+        return true;
+    }
+    cd mfb[2] = {mk(0.0), mk(0.0)};
+    f2s_ngcow_adj(ms1b, mfb);
+    yint_rev<FluidT>(c, CL, nic_s, noc_s, mfb, G);
+    if (branch == 1) {
+        start_adj<5>(c, u, i1, rt, mfb, G);
+        return true;
+    }
+    cd msb[5] = {mk(0.0), mk(0.0), mk(0.0), mk(0.0), mk(0.0)};
+    s2f_ngcow_adj(mfb, msb);
+    yint_rev<SolidT>(c, CL, 0, nic_s, msb, G);
+    start_adj<4>(c, u, i1, rt, msb, G);
+    return true;
+}
+
 // Grid of the l = 0 gravity solve (rad_solver_wg): per grid point k its
 // radius, interval and the upward and downward solutions there.  Entry e
 // of an array sits at e * st, as in StepLog.
@@ -575,10 +757,68 @@ __device__ inline bool rad_solver_wg_adj(Ctx& c, const UnitDirs& u, double rr, d
     return true;
 }
 
+// rad_solver_ng (ysg_solvers.cuh, module_solver.f90:335-441; the radial
+// system in its gravity form, rad_derivs_ng), receiver at or above the
+// source: the forward pass (its upward leg from the centre to the source in
+// the chain log), its output in yout, then the reverse sweep from yb.
+__device__ inline bool rad_solver_ng_adj(Ctx& c, const UnitDirs& u, double rr, double rs, int ir, int is,
+                                         const cd yb[2][2], cd yout[2][2], StepLog& L, StepLog& CL, SegGrad& G)
+{
+    const ModelHdr* mh = c.mh;
+    const Knot* kn = c.kn;
+    int scale1 = 0, scale2 = 0, scale3 = 0, n1 = 0;
+    const double rt = fmin(0.1 * c.dr, 0.1 * kn[2].r);
+    cd y1[2], y2[2] = {mk(1.0), mk(0.0)}, y3[2], y2s[2];
+    rad_ystart<false>(c, 1, rt, y1);
+    if (!yint_log<RadT>(c, 1, is, rt, rs, y1, &scale1, CL, 0, &n1)) return false;
+    const bool leg2 = rr != kn[mh->nknot].r, leg3 = rs != rr;
+    if (leg2) yint<RadSys>(c, mh->nknot - 1, ir, kn[mh->nknot].r, rr, y2, &scale2);
+    y2s[0] = y2[0];
+    y2s[1] = y2[1];
+    y3[0] = y2[0];
+    y3[1] = y2[1];
+    if (leg3) yint<RadSys>(c, ir, is, rr, rs, y3, &scale3);
+    const cd D = y3[1] * y1[0] - y3[0] * y1[1];
+    const bool degenerate = cabs(D) < 1.0e-100;
+    const cd delta = degenerate ? mk(0.0) : 1.0 / D;
+    const cd bv[2] = {y1[1], -y1[0]};
+    const cd dy[2] = {delta * y2[0], delta * y2[1]};
+    const double F = scale3 != 0 ? huge_pow(scale3) : 1.0;
+    for (int a = 0; a < 2; a++)
+        for (int b = 0; b < 2; b++) yout[a][b] = F * (-(dy[a] * bv[b]));
+    // reverse: yout[a][b] = -F delta y2[a] bv[b]
+    cd dyb[2] = {mk(0.0), mk(0.0)}, bvb[2] = {mk(0.0), mk(0.0)};
+    for (int a = 0; a < 2; a++)
+        for (int b = 0; b < 2; b++) {
+            const cd g = F * yb[a][b];
+            dyb[a] = dyb[a] - g * bv[b];
+            bvb[b] = bvb[b] - g * dy[a];
+        }
+    cd y1b[2] = {-bvb[1], bvb[0]};
+    const cd deltab = dyb[0] * y2[0] + dyb[1] * y2[1];
+    cd y2b[2] = {delta * dyb[0], delta * dyb[1]};
+    cd y3b[2] = {mk(0.0), mk(0.0)};
+    if (!degenerate) {
+        const cd Db = -(deltab * (delta * delta));
+        y3b[0] = -(Db * y1[1]);
+        y3b[1] = Db * y1[0];
+        y1b[0] = y1b[0] + Db * y3[1];
+        y1b[1] = y1b[1] - Db * y3[0];
+    }
+    if (leg3 && !yint_adj<RadT>(c, ir, is, rr, rs, y2s, y3b, true, L, G)) return false;
+    y2b[0] = y2b[0] + y3b[0];
+    y2b[1] = y2b[1] + y3b[1];
+    const cd e[2] = {mk(1.0), mk(0.0)};
+    if (leg2 && !yint_adj<RadT>(c, mh->nknot - 1, ir, kn[mh->nknot].r, rr, e, y2b, true, L, G)) return false;
+    yint_rev<RadT>(c, CL, 0, n1, y1b, G);
+    start_adj<6>(c, u, 1, rt, y1b, G);
+    return true;
+}
+
 // coefb: adjoints of the 15 coefficients of pair (l = 0, j); only uu(3)
 // is formed by the radial solve (yspec.f90:263-293).
 __device__ inline bool pair_radial_adj(Ctx& c, const UnitDirs& u, const EventDev& ev, int j, const cd* coefb,
-                                       StepLog& L, GridLog& GL, SegGrad& G)
+                                       StepLog& L, StepLog& CL, GridLog& GL, SegGrad& G)
 {
     const cd w = omega_of(ev, j);
     set_l(c, 0);
@@ -591,7 +831,11 @@ __device__ inline bool pair_radial_adj(Ctx& c, const UnitDirs& u, const EventDev
     if (ev.out != 0) g = out_factor(ev.out, w) * g;
     g = g / ev.rr;
     const cd yb[2][2] = {{g * sr0[0], g * sr0[1]}, {mk(0.0), mk(0.0)}};
-    if (!rad_solver_wg_adj(c, u, ev.rr, ev.rs, yb, yrad, L, GL, G)) return false;
+    if (ev.grav == 0) {
+        if (!rad_solver_ng_adj(c, u, ev.rr, ev.rs, ev.ir, ev.is, yb, yrad, L, CL, G)) return false;
+    } else if (!rad_solver_wg_adj(c, u, ev.rr, ev.rs, yb, yrad, L, GL, G)) {
+        return false;
+    }
     const cd s0b[2] = {g * yrad[0][0], g * yrad[0][1]};
     source_rad_adj(c, u, ev.is, ev.rs, ev.mm, s0b, G);
     return true;
@@ -599,7 +843,7 @@ __device__ inline bool pair_radial_adj(Ctx& c, const UnitDirs& u, const EventDev
 
 __device__ __forceinline__ bool pair_adj_supported(const ModelHdr* mh, const EventDev& ev)
 {
-    return ev.grav == 2 && ev.rr >= ev.rs && ev.is > mh->noc;
+    return ev.rr >= ev.rs && ev.is > mh->noc;
 }
 
 // wwb: adjoints of ww(1:5) of pair (l >= 2, j).  The adjoints of the
@@ -692,7 +936,26 @@ __device__ inline bool pair_spheroidal_adj(Ctx& c, const UnitDirs& u, const Even
             }
         }
     }
-    if (!sph_solver_g_adj(c, u, ev.rr, ev.rs, ev.ir, ev.is, yb, ysph, L, CL, G)) return false;
+    if (ev.grav == 2) {
+        if (!sph_solver_g_adj(c, u, ev.rr, ev.rs, ev.ir, ev.is, yb, ysph, L, CL, G)) return false;
+    } else {
+        // the 4-vector solution (U, V, R, S): its U and V rows are the
+        // outputs; the potential is zero (yspec.f90:367-374)
+        cd ybn[4][4], yng[4][4];
+        for (int b = 0; b < 4; b++) {
+            ybn[0][b] = yb[0][b];
+            ybn[1][b] = yb[1][b];
+            ybn[2][b] = ybn[3][b] = mk(0.0);
+        }
+        const bool ok = ev.grav == 1 ? sph_solver_nc_adj<1>(c, u, ev.rr, ev.rs, ev.ir, ev.is, ybn, yng, L, CL, G)
+                                     : sph_solver_nc_adj<0>(c, u, ev.rr, ev.rs, ev.ir, ev.is, ybn, yng, L, CL, G);
+        if (!ok) return false;
+        for (int b = 0; b < 4; b++) {
+            ysph[0][b] = yng[0][b];
+            ysph[1][b] = yng[1][b];
+            ysph[2][b] = mk(0.0);
+        }
+    }
     // grav(ir), the c0 coefficient of segment ir, through the correction
     if (ev.out == 2 && ev.cor != 0) {
         double gb = 0.0;

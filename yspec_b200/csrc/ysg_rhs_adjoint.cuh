@@ -184,5 +184,82 @@ struct BvecSolidGAdj {
     }
 };
 
+// MinorSolidNC: 5 components, coefficients SolidCoef
+struct MinorSolidNCAdj {
+    static constexpr int N = 5;
+    using Coef = SolidCoef;
+    using Bar = SolidCoefBar;
+    // g = A^T k
+    __device__ static __forceinline__ void tr(const SolidCoef& a, const cd* k, cd* g)
+    {
+        g[0] = a.t11 * k[0] + a.t22 * k[0] + a.s12 * k[1] + a.s22 * k[2] + (-1.0 * a.s11) * k[3];
+        g[1] = (-2.0 * a.t12) * k[2] + (2.0 * a.t21) * k[3] + (-2.0 * a.s12) * k[4];
+        g[2] = a.k22 * k[0] + (-1.0 * a.t21) * k[1] + a.t11 * k[2] + (-1.0 * a.t22) * k[2] + a.s11 * k[4];
+        g[3] = (-1.0 * a.k11) * k[0] + a.t12 * k[1] + (-1.0 * a.t11) * k[3] + a.t22 * k[3] + (-1.0 * a.s22) * k[4];
+        g[4] = a.k11 * k[2] + (-1.0 * a.k22) * k[3] + (-1.0 * a.t11) * k[4] + (-1.0 * a.t22) * k[4];
+    }
+    // s.e += k . (dA/da_e) y
+    __device__ static __forceinline__ void cgrad(const cd* k, const cd* y, SolidCoefBar& s)
+    {
+        s.t11 += k[0] * y[0] + k[2] * y[2] + -1.0 * (k[3] * y[3]) + -1.0 * (k[4] * y[4]);
+        s.t12 += k[1] * y[3] + -2.0 * (k[2] * y[1]);
+        s.k11 += -1.0 * (k[0] * y[3]) + k[2] * y[4];
+        s.k22 += k[0] * y[2] + -1.0 * (k[3] * y[4]);
+        s.s11 += -1.0 * (k[3] * y[0]) + k[4] * y[2];
+        s.s12 += k[1] * y[0] + -2.0 * (k[4] * y[1]);
+        s.s22 += k[2] * y[0] + -1.0 * (k[4] * y[3]);
+        s.t21 += -1.0 * (k[1] * y[2]) + 2.0 * (k[3] * y[1]);
+        s.t22 += k[0] * y[0] + -1.0 * (k[2] * y[2]) + k[3] * y[3] + -1.0 * (k[4] * y[4]);
+    }
+};
+
+// MinorFluidNC: 2 components, coefficients FluidCoef
+struct MinorFluidNCAdj {
+    static constexpr int N = 2;
+    using Coef = FluidCoef;
+    using Bar = FluidCoefBar;
+    // g = A^T k
+    __device__ static __forceinline__ void tr(const FluidCoef& a, const cd* k, cd* g)
+    {
+        g[0] = a.t11 * k[0] + a.s11 * k[1];
+        g[1] = a.k11 * k[0] + (-1.0 * a.t11) * k[1];
+    }
+    // s.e += k . (dA/da_e) y
+    __device__ static __forceinline__ void cgrad(const cd* k, const cd* y, FluidCoefBar& s)
+    {
+        s.t11 += k[0] * y[0] + -1.0 * (k[1] * y[1]);
+        s.k11 += k[0] * y[1];
+        s.s11 += k[1] * y[0];
+    }
+};
+
+// BvecSolidNC: 4 components, coefficients SolidCoef
+struct BvecSolidNCAdj {
+    static constexpr int N = 4;
+    using Coef = SolidCoef;
+    using Bar = SolidCoefBar;
+    // g = A^T k
+    __device__ static __forceinline__ void tr(const SolidCoef& a, const cd* k, cd* g)
+    {
+        g[0] = (-1.0 * a.t11) * k[0] + (-1.0 * a.t12) * k[1] + (-1.0 * a.k11) * k[2];
+        g[1] = (-1.0 * a.t21) * k[0] + (-1.0 * a.t22) * k[1] + (-1.0 * a.k22) * k[3];
+        g[2] = (-1.0 * a.s11) * k[0] + (-1.0 * a.s12) * k[1] + a.t11 * k[2] + a.t21 * k[3];
+        g[3] = (-1.0 * a.s12) * k[0] + (-1.0 * a.s22) * k[1] + a.t12 * k[2] + a.t22 * k[3];
+    }
+    // s.e += k . (dA/da_e) y
+    __device__ static __forceinline__ void cgrad(const cd* k, const cd* y, SolidCoefBar& s)
+    {
+        s.t11 += -1.0 * (k[0] * y[0]) + k[2] * y[2];
+        s.t12 += -1.0 * (k[1] * y[0]) + k[2] * y[3];
+        s.k11 += -1.0 * (k[2] * y[0]);
+        s.k22 += -1.0 * (k[3] * y[1]);
+        s.s11 += -1.0 * (k[0] * y[2]);
+        s.s12 += -1.0 * (k[0] * y[3]) + -1.0 * (k[1] * y[2]);
+        s.s22 += -1.0 * (k[1] * y[3]);
+        s.t21 += -1.0 * (k[0] * y[1]) + k[3] * y[2];
+        s.t22 += -1.0 * (k[1] * y[1]) + k[3] * y[3];
+    }
+};
+
 }  // namespace YSG_VARIANT
 }  // namespace ysg
