@@ -142,10 +142,11 @@ int ysg_event_potential(ysg_handle *h, const ysg_event *ev, const ysg_time *tm, 
  * (module_model.f90:175-383).  As for the tangent-linear solver, start
  * levels, step counts and rescaling are those of the uploaded model (they
  * are piecewise constant in it) and alpha / beta are not differentiated.
- * Covers the source in the mantle and the receivers at or above it, for
- * every gravity setting (self-gravitation, Cowling, none), a solid or a fluid
- * inner core, with or without an ocean; other events return
- * YSG_ERR_UNSUPPORTED.  No reference counterpart: the reference has no
+ * Covers a source and receivers in the solid above the outer core, the
+ * receivers above or below the source, for every gravity setting
+ * (self-gravitation, Cowling, none), a solid or a fluid inner core, with or
+ * without an ocean; events with the source or the receivers in the core
+ * return YSG_ERR_UNSUPPORTED.  No reference counterpart: the reference has no
  * derivatives.  Stage times (ysg_last_timings): Legendre table, reverse
  * sweeps, l-sum transpose, time-stage transpose. */
 int ysg_event_gradient(ysg_handle *h, const ysg_event *ev, const ysg_time *tm, const double *gout,

@@ -6,7 +6,8 @@ compares <dL/d(knot arrays), d> from the reverse sweep with the directional
 derivative of the same pair solve in dual numbers, for radial, toroidal and
 spheroidal pairs from l = 0 to lmax, with self-gravitation, in the Cowling
 approximation and without gravity, with a solid or a fluid inner core and
-with or without an ocean, to 1e-9 relative.  The GPU form of the
+with or without an ocean, receivers above and below the source, to 1e-9
+relative.  The GPU form of the
 same comparison, through the whole gradient pipeline, is
 tests/test_gpu_reverse.py."""
 from __future__ import annotations
@@ -33,6 +34,14 @@ CASES = [
     ("c1", {"grav": 0, "ats": 1, "out": 2, "cor": 1}),
     ("c1", {"grav": 1, "model_file": "model200_ocean.deck", "depth_r": 3.0}),
     ("c1", {"grav": 0, "model_file": "model200_fic.deck", "depth_r": 3.0, "ats": 1}),
+    # receivers below the source
+    ("c4", {"depth_s": 20.0, "depth_r": 250.0}),
+    ("c1", {"grav": 1, "depth_s": 20.0, "depth_r": 250.0, "ats": 1}),
+    ("c1", {"grav": 0, "depth_s": 20.0, "depth_r": 250.0, "ats": 1, "out": 2, "cor": 1}),
+    ("c1", {"model_file": "model200_ocean.deck", "depth_s": 3.0, "depth_r": 250.0, "ats": 1}),
+    ("c1", {"model_file": "model200_fic.deck", "depth_s": 3.0, "depth_r": 250.0, "ats": 1, "out": 2, "cor": 1}),
+    ("c1", {"grav": 1, "model_file": "model200_ocean.deck", "depth_s": 3.0, "depth_r": 250.0}),
+    ("c1", {"grav": 0, "model_file": "model200_fic.deck", "depth_s": 3.0, "depth_r": 250.0, "ats": 1}),
 ]
 
 

@@ -4,7 +4,7 @@ forward mode: for a random trace adjoint gout and random model directions d,
 <gradient(gout), d> must equal <gout, d traces / dd> to 1e-10 relative.
 Covered: the c1 and c4 configurations, displacement / velocity /
 acceleration with the potential and tilt corrections, receivers at the
-surface and at depth, an ocean and a fluid inner core, Cowling and no
+surface, at depth and below the source, an ocean and a fluid inner core, Cowling and no
 gravity, and the whole ModelSynthetics backward pass against
 its forward-mode counterpart and, at the c4 size, against central
 differences of the misfit along 20 directions."""
@@ -24,6 +24,12 @@ CASES = [
     ("c1", {"model_file": "model200_fic.deck", "depth_r": 3.0, "ats": 1, "out": 2, "cor": 1}),
     ("c4", {"grav": 1}),
     ("c1", {"grav": 0, "ats": 1, "out": 2, "cor": 1}),
+    # receivers below the source
+    ("c4", {"depth_s": 20.0, "depth_r": 250.0}),
+    ("c1", {"grav": 1, "depth_s": 20.0, "depth_r": 250.0, "ats": 1, "out": 1}),
+    ("c1", {"grav": 0, "depth_s": 20.0, "depth_r": 250.0, "ats": 1, "out": 2, "cor": 1}),
+    ("c1", {"model_file": "model200_ocean.deck", "depth_s": 3.0, "depth_r": 250.0, "ats": 1}),
+    ("c1", {"model_file": "model200_fic.deck", "depth_s": 3.0, "depth_r": 250.0, "ats": 1, "out": 2, "cor": 1}),
 ]
 
 
@@ -86,20 +92,29 @@ def test_model_synthetics_reverse_equals_forward_mode(tmp_path):
     assert np.max(np.abs(a - t)) <= 1e-9 * np.max(np.abs(t))
 
 
-def test_unsupported_path_falls_back(tmp_path):
-    """An event the reverse sweep does not cover (receivers below the source)
-    returns status 8 from Engine.gradient, and ModelSynthetics falls back to
-    the tangent-linear sweep."""
+def test_unsupported_path_falls_back(tmp_path, monkeypatch):
+    """An event the reverse sweep does not cover (a source in the outer core)
+    returns status 8 from Engine.gradient before any device work, and
+    ModelSynthetics falls back to the tangent-linear sweep when the gradient
+    reports status 8."""
     import torch
 
     from yspec_b200 import adjoint
     from yspec_b200.native import YSG_ERR_UNSUPPORTED, YspecError
 
-    eng, ev, km = _setup(tmp_path, "c1", {"depth_s": 20.0, "depth_r": 250.0})
+    eng, ev, km = _setup(tmp_path, "c1", {"depth_s": 3000.0})
+    assert ev.raw.ev.is_ <= km.view0.noc
     eng.upload(km.array_model())
     with pytest.raises(YspecError) as ei:
         eng.gradient(ev, np.zeros((ev.nr, 4, ev.nout())))
     assert ei.value.status == YSG_ERR_UNSUPPORTED
+
+    eng, ev, km = _setup(tmp_path, "c1", {})
+
+    def unsupported(*args, **kwargs):
+        raise YspecError(YSG_ERR_UNSUPPORTED, "event_gradient")
+
+    monkeypatch.setattr(eng, "gradient", unsupported)
     syn = adjoint.ModelSynthetics(eng, ev, km, knots=[10, 100])
     rho, vp, vs = (x.clone().requires_grad_() for x in km.params())
     mm = torch.tensor([1e20, 0, 0, 0, 0, 0], dtype=torch.float64)

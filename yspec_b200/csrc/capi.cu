@@ -1191,8 +1191,8 @@ int ysg_event_gradient(ysg_handle* h, const ysg_event* ev, const ysg_time* tm, c
     int rc = check_event(h, ev);
     if (rc) return rc;
     if (!tm || !gval || !gcs || tm->nr != ev->nr || (ev->nr > 0 && !gout)) return YSG_ERR_ARG;
-    // the source in the mantle, receivers at or above it
-    if (ev->rr < ev->rs || ev->is <= h->hdr.noc) return YSG_ERR_UNSUPPORTED;
+    // the source and the receivers in the solid above the outer core
+    if (ev->is <= h->hdr.noc || ev->ir <= h->hdr.noc) return YSG_ERR_UNSUPPORTED;
     const int L = ev->lmax - ev->lmin + 1;
     if (L >= (1 << 23) || L > 65535 || ev->nw >= (1 << 24) || ev->nr > 65535) return YSG_ERR_LIMIT;
     cudaSetDevice(h->device);

@@ -1,11 +1,12 @@
 // ysg_pair_adjoint.cuh -- reverse sweep of one (omega, l) solve.
 //
 // The adjoint of pair_radial / pair_toroidal / pair_spheroidal
-// (ysg_solvers.cuh) for the self-gravitating solve with the source in the
-// mantle and the receiver at or above it, with a solid or a fluid inner core
-// and with or without an ocean (rad_solver_wg, tor_solver and sph_solver_g /
-// sph_solver_fic on their receiver-above branch, module_solver.f90:25-142,
-// :446-561, :640-823, :1203-1382): given the adjoints of the pair's uu / vv /
+// (ysg_solvers.cuh) with the source and the receiver in the mantle, the
+// receiver above or below the source, with a solid or a fluid inner core
+// and with or without an ocean, for every gravity setting (rad_solver_wg /
+// rad_solver_ng, tor_solver, sph_solver_g / sph_solver_fic and their
+// Cowling and no-gravity forms on both branches, module_solver.f90:25-142,
+// :335-561, :640-1740): given the adjoints of the pair's uu / vv /
 // ww coefficients, it adds the pair's contribution to dL/dc[i][p][k] (the
 // power-form spline segments, see ysg_adjoint.cuh).  No reference
 // counterpart: the reference has no derivatives.
@@ -281,72 +282,96 @@ __device__ inline void f2s_ngcow_adj(const cd* msb, cd* mfb)
 }
 
 // ---------------------------------------------------------------------------
-// tor_solver, receiver at or above the source (module_solver.f90:25-142)
+// tor_solver (module_solver.f90:25-142), both branches
 // ---------------------------------------------------------------------------
-// The forward solve again, keeping what the reverse sweep needs; yb is the
-// adjoint of yout.  Returns false if a step log overflowed.
+// The forward solve again, keeping what the reverse sweep needs, its output
+// in yout; yb is the adjoint of yout.  The chain from the start level (to
+// the source, or to a receiver below it) is logged as it runs and reversed
+// last; the other legs are replayed when reversed.  Returns false if a step
+// log overflowed.
 __device__ inline bool tor_solver_adj(Ctx& c, const UnitDirs& u, double rr, double rs, int ir, int is,
                                       const cd yb_out[2][2], cd yout[2][2], StepLog& L, StepLog& CL, SegGrad& G)
 {
     const ModelHdr* mh = c.mh;
     const Knot* kn = c.kn;
     int scale1 = 0, scale2 = 0, scale3 = 0;
-    cd y1[2], y2[2], y3[2];
-    const int it = is;
+    cd y1[2], y2[2] = {mk(1.0), mk(0.0)}, y3[2];
+    const bool up = rr >= rs;
+    const int it = up ? is : ir;
     int i1 = tor_start_level(c, c.ll, c.omega.x, it);
     if (i1 == it && i1 > mh->noc + 1) i1 = i1 - 1;
     const double rt = kn[i1].r;
     const bool cmb_start = i1 == mh->noc + 1;
     if (cmb_start) { y1[0] = mk(1.0); y1[1] = mk(0.0); }
     else tor_ystart(c, i1, rt, y1);
-    // the leg from the start level to the source is logged as it runs (the
-    // chain log) and reversed last; the others are replayed when reversed
     int n1 = 0;
-    if (!yint_log<TorT>(c, i1, is, rt, rs, y1, &scale1, CL, 0, &n1)) return false;
-    y3[0] = y1[0];
-    y3[1] = y1[1];
+    if (!yint_log<TorT>(c, i1, it, rt, up ? rs : rr, y1, &scale1, CL, 0, &n1)) return false;
+    // the surface solution, from the solid surface down to the receiver
+    // (receiver above) or to the source (receiver below)
+    const double rbot = up ? rr : rs;
+    const int ibot = up ? ir : is;
+    const bool down2 = rbot != kn[mh->nsl].r;
+    if (down2) yint<TorSys>(c, mh->nsl - 1, ibot, kn[mh->nsl].r, rbot, y2, &scale2);
+    // y3 continues the source-side solution from the source to the receiver
+    const cd* y3s = up ? y1 : y2;
+    y3[0] = y3s[0];
+    y3[1] = y3s[1];
+    const cd y3start[2] = {y3s[0], y3s[1]};
     if (rr != rs) yint<TorSys>(c, is, ir, rs, rr, y3, &scale3);
-    y2[0] = mk(1.0);
-    y2[1] = mk(0.0);
-    const bool down2 = rr != kn[mh->nsl].r;
-    if (down2) yint<TorSys>(c, mh->nsl - 1, ir, kn[mh->nsl].r, rr, y2, &scale2);
-    const cd D = y2[1] * y3[0] - y2[0] * y3[1];
+    // D = P[1] Q[0] - P[0] Q[1]: (P, Q) = (y2, y3) above, (y3, y1) below;
+    // b from the source-side solution (y1 above, y2 below), the receiver's
+    // solution dy = delta (y2 above, y1 below)
+    const cd* P = up ? y2 : y3;
+    const cd* Q = up ? y3 : y1;
+    const cd D = P[1] * Q[0] - P[0] * Q[1];
     const cd delta = 1.0 / D;
-    const cd b0 = y1[1], b1 = -y1[0];
-    const cd dy0 = delta * y2[0], dy1 = delta * y2[1];
-    // yout[a][0] = -(dy_a b0), yout[a][1] = -(dy_a b1), times huge^scale3
+    const cd* Bs = up ? y1 : y2;
+    const cd* R = up ? y2 : y1;
+    const cd bv[2] = {Bs[1], -Bs[0]};
+    const cd dy[2] = {delta * R[0], delta * R[1]};
     const double F = huge_pow(scale3);
-    yout[0][0] = F * (-(dy0 * b0));
-    yout[1][0] = F * (-(dy1 * b0));
-    yout[0][1] = F * (-(dy0 * b1));
-    yout[1][1] = F * (-(dy1 * b1));
-    cd yb[2][2];
     for (int a = 0; a < 2; a++)
-        for (int b = 0; b < 2; b++) yb[a][b] = F * yb_out[a][b];
-    const cd dyb0 = -(yb[0][0] * b0 + yb[0][1] * b1), dyb1 = -(yb[1][0] * b0 + yb[1][1] * b1);
-    const cd b0b = -(yb[0][0] * dy0 + yb[1][0] * dy1), b1b = -(yb[0][1] * dy0 + yb[1][1] * dy1);
-    cd y1b[2] = {-b1b, b0b};
-    const cd deltab = dyb0 * y2[0] + dyb1 * y2[1];
-    cd y2b[2] = {dyb0 * delta, dyb1 * delta};
-    const cd Db = deltab * (-(delta * delta));
-    y2b[1] = y2b[1] + Db * y3[0];
-    y2b[0] = y2b[0] - Db * y3[1];
-    cd y3b[2] = {Db * y2[1], -(Db * y2[0])};
+        for (int b = 0; b < 2; b++) yout[a][b] = F * (-(dy[a] * bv[b]));
+    // reverse: yout[a][b] = -F delta R[a] bv[b]
+    cd dyb[2] = {mk(0.0), mk(0.0)}, bvb[2] = {mk(0.0), mk(0.0)};
+    for (int a = 0; a < 2; a++)
+        for (int b = 0; b < 2; b++) {
+            const cd g = F * yb_out[a][b];
+            dyb[a] = dyb[a] - g * bv[b];
+            bvb[b] = bvb[b] - g * dy[a];
+        }
+    cd y1b[2] = {mk(0.0), mk(0.0)}, y2b[2] = {mk(0.0), mk(0.0)}, y3b[2] = {mk(0.0), mk(0.0)};
+    cd* Bsb = up ? y1b : y2b;
+    cd* Rb = up ? y2b : y1b;
+    cd* Pb = up ? y2b : y3b;
+    cd* Qb = up ? y3b : y1b;
+    Bsb[1] = Bsb[1] + bvb[0];
+    Bsb[0] = Bsb[0] - bvb[1];
+    const cd deltab = dyb[0] * R[0] + dyb[1] * R[1];
+    Rb[0] = Rb[0] + delta * dyb[0];
+    Rb[1] = Rb[1] + delta * dyb[1];
+    const cd Db = -(deltab * (delta * delta));
+    Pb[1] = Pb[1] + Db * Q[0];
+    Pb[0] = Pb[0] - Db * Q[1];
+    Qb[0] = Qb[0] + Db * P[1];
+    Qb[1] = Qb[1] - Db * P[0];
+    // y3 from its start at the source
+    if (rr != rs && !yint_adj<TorT>(c, is, ir, rs, rr, y3start, y3b, true, L, G)) return false;
+    cd* y3sb = up ? y1b : y2b;
+    y3sb[0] = y3sb[0] + y3b[0];
+    y3sb[1] = y3sb[1] + y3b[1];
     // the surface solution starts from a fixed vector: only its model gradient
     const cd e2[2] = {mk(1.0), mk(0.0)};
-    if (down2 && !yint_adj<TorT>(c, mh->nsl - 1, ir, kn[mh->nsl].r, rr, e2, y2b, true, L, G)) return false;
-    // y3 starts from y1 at the source
-    if (rr != rs && !yint_adj<TorT>(c, is, ir, rs, rr, y1, y3b, true, L, G)) return false;
-    y1b[0] = y1b[0] + y3b[0];
-    y1b[1] = y1b[1] + y3b[1];
+    if (down2 && !yint_adj<TorT>(c, mh->nsl - 1, ibot, kn[mh->nsl].r, rbot, e2, y2b, true, L, G)) return false;
     yint_rev<TorT>(c, CL, 0, n1, y1b, G);
     if (!cmb_start) start_adj<0>(c, u, i1, rt, y1b, G);
     return true;
 }
 
 // ---------------------------------------------------------------------------
-// sph_solver_g, solid inner core, no ocean, receiver at or above the source
-// (module_solver.f90:640-823): yb_out (6 x 4) is the adjoint of yout.
+// sph_solver_g and sph_solver_fic (module_solver.f90:640-823, :1203-1382),
+// both branches, with or without an ocean: yb_out (6 x 4) is the adjoint
+// of yout.
 // ---------------------------------------------------------------------------
 __device__ inline bool sph_solver_g_adj(Ctx& c, const UnitDirs& u, double rr, double rs, int ir, int is,
                                         const cd yb_out[6][4], cd yout[6][4], StepLog& L, StepLog& CL,
@@ -355,21 +380,22 @@ __device__ inline bool sph_solver_g_adj(Ctx& c, const UnitDirs& u, double rr, do
     const ModelHdr* mh = c.mh;
     const Knot* kn = c.kn;
     int scale1 = 0, scale2 = 0, scale3 = 0;
-    const int it = is;
-    const double rtop = rs;
+    const bool up = rr >= rs;
+    const int it = up ? is : ir;
+    const double rtop = up ? rs : rr;
     int i1 = sph_start_level(c, c.ll, c.omega.x, it);
     double rt = kn[i1].r;
-    if (i1 == 1) rt = fmin(0.1 * c.dr, 0.1 * kn[2].r);
+    if (i1 == 1 && (up || mh->fic)) rt = fmin(0.1 * c.dr, 0.1 * kn[2].r);
     if (i1 >= it) { i1 = it - 1; rt = kn[i1].r; }
-    // the chain from the start level to the source; branch 0: solid inner
-    // core start, 1: fluid start (outer core, or a fluid inner core), 2:
-    // mantle start
-    // a fluid inner core starts from the fluid minor there, as the outer core does
+    // The chain from the start level to the source (receiver above) or to
+    // the receiver (receiver below); branch 0: solid inner core start, 1:
+    // fluid start (outer core, or a fluid inner core, which starts from the
+    // fluid minor there as the outer core does), 2: mantle start.  Its legs
+    // (inner core, outer core, mantle) are logged as they run, one after
+    // the other in the chain log, and reversed in the opposite order at the
+    // end; the other integrations are replayed in the scratch log when
+    // reversed.
     const int branch = (i1 <= mh->nic && !mh->fic) ? 0 : (i1 <= mh->noc ? 1 : 2);
-    // The chain's legs (inner core, outer core, mantle to the source) are
-    // logged as they run, one after the other in the chain log, and reversed
-    // in the opposite order at the end; the other integrations are replayed
-    // in the scratch log when reversed.
     cd st[14], ms1[14], mf[5];
     int nic_s = 0, noc_s = 0, nm_s = 0;                          // steps of the three legs
     if (branch == 0) {
@@ -393,12 +419,19 @@ __device__ inline bool sph_solver_g_adj(Ctx& c, const UnitDirs& u, double rr, do
     const double mr1 = branch == 2 ? rt : kn[mh->noc + 1].r;
     const int moff = nic_s + noc_s;
     if (!yint_log<MinorSolidGT>(c, mi1, it, mr1, rtop, ms1, &scale1, CL, moff, &nm_s)) return false;
+    // ms3 continues the chain between the receiver and the source
     cd ms3[14], ms2[14];
     for (int k = 0; k < 14; k++) ms3[k] = ms1[k];
-    if (rr > rs) yint<MinorSolidG>(c, is, ir, rs, rr, ms3, &scale3);
-    // the solution from the surface down to the receiver: through an ocean
-    // first (a fluid minor from the surface to its floor, then the solid
-    // minor from the floor), else the solid minor from the surface
+    const bool leg3 = up ? rr > rs : rs > rr;
+    const int l3a = up ? is : ir, l3b = up ? ir : is;
+    const double r3a = up ? rs : rr, r3b = up ? rr : rs;
+    if (leg3) yint<MinorSolidG>(c, l3a, l3b, r3a, r3b, ms3, &scale3);
+    // the solution from the surface down to the receiver (receiver above) or
+    // to the source (below): through an ocean first (a fluid minor from the
+    // surface to its floor, then the solid minor from the floor), else the
+    // solid minor from the surface
+    const int ibot = up ? ir : is;
+    const double rbot = up ? rr : rs;
     cd e1[14], mo[5], ms2s[14];
     unit(e1, 14, 0);
     for (int k = 0; k < 14; k++) ms2[k] = e1[k];
@@ -409,41 +442,60 @@ __device__ inline bool sph_solver_g_adj(Ctx& c, const UnitDirs& u, double rr, do
         yint<MinorFluidG>(c, mh->nknot - 1, mh->nsl + 1, kn[mh->nknot].r, kn[mh->nsl + 1].r, mf2, &scale2);
         f2s(mf2, ms2);
     }
-    const int s2i1 = mh->ocean ? mh->nsl : mh->nknot - 1;
+    const int s2i1 = mh->ocean ? mh->nsl : (up ? mh->nknot - 1 : mh->nknot);
     const double s2r1 = mh->ocean ? kn[mh->nsl].r : kn[mh->nknot].r;
     for (int k = 0; k < 14; k++) ms2s[k] = ms2[k];
-    yint<MinorSolidG>(c, s2i1, ir, s2r1, rr, ms2, &scale2);
+    yint<MinorSolidG>(c, s2i1, ibot, s2r1, rbot, ms2, &scale2);
     const cd delta = delta_solid(ms3, ms2);
     const int jump[4] = {0, 1, 3, 4};
     cd ms1b[14], ms2b[14], ms3b[14];
     for (int k = 0; k < 14; k++) ms1b[k] = ms2b[k] = ms3b[k] = mk(0.0);
     cd deltab = mk(0.0);
+    // the b-vector of each jump from the source to the receiver
+    cd* const mst = up ? ms1 : ms2;                 // the minors it starts from
+    cd* const mstb = up ? ms1b : ms2b;
+    cd* const mso = up ? ms2 : ms1;                 // the minors it is read with
+    cd* const msob = up ? ms2b : ms1b;
     for (int i = 0; i < 4; i++) {
         cd s[6];
         unit(s, 6, jump[i]);
         int scale4 = 0;
-        cd b[14], ys[6];
-        b_solid_start(ms1, s, b);
+        cd b[14], b0[14], ys[6];
+        b_solid_start(mst, s, b0);
+        for (int k = 0; k < 14; k++) b[k] = up ? b0[k] : (-b0[k]) / delta;
         int nb = 0;
         if (!yint_log<BvecSolidGT>(c, is, ir, rs, rr, b, &scale4, L, 0, &nb)) return false;
-        sph_ysol(ms2, b, ys);
-        // yout[k][i] = (-ys[k] / delta) huge^(scale3 - scale4)
+        sph_ysol(mso, b, ys);
         const double F = huge_pow(scale3 - scale4);
         cd ysb[6];
         for (int k = 0; k < 6; k++) {
-            yout[k][i] = F * (-(ys[k] / delta));
             const cd yk = F * yb_out[k][i];
-            ysb[k] = -(yk / delta);
-            deltab = deltab + yk * (ys[k] / (delta * delta));
+            if (up) {
+                // yout[k][i] = (-ys[k] / delta) F
+                yout[k][i] = F * (-(ys[k] / delta));
+                ysb[k] = -(yk / delta);
+                deltab = deltab + yk * (ys[k] / (delta * delta));
+            } else {
+                // yout[k][i] = ys[k] F, the start divided by -delta
+                yout[k][i] = F * ys[k];
+                ysb[k] = yk;
+            }
         }
         cd bb[14];
         for (int k = 0; k < 14; k++) bb[k] = mk(0.0);
-        ysol_adj(ms2, b, ysb, ms2b, bb);
+        ysol_adj(mso, b, ysb, msob, bb);
         yint_rev<BvecSolidGT>(c, L, 0, nb, bb, G);
-        bstart_adj(s, bb, ms1b);
+        if (!up) {
+            // b = -b0 / delta
+            for (int k = 0; k < 14; k++) {
+                deltab = deltab + bb[k] * (b0[k] / (delta * delta));
+                bb[k] = -(bb[k] / delta);
+            }
+        }
+        bstart_adj(s, bb, mstb);
     }
     delta_adj(ms3, ms2, deltab, ms3b, ms2b);
-    if (!yint_adj<MinorSolidGT>(c, s2i1, ir, s2r1, rr, ms2s, ms2b, true, L, G)) return false;
+    if (!yint_adj<MinorSolidGT>(c, s2i1, ibot, s2r1, rbot, ms2s, ms2b, true, L, G)) return false;
     if (mh->ocean) {
         // back through the ocean: the fluid minor starts from a fixed vector
         cd mf2b[5];
@@ -453,9 +505,7 @@ __device__ inline bool sph_solver_g_adj(Ctx& c, const UnitDirs& u, double rr, do
                                     true, L, G))
             return false;
     }
-    if (rr > rs) {
-        if (!yint_adj<MinorSolidGT>(c, is, ir, rs, rr, ms1, ms3b, true, L, G)) return false;
-    }
+    if (leg3 && !yint_adj<MinorSolidGT>(c, l3a, l3b, r3a, r3b, ms1, ms3b, true, L, G)) return false;
     for (int k = 0; k < 14; k++) ms1b[k] = ms1b[k] + ms3b[k];
     // back along the chain to the start level
     yint_rev<MinorSolidGT>(c, CL, moff, nm_s, ms1b, G);
@@ -480,15 +530,10 @@ __device__ inline bool sph_solver_g_adj(Ctx& c, const UnitDirs& u, double rr, do
 }
 
 // ---------------------------------------------------------------------------
-// The per-pair epilogues of yspec.f90:301-316 and :344-400.
-// ---------------------------------------------------------------------------
-// The class of events the reverse sweep covers: self-gravitation, a solid
-// inner core, no ocean, the receiver at or above the source.
-// ---------------------------------------------------------------------------
 // sph_solver_nc without self-gravitation (KIND 0, module_solver.f90:827-1010)
 // and in the Cowling approximation (KIND 1, :1014-1195), with their fluid
-// inner core forms (:1386-1740), receiver at or above the source: the same
-// sweep as sph_solver_g_adj on the 5-minor / 2-minor / 4-vector systems.
+// inner core forms (:1386-1740), both branches: the same sweep as
+// sph_solver_g_adj on the 5-minor / 2-minor / 4-vector systems.
 // ---------------------------------------------------------------------------
 template <int KIND>
 __device__ inline bool sph_solver_nc_adj(Ctx& c, const UnitDirs& u, double rr, double rs, int ir, int is,
@@ -501,11 +546,12 @@ __device__ inline bool sph_solver_nc_adj(Ctx& c, const UnitDirs& u, double rr, d
     const ModelHdr* mh = c.mh;
     const Knot* kn = c.kn;
     int scale1 = 0, scale2 = 0, scale3 = 0;
-    const int it = is;
-    const double rtop = rs;
+    const bool up = rr >= rs;
+    const int it = up ? is : ir;
+    const double rtop = up ? rs : rr;
     int i1 = sph_start_level(c, c.ll, c.omega.x, it);
     double rt = kn[i1].r;
-    if (i1 == 1) rt = fmin(0.1 * c.dr, 0.1 * kn[2].r);
+    if (i1 == 1 && (up || mh->fic)) rt = fmin(0.1 * c.dr, 0.1 * kn[2].r);
     if (i1 >= it) { i1 = it - 1; rt = kn[i1].r; }
     // branch 0: solid inner core start, 1: fluid start (outer core, or a
     // fluid inner core), 2: mantle start; the chain's legs in the chain log
@@ -532,8 +578,14 @@ __device__ inline bool sph_solver_nc_adj(Ctx& c, const UnitDirs& u, double rr, d
     if (!yint_log<SolidT>(c, mi1, it, mr1, rtop, ms1, &scale1, CL, moff, &nm_s)) return false;
     cd ms3[5], ms2[5], ms2s[5], mo[2];
     for (int k = 0; k < 5; k++) ms3[k] = ms1[k];
-    if (rr > rs) yint<MinorSolidNC<KIND>>(c, is, ir, rs, rr, ms3, &scale3);
-    // from the surface down to the receiver, through an ocean first
+    const bool leg3 = up ? rr > rs : rs > rr;
+    const int l3a = up ? is : ir, l3b = up ? ir : is;
+    const double r3a = up ? rs : rr, r3b = up ? rr : rs;
+    if (leg3) yint<MinorSolidNC<KIND>>(c, l3a, l3b, r3a, r3b, ms3, &scale3);
+    // from the surface down to the receiver (above) or the source (below),
+    // through an ocean first
+    const int ibot = up ? ir : is;
+    const double rbot = up ? rr : rs;
     unit(ms2, 5, 0);
     unit(mo, 2, 0);
     if (mh->ocean) {
@@ -544,34 +596,53 @@ __device__ inline bool sph_solver_nc_adj(Ctx& c, const UnitDirs& u, double rr, d
     const int s2i1 = mh->ocean ? mh->nsl : mh->nknot;
     const double s2r1 = mh->ocean ? kn[mh->nsl].r : kn[mh->nknot].r;
     for (int k = 0; k < 5; k++) ms2s[k] = ms2[k];
-    yint<MinorSolidNC<KIND>>(c, s2i1, ir, s2r1, rr, ms2, &scale2);
+    yint<MinorSolidNC<KIND>>(c, s2i1, ibot, s2r1, rbot, ms2, &scale2);
     const cd delta = delta_solid_ngcow(ms3, ms2);
     cd ms1b[5], ms2b[5], ms3b[5];
     for (int k = 0; k < 5; k++) ms1b[k] = ms2b[k] = ms3b[k] = mk(0.0);
     cd deltab = mk(0.0);
+    // the b-vector of each jump starts from the chain's end (receiver
+    // above) or from the surface solution divided by -delta (below), and is
+    // read at the receiver with the other
+    cd* const mst = up ? ms1 : ms2;
+    cd* const mstb = up ? ms1b : ms2b;
+    cd* const mso = up ? ms2 : ms1;
+    cd* const msob = up ? ms2b : ms1b;
     for (int i = 0; i < 4; i++) {
-        cd s[4], b[4], ys[4];
+        cd s[4], b[4], b0[4], ys[4];
         unit(s, 4, i);
-        b_solid_start_ngcow(ms1, s, b);
+        b_solid_start_ngcow(mst, s, b0);
+        for (int k = 0; k < 4; k++) b[k] = up ? b0[k] : (-b0[k]) / delta;
         int scale4 = 0, nb = 0;
         if (!yint_log<BvecT>(c, is, ir, rs, rr, b, &scale4, L, 0, &nb)) return false;
-        sph_ysol_ngcow(ms2, b, ys);
-        // yout[k][i] = (ys[k] / delta) huge^(scale3 - scale4)
+        sph_ysol_ngcow(mso, b, ys);
         const double F = huge_pow(scale3 - scale4);
         cd ysb[4];
         for (int k = 0; k < 4; k++) {
-            yout[k][i] = F * (ys[k] / delta);
             const cd yk = F * yb_out[k][i];
-            ysb[k] = yk / delta;
-            deltab = deltab - yk * (ys[k] / (delta * delta));
+            if (up) {
+                // yout[k][i] = (ys[k] / delta) huge^(scale3 - scale4)
+                yout[k][i] = F * (ys[k] / delta);
+                ysb[k] = yk / delta;
+                deltab = deltab - yk * (ys[k] / (delta * delta));
+            } else {
+                yout[k][i] = F * ys[k];
+                ysb[k] = yk;
+            }
         }
         cd bb[4] = {mk(0.0), mk(0.0), mk(0.0), mk(0.0)};
-        ysol_ngcow_adj(ms2, b, ysb, ms2b, bb);
+        ysol_ngcow_adj(mso, b, ysb, msob, bb);
         yint_rev<BvecT>(c, L, 0, nb, bb, G);
-        bstart_ngcow_adj(s, bb, ms1b);
+        if (!up) {
+            for (int k = 0; k < 4; k++) {
+                deltab = deltab + bb[k] * (b0[k] / (delta * delta));
+                bb[k] = -(bb[k] / delta);
+            }
+        }
+        bstart_ngcow_adj(s, bb, mstb);
     }
     delta_ngcow_adj(ms3, ms2, deltab, ms3b, ms2b);
-    if (!yint_adj<SolidT>(c, s2i1, ir, s2r1, rr, ms2s, ms2b, true, L, G)) return false;
+    if (!yint_adj<SolidT>(c, s2i1, ibot, s2r1, rbot, ms2s, ms2b, true, L, G)) return false;
     if (mh->ocean) {
         cd mf2b[2] = {mk(0.0), mk(0.0)};
         f2s_ngcow_adj(ms2b, mf2b);
@@ -579,7 +650,7 @@ __device__ inline bool sph_solver_nc_adj(Ctx& c, const UnitDirs& u, double rr, d
                               G))
             return false;
     }
-    if (rr > rs && !yint_adj<SolidT>(c, is, ir, rs, rr, ms1, ms3b, true, L, G)) return false;
+    if (leg3 && !yint_adj<SolidT>(c, l3a, l3b, r3a, r3b, ms1, ms3b, true, L, G)) return false;
     for (int k = 0; k < 5; k++) ms1b[k] = ms1b[k] + ms3b[k];
     yint_rev<SolidT>(c, CL, moff, nm_s, ms1b, G);
     if (branch == 2) {
@@ -758,35 +829,46 @@ __device__ inline bool rad_solver_wg_adj(Ctx& c, const UnitDirs& u, double rr, d
 }
 
 // rad_solver_ng (ysg_solvers.cuh, module_solver.f90:335-441; the radial
-// system in its gravity form, rad_derivs_ng), receiver at or above the
-// source: the forward pass (its upward leg from the centre to the source in
-// the chain log), its output in yout, then the reverse sweep from yb.
+// system in its gravity form, rad_derivs_ng), both branches: the forward
+// pass (its upward leg from the centre to the source or receiver in the
+// chain log), its output in yout, then the reverse sweep from yb.
 __device__ inline bool rad_solver_ng_adj(Ctx& c, const UnitDirs& u, double rr, double rs, int ir, int is,
                                          const cd yb[2][2], cd yout[2][2], StepLog& L, StepLog& CL, SegGrad& G)
 {
     const ModelHdr* mh = c.mh;
     const Knot* kn = c.kn;
+    const bool up = rr >= rs;
     int scale1 = 0, scale2 = 0, scale3 = 0, n1 = 0;
     const double rt = fmin(0.1 * c.dr, 0.1 * kn[2].r);
     cd y1[2], y2[2] = {mk(1.0), mk(0.0)}, y3[2], y2s[2];
     rad_ystart<false>(c, 1, rt, y1);
-    if (!yint_log<RadT>(c, 1, is, rt, rs, y1, &scale1, CL, 0, &n1)) return false;
-    const bool leg2 = rr != kn[mh->nknot].r, leg3 = rs != rr;
-    if (leg2) yint<RadSys>(c, mh->nknot - 1, ir, kn[mh->nknot].r, rr, y2, &scale2);
+    // the upward leg ends at the lower of the two points, the downward leg
+    // starts at the surface (above) or the top of the solid (below)
+    const int ilo = up ? is : ir, ihi = up ? ir : is;
+    const double rlo = up ? rs : rr, rhi = up ? rr : rs;
+    const int top = up ? mh->nknot : mh->nsl;
+    if (!yint_log<RadT>(c, 1, ilo, rt, rlo, y1, &scale1, CL, 0, &n1)) return false;
+    const bool leg2 = rhi != kn[top].r, leg3 = rs != rr;
+    if (leg2) yint<RadSys>(c, top - 1, ihi, kn[top].r, rhi, y2, &scale2);
     y2s[0] = y2[0];
     y2s[1] = y2[1];
     y3[0] = y2[0];
     y3[1] = y2[1];
-    if (leg3) yint<RadSys>(c, ir, is, rr, rs, y3, &scale3);
+    if (leg3) yint<RadSys>(c, ihi, ilo, rhi, rlo, y3, &scale3);
     const cd D = y3[1] * y1[0] - y3[0] * y1[1];
     const bool degenerate = cabs(D) < 1.0e-100;
     const cd delta = degenerate ? mk(0.0) : 1.0 / D;
-    const cd bv[2] = {y1[1], -y1[0]};
-    const cd dy[2] = {delta * y2[0], delta * y2[1]};
-    const double F = scale3 != 0 ? huge_pow(scale3) : 1.0;
+    // ya forms b, yr is read at the receiver
+    const cd* ya = up ? y1 : y2;
+    const cd* yr = up ? y2 : y1;
+    const cd bv[2] = {ya[1], -ya[0]};
+    const cd dy[2] = {delta * yr[0], delta * yr[1]};
+    // the receiver-below branch undoes only a positive scale3
+    // (module_solver.f90:433-437)
+    const double F = (up ? scale3 != 0 : scale3 > 0) ? huge_pow(scale3) : 1.0;
     for (int a = 0; a < 2; a++)
         for (int b = 0; b < 2; b++) yout[a][b] = F * (-(dy[a] * bv[b]));
-    // reverse: yout[a][b] = -F delta y2[a] bv[b]
+    // reverse: yout[a][b] = -F delta yr[a] bv[b]
     cd dyb[2] = {mk(0.0), mk(0.0)}, bvb[2] = {mk(0.0), mk(0.0)};
     for (int a = 0; a < 2; a++)
         for (int b = 0; b < 2; b++) {
@@ -794,9 +876,14 @@ __device__ inline bool rad_solver_ng_adj(Ctx& c, const UnitDirs& u, double rr, d
             dyb[a] = dyb[a] - g * bv[b];
             bvb[b] = bvb[b] - g * dy[a];
         }
-    cd y1b[2] = {-bvb[1], bvb[0]};
-    const cd deltab = dyb[0] * y2[0] + dyb[1] * y2[1];
-    cd y2b[2] = {delta * dyb[0], delta * dyb[1]};
+    const cd yab[2] = {-bvb[1], bvb[0]};
+    const cd deltab = dyb[0] * yr[0] + dyb[1] * yr[1];
+    const cd yrb[2] = {delta * dyb[0], delta * dyb[1]};
+    cd y1b[2], y2b[2];
+    for (int k = 0; k < 2; k++) {
+        y1b[k] = up ? yab[k] : yrb[k];
+        y2b[k] = up ? yrb[k] : yab[k];
+    }
     cd y3b[2] = {mk(0.0), mk(0.0)};
     if (!degenerate) {
         const cd Db = -(deltab * (delta * delta));
@@ -805,16 +892,19 @@ __device__ inline bool rad_solver_ng_adj(Ctx& c, const UnitDirs& u, double rr, d
         y1b[0] = y1b[0] + Db * y3[1];
         y1b[1] = y1b[1] - Db * y3[0];
     }
-    if (leg3 && !yint_adj<RadT>(c, ir, is, rr, rs, y2s, y3b, true, L, G)) return false;
+    if (leg3 && !yint_adj<RadT>(c, ihi, ilo, rhi, rlo, y2s, y3b, true, L, G)) return false;
     y2b[0] = y2b[0] + y3b[0];
     y2b[1] = y2b[1] + y3b[1];
     const cd e[2] = {mk(1.0), mk(0.0)};
-    if (leg2 && !yint_adj<RadT>(c, mh->nknot - 1, ir, kn[mh->nknot].r, rr, e, y2b, true, L, G)) return false;
+    if (leg2 && !yint_adj<RadT>(c, top - 1, ihi, kn[top].r, rhi, e, y2b, true, L, G)) return false;
     yint_rev<RadT>(c, CL, 0, n1, y1b, G);
     start_adj<6>(c, u, 1, rt, y1b, G);
     return true;
 }
 
+// ---------------------------------------------------------------------------
+// The per-pair epilogues of yspec.f90:301-316 and :344-400.
+// ---------------------------------------------------------------------------
 // coefb: adjoints of the 15 coefficients of pair (l = 0, j); only uu(3)
 // is formed by the radial solve (yspec.f90:263-293).
 __device__ inline bool pair_radial_adj(Ctx& c, const UnitDirs& u, const EventDev& ev, int j, const cd* coefb,
@@ -839,11 +929,6 @@ __device__ inline bool pair_radial_adj(Ctx& c, const UnitDirs& u, const EventDev
     const cd s0b[2] = {g * yrad[0][0], g * yrad[0][1]};
     source_rad_adj(c, u, ev.is, ev.rs, ev.mm, s0b, G);
     return true;
-}
-
-__device__ __forceinline__ bool pair_adj_supported(const ModelHdr* mh, const EventDev& ev)
-{
-    return ev.rr >= ev.rs && ev.is > mh->noc;
 }
 
 // wwb: adjoints of ww(1:5) of pair (l >= 2, j).  The adjoints of the
