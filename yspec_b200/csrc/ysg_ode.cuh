@@ -535,6 +535,41 @@ struct BvecSolidG {
     }
 };
 
+// The transpose of BvecSolidG's system: d = A^T k for the coefficient
+// matrix A of sph_bvec_solid_derivs (module_int.f90:1016-1057).  The
+// b-vector solves of the batched form integrate it backwards to obtain only
+// the response rows a pair needs (sph_solver_g).
+struct BvecSolidGTr {
+    static constexpr int N = 14, CLS = 7;
+    template <class Out>
+    __device__ static __forceinline__ void tr(const SolidCoef& a, const mcplx* k, Out d)
+    {
+        const mcplx t11 = a.t11, t12 = a.t12, k11 = a.k11, k22 = a.k22;
+        const mcplx s11 = a.s11, s12 = a.s12, s22 = a.s22;
+        const mreal t21 = a.t21, t22 = a.t22, t31 = a.t31, t33 = a.t33, k33 = a.k33;
+        const mreal s13 = a.s13, s23 = a.s23;
+        d[0] = cmsc(cmsc(k11 * k[6], (t11 + t22), k[0]), k22, k[3]);
+        d[1] = cmsc(cmsc(cmsc(k11 * k[9], (t11 + t33), k[1]), k33, k[4]), t12, k[5]);
+        d[2] = cmsc(cmsc(cmsc(cmsc(cmac(t21 * k[3], t31, (2.0 * k[4])), s12, k[0]), s23, k[5]), t12, k[6]), s13, (2.0 * k[1]));
+        d[3] = cmsc(cmsc(cmsc(cmsc(cmac(t12 * k[2], (t22 - t11), k[3]), s22, k[0]), s23, k[1]), t12, k[7]), k11, k[11]);
+        d[4] = cmsc(cmsc(cmsc((t33 - t11) * k[4], s23, k[0]), t12, k[8]), k11, k[12]);
+        d[5] = cmsc(cmsc(cmsc(cmac(t31 * k[0], k22, k[10]), t21, k[1]), (t22 + t33), k[5]), k33, k[8]);
+        d[6] = cmsc(cmsc(cmac(cmac(cmac(cmac(s11 * k[0], (t11 - t22), k[6]), t21, k[7]), t31, k[8]), k22, k[11]), t21, k[2]), s13, k[5]);
+        d[7] = cmsc(cmsc(cmsc(cmac(cmac(s12 * k[0], t31, k[4]), t12, k[6]), s13, k[1]), t21, k[3]), s23, (2.0 * k[5]));
+        d[8] = cmsc(cmsc(cmac(s13 * k[0], (t33 - t22), k[8]), t21, k[4]), k22, k[13]);
+        d[9] = cmsc(cmac(cmac(cmac(cmac(s11 * k[1], s12, k[5]), (t11 - t33), k[9]), t21, k[10]), k33, k[12]), t31, k[2]);
+        d[10] = cmsc(cmac(cmac(cmac(cmac(s12 * k[1], s22, k[5]), t12, k[9]), (t22 - t33), k[10]), k33, k[13]), t31, k[3]);
+        d[11] = cmsc(cmsc(cmsc(cmsc(cmac(cmac(cmac(s12 * k[2], s22, k[6]), s23, k[9]), (t11 + t22), k[11]), s11, k[3]), s12, k[7]), s13, k[10]), t31, k[13]);
+        d[12] = cmsc(cmsc(cmac(cmac(cmac(s13 * k[2], s23, k[6]), (t11 + t33), k[12]), t21, k[13]), s11, k[4]), s12, k[8]);
+        d[13] = cmsc(cmsc(cmac(cmac(cmac(s13 * k[3], s23, k[7]), t12, k[12]), (t22 + t33), k[13]), s12, k[4]), s22, k[8]);
+    }
+    template <class Out>
+    __device__ static __forceinline__ void f(const Ctx& c, double r, const mcplx* k, Out d)
+    {
+        tr(solid_amat<2>(c, r), k, d);
+    }
+};
+
 // module_int.f90:1060-1110 sph_bvec_solid_derivs_ng / _cow
 template <int KIND>
 struct BvecSolidNC {
@@ -547,6 +582,22 @@ struct BvecSolidNC {
         d[1] = cmsc(cmsc(cmsc(-(a.s12 * b[2]), a.s22, b[3]), a.t12, b[0]), a.t22, b[1]);
         d[2] = cmac(cmac(-(a.k11 * b[0]), a.t11, b[2]), a.t12, b[3]);
         d[3] = cmac(cmac(-(a.k22 * b[1]), a.t21, b[2]), a.t22, b[3]);
+    }
+};
+
+// The transpose of BvecSolidNC's system (module_int.f90:1060-1110), for
+// the backward response-row integrations of sph_solver_nc.
+template <int KIND>
+struct BvecSolidNCTr {
+    static constexpr int N = 4, CLS = 3;
+    template <class Out>
+    __device__ static __forceinline__ void f(const Ctx& c, double r, const mcplx* k, Out d)
+    {
+        const SolidCoef a = solid_amat<KIND>(c, r);
+        d[0] = cmsc(cmsc(-(a.t11 * k[0]), a.t12, k[1]), a.k11, k[2]);
+        d[1] = cmsc(cmsc(-(a.t21 * k[0]), a.t22, k[1]), a.k22, k[3]);
+        d[2] = cmsc(cmsc(cmac(a.t11 * k[2], a.t21, k[3]), a.s11, k[0]), a.s12, k[1]);
+        d[3] = cmsc(cmsc(cmac(a.t12 * k[2], a.t22, k[3]), a.s12, k[0]), a.s22, k[1]);
     }
 };
 
@@ -629,25 +680,6 @@ __constant__ double ck_fold[6][4] = {
 __constant__ int ck_slot[6] = {0, 1, 2, 3, 1, 1};
 __constant__ double ck_w[6] = {1.0, 1.0, 1.0, 1.0, 253.0 / 4096.0, 512.0 / 1771.0};
 
-// Derivative writer: stores (add = false) or adds w * value (add = true)
-// into one slab slot.  Held by value so it lives in registers.
-struct SlotOut {
-    cd* p;
-    double w;
-    bool add;
-    struct Ref {
-        cd* a;
-        double w;
-        bool add;
-        __device__ __forceinline__ void operator=(cd v) const
-        {
-            if (add) *a += w * v;
-            else *a = v;
-        }
-    };
-    __device__ __forceinline__ Ref operator[](int i) const { return Ref{p + i * KS, w, add}; }
-};
-
 // The step as a runtime loop over the six stages with one copy of the
 // right-hand side (six inlined 14-component bodies overflow the
 // instruction cache); the stage inputs and the two folds are loops over
@@ -684,11 +716,98 @@ __device__ __forceinline__ void rkck_step_loop(const Ctx& c, cd* y, double x, do
                 a1[o] = f0 * kb[o] + f1 * a1[o] + f2 * kb[2 * S + o] + f3 * kb[3 * S + o];
             }
         }
-        Sys::f(c, x + ck_a[s] * h, yt, SlotOut{kb + ck_slot[s] * S, ck_w[s], s >= 4});
+        // the derivative is formed in registers and written in one pass:
+        // stored into its slot (stages 1-4) or added with its weight into A1
+        cd d[N];
+        Sys::f(c, x + ck_a[s] * h, yt, d);
+        if (s < 4) {
+            cd* const o = kb + s * S;
+#pragma unroll
+            for (int i = 0; i < N; i++) o[i * KS] = d[i];
+        } else {
+            const double w = ck_w[s];
+            cd* const o = kb + S;
+#pragma unroll
+            for (int i = 0; i < N; i++) o[i * KS] += w * d[i];
+        }
     }
     const cd* a1 = kb + S;
 #pragma unroll
     for (int i = 0; i < N; i++) y[i] = y[i] + h * a1[i * KS];
+}
+
+// Transposed step for a linear system y' = A(r) y: w <- M^T w, where M is
+// the matrix of one Cash-Karp step at (x, h) (M y = the step's result from
+// y).  With Y_s the stage inputs and k_s = A_s Y_s, the step is
+// y' = y + h sum_s c_s k_s, Y_s = y + h sum_{t<s} b_st k_t; its transpose
+// visits the stages backwards:
+//   K_s = h (c_s w + sum_{u>s} b_us G_u),  G_s = A_s^T K_s,
+//   w' = w + sum_s G_s.
+// The linear system needs no forward state: A_s is formed again at the
+// stage radius.  Four slots as in the forward step: G6..G3 are stored in
+// A0..A3; forming K2 folds them into A1 = b61 G6 + b51 G5 + b41 G4 + b31 G3
+// (the part of K1 still to come) and A0 = G6 + G5 + G4 + G3 (the part of
+// w'), G2 is added into both (b21 into A1), K1 = h (c1 w + A1), G1 is added
+// into A0, and w' = w + A0.
+//   ckt_w[s]      weight of w in K_s (times h)
+//   ckt_in[s][t]  weight of slot t in K_s (times h)
+__constant__ double ckt_w[6] = {37.0 / 378.0, 0.0, 250.0 / 621.0, 125.0 / 594.0, 0.0, 512.0 / 1771.0};
+__constant__ double ckt_in[6][4] = {
+    {0.0, 1.0, 0.0, 0.0},
+    {175.0 / 512.0, 2.5, -0.9, 9.0 / 40.0},
+    {575.0 / 13824.0, -70.0 / 27.0, 1.2, 0.0},
+    {44275.0 / 110592.0, 35.0 / 27.0, 0.0, 0.0},
+    {253.0 / 4096.0, 0.0, 0.0, 0.0},
+    {0.0, 0.0, 0.0, 0.0}};
+
+template <class Sys>
+__device__ __forceinline__ void rkck_step_loop_T(const Ctx& c, cd* w, double x, double h)
+{
+    constexpr int N = Sys::N;
+    constexpr int S = N * KS;
+    cd* const kb = c.kb;
+    cd yt[N];
+#pragma unroll 1
+    for (int s = 5; s >= 0; s--) {
+        const double hw = h * ckt_w[s];
+#pragma unroll
+        for (int i = 0; i < N; i++) yt[i] = hw * w[i];
+#pragma unroll 1
+        for (int t = 0; t < 4; t++) {
+            const double wt = ckt_in[s][t];
+            if (wt == 0.0) continue;
+            const double hb = h * wt;
+            const cd* kt = kb + t * S;
+#pragma unroll
+            for (int i = 0; i < N; i++) yt[i] += hb * kt[i * KS];
+        }
+        if (s == 1) {
+            cd* const a1 = kb + S;
+#pragma unroll 2
+            for (int i = 0; i < N; i++) {
+                const int o = i * KS;
+                const cd g6 = kb[o], g5 = a1[o], g4 = kb[2 * S + o], g3 = kb[3 * S + o];
+                a1[o] = (1631.0 / 55296.0) * g6 + (-11.0 / 54.0) * g5 + 0.3 * g4 + (3.0 / 40.0) * g3;
+                kb[o] = (g6 + g5) + (g4 + g3);
+            }
+        }
+        cd d[N];
+        Sys::f(c, x + ck_a[s] * h, yt, d);
+        if (s >= 2) {
+            cd* const o = kb + (5 - s) * S;
+#pragma unroll
+            for (int i = 0; i < N; i++) o[i * KS] = d[i];
+        } else {
+#pragma unroll
+            for (int i = 0; i < N; i++) kb[i * KS] += d[i];
+            if (s == 1) {
+#pragma unroll
+                for (int i = 0; i < N; i++) kb[S + i * KS] += 0.2 * d[i];
+            }
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < N; i++) w[i] = w[i] + kb[i * KS];
 }
 
 // The looped step with the four slots in a per-thread array (local
@@ -859,6 +978,56 @@ __device__ YSG_YINT_ATTR void yint(Ctx& cio, int i1, int i2, double r1, double r
 #if YSG_SMEM_STAGES
 #pragma unroll
     for (int k = 0; k < Sys::N; k++) yio[k] = y[k];
+    cio.il = c.il;
+    cio.nst[Sys::CLS] = c.nst[Sys::CLS];
+#endif
+}
+
+// The transpose of yint for a linear system (Sys the transposed system, e.g.
+// BvecSolidGTr): w <- (M_1 ... M_n)^T w for the steps M_j that
+// yint(c, i1, i2, r1, r2) takes, visited in reverse order at the same
+// (x, h), with yint's 1e+-20 rescaling of w counted in *scale.  The
+// count-only build counts the same steps as the forward integration.
+template <class Sys>
+__device__ YSG_YINT_ATTR void yint_T(Ctx& cio, int i1, int i2, double r1, double r2, mcplx* wio, int* scale)
+{
+#if YSG_COUNT_ONLY
+    yint<Sys>(cio, i1, i2, r1, r2, wio, scale);     // the same steps, counted
+#elif !YSG_SMEM_STAGES
+    static_assert(sizeof(Sys) == 0, "yint_T is built in the shared-memory and count-only forms only");
+#else
+    if (r2 == r1) return;
+    Ctx c = cio;
+    cd w[Sys::N];
+#pragma unroll
+    for (int k = 0; k < Sys::N; k++) w[k] = wio[k];
+    const bool up = r2 > r1;
+    const Knot* kn = c.kn;
+    const int di = up ? 1 : -1;
+    for (int i = i2; up ? (i >= i1) : (i <= i1); i -= di) {
+        double rr1, rr2;
+        if (up) {
+            rr1 = (i == i1) ? r1 : kn[i].r;
+            rr2 = (i == i2) ? r2 : kn[i + 1].r;
+        } else {
+            rr1 = (i == i1) ? r1 : kn[i + 1].r;
+            rr2 = (i == i2) ? r2 : kn[i].r;
+        }
+        if (rr1 == rr2) continue;
+        c.il = i;
+        double drr = steps(c, i);
+        const double nf = floor(fabs(rr2 - rr1) / drr);
+        int n = 2 + (int)fmin(nf, 4194304.0);
+        drr = (rr2 - rr1) / (double)(n - 1);
+        c.nst[Sys::CLS] += (unsigned)(n - 1);
+        for (int j = n - 1; j >= 1; j--) {
+            double rr = __dadd_rn(rr1, __dmul_rn((double)(j - 1), drr));
+            rkck_step_loop_T<Sys>(c, w, rr, drr);
+            if (scale) rescale<Sys::N>(w, scale);
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < Sys::N; k++) wio[k] = w[k];
     cio.il = c.il;
     cio.nst[Sys::CLS] = c.nst[Sys::CLS];
 #endif
@@ -1258,6 +1427,60 @@ __device__ __forceinline__ void sph_ysol(const mcplx* m, const mcplx* b, mcplx* 
     y[5] = YM(2) * YB(6) - YM(3) * YB(2) + YM(4) * YB(1) + YM(7) * YB(11) +
            YM(8) * (YB(3) - YB(8)) + YM(9) * YB(4) - YM(11) * YB(10) + YM(12) * YB(7) +
            YM(14) * YB(12);
+}
+
+// Row k (0, 1 or 2) of sph_ysol as a vector: q . b = sph_ysol(m, b)[k].
+__device__ __forceinline__ void sph_ysol_row(const mcplx* m, int k, mcplx* q)
+{
+#pragma unroll
+    for (int j = 0; j < 14; j++) q[j] = mk(0.0);
+    if (k == 0) {
+        q[2] = YM(3); q[5] = YM(1); q[6] = YM(2); q[7] = 2.0 * YM(3); q[8] = YM(4);
+        q[9] = YM(5); q[10] = YM(6); q[11] = YM(7); q[12] = YM(8); q[13] = YM(9);
+    } else if (k == 1) {
+        q[1] = -YM(1); q[2] = -2.0 * YM(2); q[7] = -YM(2); q[3] = -YM(3); q[4] = -YM(4);
+        q[10] = -YM(5); q[13] = -YM(8); q[9] = YM(10); q[11] = YM(11); q[12] = YM(12);
+    } else {
+        q[0] = YM(1); q[8] = -YM(2); q[4] = YM(3); q[7] = YM(5); q[2] = -YM(5);
+        q[3] = -YM(6); q[13] = YM(7); q[6] = -YM(10); q[12] = -YM(11); q[11] = YM(13);
+    }
+}
+
+// The transpose of b_solid_start in the jump vector: u[s] = w . b(m, e_s),
+// so that w . b_solid_start(m, s) = sum_s u[s] s[s].
+__device__ __forceinline__ void b_solid_start_T(const mcplx* m, const mcplx* w, mcplx* u)
+{
+    u[0] = YM(14) * w[5] - YM(7) * w[6] - YM(11) * w[7] - YM(13) * w[8] - YM(8) * w[9] -
+           YM(12) * w[10] + YM(2) * w[11] + YM(5) * w[12] + YM(10) * w[13];
+    u[1] = -(YM(14) * w[1]) + YM(7) * w[2] + YM(11) * w[3] + YM(13) * w[4] - YM(9) * w[9] +
+           YM(8) * w[10] + YM(3) * w[11] + YM(6) * w[12] - YM(5) * w[13];
+    u[2] = YM(14) * w[0] + YM(8) * w[2] + YM(12) * w[3] - YM(11) * w[4] + YM(9) * w[6] -
+           YM(8) * w[7] + YM(7) * w[8] + YM(4) * w[11] - YM(3) * w[12] + YM(2) * w[13];
+    u[3] = -(YM(7) * w[0]) - YM(8) * w[1] - YM(2) * w[3] - YM(5) * w[4] - YM(9) * w[5] -
+           YM(3) * w[7] - YM(6) * w[8] - YM(4) * w[10] - YM(1) * w[13];
+    u[4] = -(YM(11) * w[0]) - YM(12) * w[1] + YM(2) * w[2] - YM(10) * w[4] + YM(8) * w[5] +
+           YM(3) * w[6] + YM(5) * w[8] + YM(4) * w[9] + YM(1) * w[12];
+    u[5] = -(YM(13) * w[0]) + YM(11) * w[1] + YM(5) * w[2] + YM(10) * w[3] - YM(7) * w[5] +
+           YM(6) * w[6] - YM(5) * w[7] - YM(3) * w[9] + YM(2) * w[10] - YM(1) * w[11];
+}
+
+// Row k (0 or 1) of sph_ysol_ngcow as a vector, and the transpose of
+// b_solid_start_ngcow in the jump vector (as sph_ysol_row, b_solid_start_T).
+__device__ __forceinline__ void sph_ysol_row_ngcow(const mcplx* m, int k, mcplx* q)
+{
+    if (k == 0) {
+        q[0] = mk(0.0); q[1] = YM(1); q[2] = YM(2); q[3] = YM(3);
+    } else {
+        q[0] = -YM(1); q[1] = mk(0.0); q[2] = YM(4); q[3] = -YM(2);
+    }
+}
+
+__device__ __forceinline__ void b_solid_start_T_ngcow(const mcplx* m, const mcplx* w, mcplx* u)
+{
+    u[0] = YM(5) * w[1] + YM(2) * w[2] + YM(4) * w[3];
+    u[1] = -(YM(5) * w[0]) + YM(3) * w[2] - YM(2) * w[3];
+    u[2] = -(YM(2) * w[0]) - YM(3) * w[1] + YM(1) * w[3];
+    u[3] = -(YM(4) * w[0]) + YM(2) * w[1] - YM(1) * w[2];
 }
 
 __device__ __forceinline__ void sph_ysol_ngcow(const mcplx* m, const mcplx* b, mcplx* y)

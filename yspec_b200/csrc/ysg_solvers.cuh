@@ -324,8 +324,12 @@ __device__ inline void rad_solver_wg(Ctx& c, double rr, double rs, mcplx yout[2]
 
 // Spheroidal solve with self-gravitation: sph_solver (:640-823) and
 // sph_solver_fic (:1203-1382).  yout[6][4] holds the responses to unit
-// jumps in components 1, 2, 4, 5 (yspec.f90:234-238).
-__device__ inline void sph_solver_g(Ctx& c, double rr, double rs, int ir, int is, mcplx yout[6][4])
+// jumps in components 1, 2, 4, 5 (yspec.f90:234-238).  `rows` (bit k for
+// yout[k]) names the rows the caller uses; the shared-memory form computes
+// only those (rows 0-2) and leaves the others zero, the other forms compute
+// all six.
+__device__ inline void sph_solver_g(Ctx& c, double rr, double rs, int ir, int is, mcplx yout[6][4],
+                                    int rows = 0x3f)
 {
     const ModelHdr* mh = c.mh;
     const Knot* kn = c.kn;
@@ -385,6 +389,43 @@ __device__ inline void sph_solver_g(Ctx& c, double rr, double rs, int ir, int is
     }
     mcplx delta = delta_solid(ms3, ms2);
     const int jump[4] = {0, 1, 3, 4};
+#if YSG_SMEM_STAGES || YSG_COUNT_ONLY
+    // Row k of the responses to the four jumps is ys_k,i = q_k . Phi b_i:
+    // Phi the b-vector propagator from the source to the receiver, b_i the
+    // start vector of jump i (b_solid_start of the minor at the source end)
+    // and q_k row k of sph_ysol (the minor at the receiver end).  One
+    // backward integration of the transposed system per needed row,
+    // w_k = Phi^T q_k, gives ys_k,i = w_k . b_i for all four jumps at once,
+    // in place of four forward b-vector integrations.  The same quantity
+    // as the loop below, different only in rounding.
+    {
+        const mcplx* mq = up ? ms2 : ms1;
+        const mcplx* mb = up ? ms1 : ms2;
+        unsigned nrow = 0;
+        for (int k = 0; k < 6; k++) {
+            if (k > 2 || !((rows >> k) & 1)) {
+                for (int i = 0; i < 4; i++) yout[k][i] = mk(0.0);
+                continue;
+            }
+            nrow++;
+#if YSG_COUNT_ONLY
+            // the rows integrate the same span: one pass counts for each
+            if (nrow == 1) yint_T<BvecSolidGTr>(c, is, ir, rs, rr, nullptr, nullptr);
+            continue;
+#endif
+            mcplx w[14], u[6];
+            sph_ysol_row(mq, k, w);
+            int sw = 0;
+            yint_T<BvecSolidGTr>(c, is, ir, rs, rr, w, &sw);
+            b_solid_start_T(mb, w, u);
+            const double f = huge_pow(scale3 - sw);
+            for (int i = 0; i < 4; i++) yout[k][i] = ((-u[jump[i]]) / delta) * f;
+        }
+        if (YSG_COUNT_ONLY) c.nst[BvecSolidGTr::CLS] *= nrow;
+        return;
+    }
+#endif
+    (void)rows;
     // the four jumps integrate the same span at the same omega: in the
     // count-only build one pass counts for four
     for (int i = 0; i < (YSG_COUNT_ONLY ? 1 : 4); i++) {
@@ -412,6 +453,8 @@ __device__ inline void sph_solver_g(Ctx& c, double rr, double rs, int ir, int is
 // No gravity (KIND 0) / Cowling (KIND 1): sph_solver_ng (:827-1010),
 // sph_solver_cow (:1014-1195), sph_solver_ng_fic (:1386-1562),
 // sph_solver_cow_fic (:1568-1740).  yout[4][4], ss = I (yspec.f90:240-243).
+// The shared-memory form computes only rows 0 and 1 (the ones the pair
+// uses) and leaves rows 2 and 3 zero.
 template <int KIND>
 __device__ inline void sph_solver_nc(Ctx& c, double rr, double rs, int ir, int is, mcplx yout[4][4])
 {
@@ -466,6 +509,33 @@ __device__ inline void sph_solver_nc(Ctx& c, double rr, double rs, int ir, int i
         yint<MinorSolidNC<KIND>>(c, mh->nknot, ibot, kn[mh->nknot].r, rbot, ms2, &scale2);
     }
     mcplx delta = delta_solid_ngcow(ms3, ms2);
+#if YSG_SMEM_STAGES || YSG_COUNT_ONLY
+    // rows 0 and 1 from backward integrations of the transposed system, as
+    // in sph_solver_g (the receiver-above branch divides by delta after the
+    // integration, the other negates and divides the start vector)
+    {
+#if YSG_COUNT_ONLY
+        yint_T<BvecSolidNCTr<KIND>>(c, is, ir, rs, rr, nullptr, nullptr);
+        c.nst[BvecSolidNCTr<KIND>::CLS] *= 2u;
+#else
+        const mcplx* mq = up ? ms2 : ms1;
+        const mcplx* mb = up ? ms1 : ms2;
+        const mcplx sg = up ? mk(1.0) : mk(-1.0);
+        for (int k = 0; k < 2; k++) {
+            mcplx w[4], u[4];
+            sph_ysol_row_ngcow(mq, k, w);
+            int sw = 0;
+            yint_T<BvecSolidNCTr<KIND>>(c, is, ir, rs, rr, w, &sw);
+            b_solid_start_T_ngcow(mb, w, u);
+            const double f = huge_pow(scale3 - sw);
+            for (int i = 0; i < 4; i++) yout[k][i] = ((sg * u[i]) / delta) * f;
+        }
+        for (int k = 2; k < 4; k++)
+            for (int i = 0; i < 4; i++) yout[k][i] = mk(0.0);
+#endif
+        return;
+    }
+#endif
     for (int i = 0; i < (YSG_COUNT_ONLY ? 1 : 4); i++) {     // see sph_solver_g
         mcplx s[4] = {mk(0.0), mk(0.0), mk(0.0), mk(0.0)};
         s[i] = mk(1.0);
@@ -632,7 +702,11 @@ __device__ inline void pair_spheroidal(Ctx& c, const EventDev& ev, int l, int j,
     mcplx svs[5][6], ysph[6][4];
     source_vector_sph(c, ev.is, ev.rs, ev.mm, svs);
     if (ev.grav == 2) {
-        sph_solver_g(c, ev.rr, ev.rs, ev.ir, ev.is, ysph);
+        // the rows of the responses used below: the potential (row 2) alone,
+        // or the two displacement rows, with row 2 for the tilt and
+        // potential correction of the acceleration
+        const int rows = ev.pot ? 0x4 : ((ev.out == 2 && ev.cor != 0) ? 0x7 : 0x3);
+        sph_solver_g(c, ev.rr, ev.rs, ev.ir, ev.is, ysph, rows);
     } else {
         mcplx yng[4][4];
         if (ev.grav == 1) sph_solver_nc<1>(c, ev.rr, ev.rs, ev.ir, ev.is, yng);
