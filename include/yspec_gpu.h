@@ -218,7 +218,10 @@ int ysg_traces_noalloc(const ysg_time *tm, const double *d_ur, const double *d_u
 /* Several events through the batched persistent solver: one launch per
  * stage for all events, CUDA-graph captured.  outs[e] receives the traces of
  * event e as ysg_event_traces does; nouts[e] its row count.  Events share
- * the uploaded model. */
+ * the uploaded model.  With more than one event, each event's l-sum and
+ * time series run back to back on a side stream and its traces are copied
+ * out as soon as they are complete, beside the other events' stages; the
+ * call returns when every copy has finished. */
 int ysg_batch_run(ysg_handle *h, int nev, const ysg_event *evs, const ysg_time *tms,
                   double **outs, int *nouts);
 
@@ -262,7 +265,9 @@ int ysg_last_schedule(ysg_handle *h, int *sched, float tune_ms[3]);
 /* Device times in ms of the last event's stages, measured with CUDA events:
  * [0] Legendre table, [1] solves, [2] l-sum, [3] filter + inverse FFT +
  * post-processing.  For a single event (not a batch) the Legendre table is
- * built on a second stream beside the solves, so [0] overlaps [1]. */
+ * built on a second stream beside the solves, so [0] overlaps [1].  For a
+ * batch of more than one event, [2] covers the l-sums and the time series
+ * together (they run per event, back to back) and [3] is zero. */
 int ysg_last_timings(ysg_handle *h, float ms[4]);
 
 /* Counters of the last solve stage: number of (omega,l) pairs and the

@@ -121,6 +121,13 @@ struct ysg_handle {
     static constexpr int NSIDE = 4;
     cudaStream_t side[NSIDE] = {};
     cudaEvent_t fork_ev = nullptr, join_ev[NSIDE] = {};
+    // A batch's trace copies run on their own stream: the copy of event e
+    // waits only for the end of e's l-sum and time series (done_ev[e], an
+    // event-record node of the batch graph), so it overlaps the later
+    // events' stages.
+    cudaStream_t copy_st = nullptr;
+    cudaEvent_t copy_ev = nullptr;
+    std::vector<cudaEvent_t> done_ev;
     DevBuf scratch[NSIDE];
     DevBuf work, status, items, counter, evdev, coefptr;
     int nitems = 0;                  // schedule-0 tiles
@@ -616,7 +623,7 @@ cudaStream_t stream_of(ysg_handle* h, int nside, int e) { return nside ? h->side
 // K2 (all slots) -> K1 -> K3 (all slots), with timing events between the
 // stage groups; no host synchronisation.  The per-event kernels of a group
 // run on the side streams.
-int enqueue_spectra(ysg_handle* h, int nev)
+int enqueue_spectra(ysg_handle* h, int nev, bool lsum = true)
 {
     const int ns = side_count(nev);
     CK(record(h, 0));
@@ -649,6 +656,7 @@ int enqueue_spectra(ysg_handle* h, int nev)
     rc = enqueue_solve(h, nev);
     if (rc) return rc;
     CK(record(h, 2));
+    if (!lsum) return YSG_OK;        // the l-sums follow per event (enqueue_chains)
     if (h->leg_overlap) CK(cudaStreamWaitEvent(h->st, h->join_ev[1], 0));
     if (ns && (rc = fork_side(h, ns))) return rc;
     for (int e = 0; e < nev; e++) {
@@ -705,6 +713,35 @@ int enqueue_traces(ysg_handle* h, int nev, int ns)
     return YSG_OK;
 }
 
+// A batch's K3 and K4 as one chain per event (slot e on side stream e % ns,
+// each with its own scratch rows; ns = 0: all on the handle's stream), the
+// end of each chain recorded as done_ev[e] for its trace copy.  Timing: the
+// two stages share one interval, [2] of ysg_last_timings, and [3] is empty.
+int enqueue_chains(ysg_handle* h, int nev, int ns)
+{
+    int rc = ns ? fork_side(h, ns) : YSG_OK;
+    if (rc) return rc;
+    for (int e = 0; e < nev; e++) {
+        Slot& s = h->slots[(size_t)e];
+        const EventDev& d = s.pev;
+        const TraceDev& td = s.ptd;
+        const size_t nspec = (size_t)d.nw * std::max(s.nr, 1);
+        cd* d_ur = s.spec.as<cd>();
+        cudaStream_t st = stream_of(h, ns, e);
+        h->launches += s.nr > 0 ? 4 : 0;    // l-sum, pass A, pass B, rotation
+        CK(launch_lsum(d.nw, s.nr, d.lmin, d.lmax, s.coef.as<cd>(), s.leg.as<double>(), s.E.as<cd>(),
+                       d_ur, d_ur + nspec, d_ur + 2 * nspec, st));
+        CK(launch_ifft(td, d_ur, d_ur + nspec, d_ur + 2 * nspec, s.filt.as<double>(), s.tw.as<cd>(),
+                       s.expt.as<double>(), s.cs.as<double>(), h->scratch[ns ? e % ns : 0].as<cd>(),
+                       s.out.as<double>(), st));
+        CK(cudaEventRecordWithFlags(h->done_ev[(size_t)e], st, cudaEventRecordExternal));
+    }
+    if (ns && (rc = join_side(h, ns))) return rc;
+    CK(record(h, 3));
+    CK(record(h, 4));
+    return YSG_OK;
+}
+
 // Wait for the stream, read the solve counters and the status word.
 int finish(ysg_handle* h, int nev, bool spectra, bool traces)
 {
@@ -735,13 +772,13 @@ int finish(ysg_handle* h, int nev, bool spectra, bool traces)
     return status ? YSG_ERR_DEVICE_WAIT : YSG_OK;
 }
 
-int copy_out(ysg_handle* h, const Slot& s, double* out, int* nout)
+int copy_out(ysg_handle* h, const Slot& s, double* out, int* nout, cudaStream_t st = nullptr)
 {
     const TraceDev& td = s.ptd;
     if (nout) *nout = td.nout;
     if (out && td.nr > 0) {
         CK(cudaMemcpyAsync(out, s.out.p, (size_t)td.nout * 4 * td.nr * sizeof(double),
-                           cudaMemcpyDeviceToHost, h->st));
+                           cudaMemcpyDeviceToHost, st ? st : h->st));
         h->d2h += (double)td.nout * 4 * td.nr * sizeof(double);
     }
     return YSG_OK;
@@ -777,10 +814,18 @@ int launch_batch_graph(ysg_handle* h, int nev)
     int ns4 = 0;
     int rc0 = ensure_ifft_scratch(h, nev, &ns4);
     if (rc0) return rc0;
+    // several events: K3 and K4 chained per event, so that each event's
+    // trace copy can start while the others are still in their stages
+    const bool chain = nev > 1;
+    while (chain && h->done_ev.size() < (size_t)nev) {
+        cudaEvent_t e = nullptr;
+        CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        h->done_ev.push_back(e);
+    }
     CK(cudaStreamBeginCapture(h->st, cudaStreamCaptureModeRelaxed));
     h->capturing = true;
-    int rc = enqueue_spectra(h, nev);
-    if (!rc) rc = enqueue_traces(h, nev, ns4);
+    int rc = enqueue_spectra(h, nev, !chain);
+    if (!rc) rc = chain ? enqueue_chains(h, nev, ns4) : enqueue_traces(h, nev, ns4);
     h->capturing = false;
     cudaGraph_t g = nullptr;
     cudaError_t ce = cudaStreamEndCapture(h->st, &g);
@@ -959,6 +1004,8 @@ int ysg_create(ysg_handle** out, int device)
     for (int i = 0; i < ysg_handle::NSIDE; i++)
         ok = ok && cudaStreamCreateWithFlags(&h->side[i], cudaStreamNonBlocking) == cudaSuccess &&
              cudaEventCreateWithFlags(&h->join_ev[i], cudaEventDisableTiming) == cudaSuccess;
+    ok = ok && cudaStreamCreateWithFlags(&h->copy_st, cudaStreamNonBlocking) == cudaSuccess &&
+         cudaEventCreateWithFlags(&h->copy_ev, cudaEventDisableTiming) == cudaSuccess;
     if (!ok || h->status.ensure(sizeof(int)) != cudaSuccess ||
         h->work.ensure(NSYS_COUNT * sizeof(unsigned long long)) != cudaSuccess) {
         ysg_destroy(h);
@@ -991,6 +1038,13 @@ void ysg_destroy(ysg_handle* h)
         if (h->join_ev[i]) cudaEventDestroy(h->join_ev[i]);
     }
     if (h->fork_ev) cudaEventDestroy(h->fork_ev);
+    if (h->copy_st) {
+        cudaStreamSynchronize(h->copy_st);
+        cudaStreamDestroy(h->copy_st);
+    }
+    if (h->copy_ev) cudaEventDestroy(h->copy_ev);
+    for (cudaEvent_t e : h->done_ev)
+        if (e) cudaEventDestroy(e);
     if (h->st) cudaStreamDestroy(h->st);
     delete h;
 }
@@ -1527,8 +1581,18 @@ int ysg_batch_run(ysg_handle* h, int nev, const ysg_event* evs, const ysg_time* 
     h->launches = 0;
     int rc = launch_batch_graph(h, nev);
     if (rc) return rc;
-    for (int e = 0; e < nev; e++) {
-        rc = copy_out(h, h->slots[(size_t)e], outs[e], nouts ? &nouts[e] : nullptr);
+    if (nev > 1) {
+        // each copy waits for its own event's chain (enqueue_chains); the
+        // handle's stream then waits for the copies
+        for (int e = 0; e < nev; e++) {
+            CK(cudaStreamWaitEvent(h->copy_st, h->done_ev[(size_t)e], 0));
+            rc = copy_out(h, h->slots[(size_t)e], outs[e], nouts ? &nouts[e] : nullptr, h->copy_st);
+            if (rc) return rc;
+        }
+        CK(cudaEventRecord(h->copy_ev, h->copy_st));
+        CK(cudaStreamWaitEvent(h->st, h->copy_ev, 0));
+    } else {
+        rc = copy_out(h, h->slots[0], outs[0], nouts ? &nouts[0] : nullptr);
         if (rc) return rc;
     }
     return finish(h, nev, true, true);

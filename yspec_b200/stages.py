@@ -10,7 +10,9 @@ Runs the configuration's first event through `Engine.run` (or, with
 prints, per run, the device time of each stage (Legendre table, solves,
 l-sum, filter + inverse FFT) measured with CUDA events on the engine's
 stream, the number of (omega,l) solves and the counted FP64 work of the
-solve stage.  With --gradient it runs the reverse mode instead
+solve stage.  A batch of several events runs each event's l-sum and time
+series back to back, so its "lsum" time covers both and "ifft" is zero.
+With --gradient it runs the reverse mode instead
 (Engine.gradient of a seeded random trace adjoint) and prints its stages
 (Legendre table, reverse sweeps, l-sum transpose, time-stage transpose).
 It is also the small, self-contained command used for ncu captures of one
