@@ -61,6 +61,12 @@ __device__ __forceinline__ cd out_factor(int out, cd w)
 namespace ysg {
 inline namespace YSG_VARIANT {
 
+// Rows of the spheroidal response matrices a form computes: the
+// shared-memory form and its cost model form only the rows a pair uses
+// (sph_solver_g: 0-2, sph_solver_nc: 0-1), the other forms all of them.
+constexpr int kSphRows = (YSG_SMEM_STAGES || YSG_COUNT_ONLY) ? 3 : 6;
+constexpr int kNcRows = (YSG_SMEM_STAGES || YSG_COUNT_ONLY) ? 2 : 4;
+
 __device__ __forceinline__ double huge_pow(int k)
 {
     if (YSG_COUNT_ONLY) return 1.0;
@@ -328,8 +334,8 @@ __device__ inline void rad_solver_wg(Ctx& c, double rr, double rs, mcplx yout[2]
 // yout[k]) names the rows the caller uses; the shared-memory form computes
 // only those (rows 0-2) and leaves the others zero, the other forms compute
 // all six.
-__device__ inline void sph_solver_g(Ctx& c, double rr, double rs, int ir, int is, mcplx yout[6][4],
-                                    int rows = 0x3f)
+__device__ inline void sph_solver_g(Ctx& c, double rr, double rs, int ir, int is,
+                                    mcplx yout[kSphRows][4], int rows = 0x3f)
 {
     const ModelHdr* mh = c.mh;
     const Knot* kn = c.kn;
@@ -402,8 +408,8 @@ __device__ inline void sph_solver_g(Ctx& c, double rr, double rs, int ir, int is
         const mcplx* mq = up ? ms2 : ms1;
         const mcplx* mb = up ? ms1 : ms2;
         unsigned nrow = 0;
-        for (int k = 0; k < 6; k++) {
-            if (k > 2 || !((rows >> k) & 1)) {
+        for (int k = 0; k < kSphRows; k++) {
+            if (!((rows >> k) & 1)) {
                 for (int i = 0; i < 4; i++) yout[k][i] = mk(0.0);
                 continue;
             }
@@ -422,13 +428,10 @@ __device__ inline void sph_solver_g(Ctx& c, double rr, double rs, int ir, int is
             for (int i = 0; i < 4; i++) yout[k][i] = ((-u[jump[i]]) / delta) * f;
         }
         if (YSG_COUNT_ONLY) c.nst[BvecSolidGTr::CLS] *= nrow;
-        return;
     }
-#endif
+#else
     (void)rows;
-    // the four jumps integrate the same span at the same omega: in the
-    // count-only build one pass counts for four
-    for (int i = 0; i < (YSG_COUNT_ONLY ? 1 : 4); i++) {
+    for (int i = 0; i < 4; i++) {
         mcplx s[6] = {mk(0.0), mk(0.0), mk(0.0), mk(0.0), mk(0.0), mk(0.0)};
         s[jump[i]] = mk(1.0);
         int scale4 = 0;
@@ -447,7 +450,7 @@ __device__ inline void sph_solver_g(Ctx& c, double rr, double rs, int ir, int is
         double f = huge_pow(scale3 - scale4);
         for (int k = 0; k < 6; k++) yout[k][i] = ys[k] * f;
     }
-    if (YSG_COUNT_ONLY) c.nst[BvecSolidG::CLS] *= 4u;
+#endif
 }
 
 // No gravity (KIND 0) / Cowling (KIND 1): sph_solver_ng (:827-1010),
@@ -456,7 +459,7 @@ __device__ inline void sph_solver_g(Ctx& c, double rr, double rs, int ir, int is
 // The shared-memory form computes only rows 0 and 1 (the ones the pair
 // uses) and leaves rows 2 and 3 zero.
 template <int KIND>
-__device__ inline void sph_solver_nc(Ctx& c, double rr, double rs, int ir, int is, mcplx yout[4][4])
+__device__ inline void sph_solver_nc(Ctx& c, double rr, double rs, int ir, int is, mcplx yout[kNcRows][4])
 {
     const ModelHdr* mh = c.mh;
     const Knot* kn = c.kn;
@@ -530,13 +533,10 @@ __device__ inline void sph_solver_nc(Ctx& c, double rr, double rs, int ir, int i
             const double f = huge_pow(scale3 - sw);
             for (int i = 0; i < 4; i++) yout[k][i] = ((sg * u[i]) / delta) * f;
         }
-        for (int k = 2; k < 4; k++)
-            for (int i = 0; i < 4; i++) yout[k][i] = mk(0.0);
 #endif
-        return;
     }
-#endif
-    for (int i = 0; i < (YSG_COUNT_ONLY ? 1 : 4); i++) {     // see sph_solver_g
+#else
+    for (int i = 0; i < 4; i++) {     // see sph_solver_g
         mcplx s[4] = {mk(0.0), mk(0.0), mk(0.0), mk(0.0)};
         s[i] = mk(1.0);
         int scale4 = 0;
@@ -555,7 +555,7 @@ __device__ inline void sph_solver_nc(Ctx& c, double rr, double rs, int ir, int i
         double f = huge_pow(scale3 - scale4);
         for (int k = 0; k < 4; k++) yout[k][i] = ys[k] * f;
     }
-    if (YSG_COUNT_ONLY) c.nst[BvecSolidNC<KIND>::CLS] *= 4u;
+#endif
 }
 
 // ---------------------------------------------------------------------------
@@ -699,8 +699,7 @@ __device__ inline void pair_spheroidal(Ctx& c, const EventDev& ev, int l, int j,
     set_l(c, l);
     set_omega(c, w);
     alpha_steps(c);
-    mcplx svs[5][6], ysph[6][4];
-    source_vector_sph(c, ev.is, ev.rs, ev.mm, svs);
+    mcplx ysph[kSphRows][4];
     if (ev.grav == 2) {
         // the rows of the responses used below: the potential (row 2) alone,
         // or the two displacement rows, with row 2 for the tilt and
@@ -708,7 +707,7 @@ __device__ inline void pair_spheroidal(Ctx& c, const EventDev& ev, int l, int j,
         const int rows = ev.pot ? 0x4 : ((ev.out == 2 && ev.cor != 0) ? 0x7 : 0x3);
         sph_solver_g(c, ev.rr, ev.rs, ev.ir, ev.is, ysph, rows);
     } else {
-        mcplx yng[4][4];
+        mcplx yng[kNcRows][4];
         if (ev.grav == 1) sph_solver_nc<1>(c, ev.rr, ev.rs, ev.ir, ev.is, yng);
         else sph_solver_nc<0>(c, ev.rr, ev.rs, ev.ir, ev.is, yng);
         for (int b = 0; b < 4; b++) {                  // yspec.f90:367-374
@@ -717,6 +716,10 @@ __device__ inline void pair_spheroidal(Ctx& c, const EventDev& ev, int l, int j,
             ysph[2][b] = mk(0.0);
         }
     }
+    // the source vectors depend on none of the solve's state: formed after
+    // it, they share no stack with the solver's minors
+    mcplx svs[5][6];
+    source_vector_sph(c, ev.is, ev.rs, ev.mm, svs);
     double zeta = (double)sqrtf((float)(l * (l + 1)));   // yspec.f90:255 (FP32)
     if (ev.pot) {
         // the potential perturbation at the receiver (the third solution
