@@ -249,7 +249,7 @@ class ModelSynthetics:
         transpose of the model chain by autograd."""
         import torch
 
-        from .model_chain import PARAMS
+        from .model_chain import PARAMS, ArrayModel
 
         km, eng = self.km, self.engine
         p = (rho.detach().cpu(), vp.detach().cpu(), vs.detach().cpu())
@@ -257,13 +257,16 @@ class ModelSynthetics:
         g = np.asarray(grad.detach().cpu().numpy(), dtype=np.float64)
         gout = np.zeros((g.shape[0], 4, g.shape[2]))
         gout[:, 1:4, :] = g
-        eng.upload(km.array_model(*p))
-        gval, gcs = eng.gradient(ev, gout)
-        # autograd runs backward passes with gradients off; the chain's own
-        # graph is needed here
+        # the chain at p once, with its graph (autograd runs backward passes
+        # with gradients off): its values are the model the reverse sweep runs
+        # on, as km.array_model(*p) would form them, and its graph carries
+        # dL/d(arrays) back to the knot parameters
         with torch.enable_grad():
             pp = tuple(x.clone().requires_grad_() for x in p)
             arrs = km.arrays(*pp)
+        eng.upload(ArrayModel(km.view0, km.r.numpy(), arrs, km.host.array("alpha"), km.host.array("beta")))
+        gval, gcs = eng.gradient(ev, gout)
+        with torch.enable_grad():
             s = sum((torch.from_numpy(gval[i]) * arrs[name]).sum() +
                     (torch.from_numpy(gcs[i]) * arrs[name + "_cs"]).sum() for i, name in enumerate(PARAMS))
             gr = torch.autograd.grad(s, pp, allow_unused=True)

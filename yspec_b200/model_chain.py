@@ -127,6 +127,31 @@ class _LayerSpline:
         return torch.stack(u)
 
 
+def _spline_fn():
+    """The spline map as an autograd function: the forward runs the
+    recurrences (the values the upload uses), the backward applies the
+    transpose of the same linear map, S^T g."""
+    import torch
+
+    global _SPLINE_FN
+    if _SPLINE_FN is None:
+        class _SplineFn(torch.autograd.Function):
+            @staticmethod
+            def forward(ctx, Y, km):
+                ctx.km = km
+                return km._spline_rec(Y)
+
+            @staticmethod
+            def backward(ctx, g):
+                return ctx.km.spline_matrix().T @ g, None
+
+        _SPLINE_FN = _SplineFn
+    return _SPLINE_FN
+
+
+_SPLINE_FN = None
+
+
 class KnotModel:
     """A deck as a differentiable function of its knot parameters.
 
@@ -164,13 +189,35 @@ class KnotModel:
 
     # -- the chain ----------------------------------------------------------
     def _spline(self, y):
-        """Per-layer spline second derivatives of y: (nknot,) or (nknot, m)."""
+        """Per-layer spline second derivatives of y: (nknot,) or (nknot, m).
+        The map is linear in y; under autograd its transpose is applied as
+        one product with the operator's matrix (_SplineFn) instead of
+        reversing the per-knot recurrences op by op."""
         import torch
 
         col = y.dim() == 1
         Y = y[:, None] if col else y
-        out = torch.cat([sp(Y[lo:hi + 1]) for sp, (lo, hi) in zip(self.spl, self.layers)])
+        if torch.is_grad_enabled() and Y.requires_grad and not Y.is_complex():
+            out = _spline_fn().apply(Y, self)
+        else:
+            out = self._spline_rec(Y)
         return out[:, 0] if col else out
+
+    def _spline_rec(self, Y):
+        """The recurrences of spline_r / tridag_ser_r, layer by layer."""
+        import torch
+
+        return torch.cat([sp(Y[lo:hi + 1]) for sp, (lo, hi) in zip(self.spl, self.layers)])
+
+    def spline_matrix(self):
+        """S with _spline(y) = S y (block diagonal, one block per layer),
+        formed once by the recurrences on the identity."""
+        import torch
+
+        if getattr(self, "_S", None) is None:
+            with torch.no_grad():
+                self._S = self._spline_rec(torch.eye(self.nknot, dtype=torch.float64))
+        return self._S
 
     def _gauss_setup(self, r: np.ndarray):
         """Interval index of the five gauslv nodes on every knot interval, and
