@@ -115,7 +115,10 @@ __global__ void __launch_bounds__(SolveCfg<PART>::BLOCK, SolveCfg<PART>::MINB)
             }
         }
         cd* dst = coefs[e] + (size_t)li * NCOEF * ev.nw + (j - 1);
-        for (int q = q0; q < q1; q++) dst[(size_t)q * ev.nw] = out[q];
+        // streaming stores: the coefficients are not read again in this
+        // launch, so they should not push the threads' stack frames out of L2
+        for (int q = q0; q < q1; q++)
+            __stcs(reinterpret_cast<double2*>(dst + (size_t)q * ev.nw), make_double2(out[q].x, out[q].y));
     }
     for (int q = 0; q < NSYS; q++) {
         unsigned long long v = c.nst[q];
