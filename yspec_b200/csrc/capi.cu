@@ -131,6 +131,7 @@ struct ysg_handle {
     DevBuf scratch[NSIDE];
     DevBuf work, status, items, counter, evdev, coefptr;
     int nitems = 0;                  // schedule-0 tiles
+    bool tiles_ready = false;        // the tiles of the active slots are on the device
     long long npairs = 0;            // pairs of the active slots
     int nev_items = 0;               // slots the items were built for
     DevBuf offs, keys0, keys1, vals0, vals1, sort_tmp;
@@ -272,19 +273,37 @@ void build_items(std::vector<Item>& out, int e, const EventDev& ev)
         for (int j0 = 0; j0 < ev.nw; j0 += 32) out.push_back({e, li, j0, item_cost(ev, li, j0)});
 }
 
-int upload_items(ysg_handle* h, std::vector<Item>& items, const std::vector<EventDev>& evs,
-                 const std::vector<cd*>& coefs)
+// The schedule-0 tiles of slots 0..nev-1, longest first, built and uploaded
+// only when a schedule-0 solve is about to run (a fixed or tuned schedule
+// 0, or the autotuner's trial of it): the cost-sorted schedules 1 and 2
+// never read them, and at c5 sizes the list has a million entries to sort.
+int ensure_tiles(ysg_handle* h, int nev)
 {
+    if (h->tiles_ready) return YSG_OK;
+    std::vector<Item> items;
+    for (int e = 0; e < nev; e++) build_items(items, e, h->slots[(size_t)e].pev);
     std::stable_sort(items.begin(), items.end(),
                      [](const Item& a, const Item& b) { return a.cost > b.cost; });
     std::vector<int4> packed(items.size());
     for (size_t i = 0; i < items.size(); i++) packed[i] = make_int4(items[i].ev, items[i].li, items[i].j0, 0);
     CK(h->items.ensure(std::max<size_t>(packed.size(), 1) * sizeof(int4)));
+    if (!packed.empty())
+        CK(cudaMemcpyAsync(h->items.p, packed.data(), packed.size() * sizeof(int4), cudaMemcpyHostToDevice, h->st));
+    CK(cudaStreamSynchronize(h->st));    // the host list goes out of scope
+    h->h2d += (double)(packed.size() * sizeof(int4));
+    h->nitems = (int)packed.size();
+    h->tiles_ready = true;
+    return YSG_OK;
+}
+
+int upload_items(ysg_handle* h, const std::vector<EventDev>& evs, const std::vector<cd*>& coefs)
+{
+    h->tiles_ready = false;
+    h->nitems = 0;
+    CK(h->items.ensure(sizeof(int4)));
     CK(h->evdev.ensure(std::max<size_t>(evs.size(), 1) * sizeof(EventDev)));
     CK(h->coefptr.ensure(std::max<size_t>(coefs.size(), 1) * sizeof(cd*)));
     CK(h->counter.ensure(2 * sizeof(int)));
-    if (!packed.empty())
-        CK(cudaMemcpyAsync(h->items.p, packed.data(), packed.size() * sizeof(int4), cudaMemcpyHostToDevice, h->st));
     CK(cudaMemcpyAsync(h->evdev.p, evs.data(), evs.size() * sizeof(EventDev), cudaMemcpyHostToDevice, h->st));
     CK(cudaMemcpyAsync(h->coefptr.p, coefs.data(), coefs.size() * sizeof(cd*), cudaMemcpyHostToDevice, h->st));
     // flat pair offsets of the events and buffers of the pair schedule
@@ -308,9 +327,8 @@ int upload_items(ysg_handle* h, std::vector<Item>& items, const std::vector<Even
     CK(h->vals1.ensure(pb));
     CK(h->sort_tmp.ensure(std::max<size_t>(pair_sort_tmp_bytes(np), 16)));
     CK(cudaStreamSynchronize(h->st));
-    h->h2d += (double)(packed.size() * sizeof(int4) + evs.size() * sizeof(EventDev) +
-                       coefs.size() * sizeof(cd*) + (off.size() + poff.size()) * sizeof(long long));
-    h->nitems = (int)packed.size();
+    h->h2d += (double)(evs.size() * sizeof(EventDev) + coefs.size() * sizeof(cd*) +
+                       (off.size() + poff.size()) * sizeof(long long));
     h->npairs = np;
     h->nev_items = (int)evs.size();
     for (int v = 0; v < NSOLVE_KERNELS; v++) {
@@ -323,15 +341,13 @@ int upload_items(ysg_handle* h, std::vector<Item>& items, const std::vector<Even
 // Work items of the batched solver for slots 0..nev-1, longest first.
 int upload_batch_items(ysg_handle* h, int nev)
 {
-    std::vector<Item> items;
     std::vector<EventDev> evs((size_t)nev);
     std::vector<cd*> coefs((size_t)nev);
     for (int e = 0; e < nev; e++) {
         evs[(size_t)e] = h->slots[(size_t)e].pev;
         coefs[(size_t)e] = h->slots[(size_t)e].coef.as<cd>();
-        build_items(items, e, evs[(size_t)e]);
     }
-    return upload_items(h, items, evs, coefs);
+    return upload_items(h, evs, coefs);
 }
 
 // Event inputs to the device: cos/sin of delta and e^{i m azst}
@@ -547,11 +563,11 @@ int resolve_schedule(ysg_handle* h, int nev)
     }
     if (!packable) {
         h->cur_sched = 0;
-        return YSG_OK;
+        return ensure_tiles(h, nev);
     }
     if (h->sched >= 0) {
         h->cur_sched = h->sched;
-        return YSG_OK;
+        return h->sched == 0 ? ensure_tiles(h, nev) : YSG_OK;
     }
     long long maxl = 0, maxw = 0;
     for (int e = 0; e < nev; e++) {
@@ -568,8 +584,10 @@ int resolve_schedule(ysg_handle* h, int nev)
     auto it = h->tuned.find(sig);
     if (it != h->tuned.end()) {
         h->cur_sched = it->second;
-        return YSG_OK;
+        return it->second == 0 ? ensure_tiles(h, nev) : YSG_OK;
     }
+    int rc0 = ensure_tiles(h, nev);     // the trials include schedule 0
+    if (rc0) return rc0;
     // The first tuning of a handle runs each schedule once untimed: with lazy
     // module loading a kernel's first launch also loads its module on the
     // host, which would be charged to whichever schedule launches it first.
