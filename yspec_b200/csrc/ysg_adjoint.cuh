@@ -412,7 +412,16 @@ __device__ __noinline__ bool yint_log(Ctx& c, int i1, int i2, double r1, double 
             if (q >= L.nmax) return false;
             double rr = __dadd_rn(rr1, __dmul_rn((double)(j - 1), drr));
             const size_t e = (size_t)q * L.st;
+            // streaming stores (evict-first): a log outgrows L2 and is read
+            // back only by the reverse pass, so it should not push the
+            // threads' stack frames out of L2
+#ifdef __CUDA_ARCH__
+            for (int k = 0; k < N; k++)
+                __stcs(reinterpret_cast<double2*>(L.y + ((size_t)q * LOG_N + k) * L.st),
+                       make_double2(y[k].x, y[k].y));
+#else
             for (int k = 0; k < N; k++) L.y[((size_t)q * LOG_N + k) * L.st] = y[k];
+#endif
             L.x[e] = rr;
             L.h[e] = drr;
             L.il[e] = i;
